@@ -1,0 +1,440 @@
+"""Generate the golden fixtures for the FR residual-and-update path.
+
+Runs the reference implementation (AutoFlowCFD, pure Python + Numba, read from
+``/root/reference``) on small meshes from ``autoflowcfd_b200.boxmesh`` and
+stores, per case, every input the path consumes (operators, Jacobians, the
+flattened face tables, boundary configuration, turbulence fields, state) and
+the reference's own outputs:
+
+* inviscid and viscous residuals (``FRSolver.compute_inviscid_residual`` /
+  ``compute_viscous_residual``, ``core/fr_solver/solver.py:351-432``);
+* the local time step (``core/fr_solver/cfl.py:12-147``);
+* the SST source / transport / point-implicit update
+  (``core/fr_solver/turbulence.py:178-330``);
+* the state after one and two ``FRSolver.step`` calls
+  (``core/fr_solver/step.py:15-221``) and their residual norms;
+* the wall force coefficients (``postprocess/fr_coefficients.py:27-152``).
+
+The reference cannot be imported where the tests run on a GPU, so the outputs
+are committed as ``tests/golden/*.npz``.  Re-run with
+``NUMBA_CACHE_DIR=/tmp/nc python tests/golden/make_golden.py``.
+"""
+
+import copy
+import os
+import sys
+import types
+from types import SimpleNamespace
+
+import numpy as np
+
+REF = "/root/reference"
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REF, "src"))
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/afr_numba_cache")
+
+from autoflowcfd_b200 import boxmesh  # noqa: E402
+
+GAMMA = 1.4
+BC_CODES = {"WALL": 0, "FARFIELD": 1, "INLET": 2, "OUTLET": 3, "SYMMETRY": 4}
+
+
+class _Nodes:
+    def __init__(self, c):
+        self._c = c
+
+    def get_coordinates(self):
+        return self._c
+
+
+class _Cells:
+    def __init__(self, conn):
+        self.connectivity = conn
+
+
+class _Bnd:
+    def __init__(self, groups, bc_types):
+        self.groups = groups
+        self.bc_types = bc_types
+
+
+def ref_mesh(box, order, bc_types=None):
+    """Load a BoxMesh through the reference's own HighOrderMesh loader.
+
+    ``bc_types`` maps plane names to the mesh-level boundary types the
+    reference's force integration reads (``postprocess/fr_coefficients.py:74-79``)."""
+    from autoflowcfd.grid.high_order.high_order_mesh import HighOrderMesh
+    from autoflowcfd.grid.schema.grid_boundaries import BoundaryMap
+
+    nodes = box.nodes.copy()
+    conn = box.conn.astype(np.int32).copy()
+    Lx, Ly, Lz = box.lengths
+    tol = 1e-9 * max(Lx, Ly, Lz, 1.0)
+    ijk = box.node_ijk(conn)  # cells touching a plane with >= 3 nodes, by lattice index
+    groups = {}
+    for name, ax, val in (("x_min", 0, 0), ("x_max", 0, box.shape[0]), ("y_min", 1, 0),
+                          ("y_max", 1, box.shape[1]), ("z_min", 2, 0), ("z_max", 2, box.shape[2])):
+        groups[name] = np.flatnonzero((ijk[:, :, ax] == val).sum(axis=1) >= 3).astype(np.int32)
+    if box.periodic:
+        bmap = BoundaryMap(
+            groups=groups, bc_types={n: "PERIODIC" for n in groups},
+            parameters={"x_min": {"paired_with": "x_max", "translation": [Lx, 0.0, 0.0]},
+                        "y_min": {"paired_with": "y_max", "translation": [0.0, Ly, 0.0]},
+                        "z_min": {"paired_with": "z_max", "translation": [0.0, 0.0, Lz]}})
+    else:
+        bmap = _Bnd(groups, dict(bc_types or {n: "FARFIELD" for n in groups}))
+    if box.kind == "prism":
+        vol = SimpleNamespace(cell_count=len(conn), nodes=_Nodes(nodes), cells=_Cells(np.zeros((0, 4), np.int32)),
+                              prism_cells=_Cells(conn), boundaries=bmap)
+    else:
+        vol = SimpleNamespace(cell_count=len(conn), nodes=_Nodes(nodes), cells=_Cells(conn),
+                              prism_cells=_Cells(np.zeros((0, 6), np.int32)), boundaries=bmap)
+    mesh = HighOrderMesh(order=order)
+    mesh.load_from_volume_mesh(vol, build_faces=True)
+    return mesh
+
+
+def plane_provider(mesh, box, plane_cfg):
+    """Face-exact BoundaryGhostStateProvider keyed by the plane each boundary
+    face centre lies on (same construction as the reference's
+    ``tests/validation/_channel_mesh.py:19-66``)."""
+    from autoflowcfd.boundary.fr_ghost_state import BoundaryGhostStateProvider
+
+    fc = mesh.face_connectivity
+    group_code = np.full(fc.n_faces, -1, dtype=np.int32)
+    bidx = fc.get_boundary_face_indices()
+    if len(bidx):
+        planes = box.plane_of_faces(fc.face_node_ids[bidx])
+        assert np.all(planes >= 0), "boundary face off the box planes"
+        group_code[bidx] = planes
+    code_to_config = {i: plane_cfg[name] for i, name in enumerate(boxmesh.PLANE_NAMES)}
+    default = {"type": "FARFIELD", "Q_free": list(plane_cfg.get("_default_Q", [1.225, 0.0, 0.0, 0.0, 101325.0]))}
+    return BoundaryGhostStateProvider(group_code, code_to_config, default)
+
+
+def bc_tables(provider, n_faces):
+    """Lower a BoundaryGhostStateProvider to plain arrays."""
+    if provider is None:
+        return dict(bc_group=np.full(n_faces, -1, np.int32), bc_type=np.zeros(1, np.int32),
+                    bc_noslip=np.ones(1, np.int32), bc_wall_vel=np.zeros((1, 3)),
+                    bc_Q=np.zeros((1, 5)), bc_p_out=np.zeros(1), bc_default=np.int32(0))
+    codes = sorted(provider.code_to_config)
+    n = (max(codes) + 1 if codes else 0) + 1  # last slot = default config
+    t = np.zeros(n, np.int32)
+    ns = np.ones(n, np.int32)
+    wv = np.zeros((n, 3))
+    Q = np.zeros((n, 5))
+    po = np.zeros(n)
+
+    def put(i, cfg):
+        t[i] = BC_CODES[cfg["type"]]
+        ns[i] = 1 if cfg.get("is_no_slip", True) else 0
+        if cfg.get("wall_velocity") is not None:
+            wv[i] = np.asarray(cfg["wall_velocity"], float)
+        if "Q_free" in cfg:
+            Q[i] = np.asarray(cfg["Q_free"], float)
+        if "Q_inlet" in cfg:
+            Q[i] = np.asarray(cfg["Q_inlet"], float)
+        po[i] = float(cfg.get("p_outlet", 0.0))
+
+    for c in codes:
+        put(c, provider.code_to_config[c])
+    put(n - 1, provider.default_config)
+    gc = np.asarray(provider.group_code, np.int32).copy()
+    gc[(gc < 0) | ~np.isin(gc, codes)] = n - 1
+    return dict(bc_group=gc, bc_type=t, bc_noslip=ns, bc_wall_vel=wv, bc_Q=Q, bc_p_out=po,
+                bc_default=np.int32(n - 1))
+
+
+def flat_tables(mesh, ops):
+    from autoflowcfd.core.fr_operators.face_kernels import get_flat_face_geometry
+
+    f = get_flat_face_geometry(mesh, ops)
+    colors = np.full(f.n_faces, -1, np.int32)
+    for c, idx in enumerate(f.color_face_indices):
+        colors[idx] = c
+    return dict(
+        owner_cell=f.owner_cell, neighbor_cell=f.neighbor_cell, is_boundary=f.is_boundary.astype(np.uint8),
+        owner_axis=f.owner_axis, owner_side=f.owner_side, neighbor_axis=f.neighbor_axis,
+        neighbor_side=f.neighbor_side, owner_is_primary=f.owner_is_primary.astype(np.uint8),
+        neighbor_is_primary=f.neighbor_is_primary.astype(np.uint8), true_normal=f.true_normal,
+        nb_src0_cell=f.neighbor_src0_cell, nb_src0_mat=f.neighbor_src0_mat, nb_src1_idx=f.neighbor_src1_idx,
+        nb_src1_cell=f.neighbor_src1_cell, nb_src1_mat=f.neighbor_src1_mat.reshape(-1, f.n_fp, f.n_sps),
+        ow_src0_cell=f.owner_src0_cell, ow_src0_mat=f.owner_src0_mat, ow_src1_idx=f.owner_src1_idx,
+        ow_src1_cell=f.owner_src1_cell, ow_src1_mat=f.owner_src1_mat.reshape(-1, f.n_fp, f.n_sps),
+        boundary_extrap=f.boundary_extrap, g_left=f.g_left, g_right=f.g_right,
+        dist_fp_of_sp=f.dist_fp_of_sp, dist_axis_coord_of_sp=f.dist_axis_coord_of_sp, colors=colors,
+    )
+
+
+def op_tables(ops):
+    return dict(
+        D_3d_prism=ops.D_3d_prism, D_3d_tet=ops.D_3d_tet,
+        c2f_prism=ops.overint_interp_c2f_prism, c2f_tet=ops.overint_interp_c2f_tet,
+        Dfine_prism=ops.overint_D_fine_prism, Dfine_tet=ops.overint_D_fine_tet,
+        f2c_prism=ops.overint_restrict_f2c_prism, f2c_tet=ops.overint_restrict_f2c_tet,
+        filter_prism=ops.filter_prism, filter_tet=ops.filter_tet,
+    )
+
+
+def conserved(rho, u, v, w, p):
+    E = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return np.stack([rho, rho * u, rho * v, rho * w, E], axis=-1)
+
+
+def vortex_state(x, y, Lx, Ly, rc, rho_inf, p_inf, u_inf, beta=5.0):
+    """Isentropic vortex (``tests/validation/_isentropic_vortex.py:42-71``),
+    centre at the box centre, core radius rc."""
+    a_inf = np.sqrt(GAMMA * p_inf / rho_inf)
+    dx = x - 0.5 * Lx
+    dy = y - 0.5 * Ly
+    r2 = (dx / rc) ** 2 + (dy / rc) ** 2
+    swirl = (beta * a_inf / (2 * np.pi)) * np.exp(0.5 * (1 - r2))
+    theta = 1 - (GAMMA - 1) * beta**2 / (8 * GAMMA * np.pi**2) * np.exp(1 - r2)
+    rho = rho_inf * theta ** (1 / (GAMMA - 1))
+    p = p_inf * theta ** (GAMMA / (GAMMA - 1))
+    return conserved(rho, u_inf - swirl * dy / rc, swirl * dx / rc, np.zeros_like(x), p)
+
+
+def tgv_state(x, y, z, L, u0, rho0, p0):
+    """Taylor-Green vortex initial field (``tests/validation/test_tgv.py:96-112``)."""
+    k = 2 * np.pi / L
+    u = u0 * np.sin(k * x) * np.cos(k * y) * np.cos(k * z)
+    v = -u0 * np.cos(k * x) * np.sin(k * y) * np.cos(k * z)
+    w = np.zeros_like(u)
+    p = p0 + rho0 * u0**2 / 16 * (np.cos(2 * k * x) + np.cos(2 * k * y)) * (np.cos(2 * k * z) + 2)
+    rho = p / p0 * rho0
+    return conserved(rho, u, v, w, p)
+
+
+def channel_state(x, y, z, L, rho_inf, u_inf, p_inf, seed):
+    """Freestream with a smooth, seeded multi-mode perturbation (a few percent)."""
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0, 2 * np.pi, size=8)
+    Lx, Ly, Lz = L
+    s = lambda i, a, b, c: np.sin(2 * np.pi * (a * x / Lx + b * y / Ly + c * z / Lz) + ph[i])  # noqa: E731
+    rho = rho_inf * (1 + 0.02 * s(0, 1, 1, 0) + 0.01 * s(1, 0, 2, 1))
+    u = u_inf * (1 + 0.05 * s(2, 2, 0, 1)) * np.tanh(6 * z / Lz + 0.3)
+    v = 0.04 * u_inf * s(3, 1, 1, 1)
+    w = 0.03 * u_inf * s(4, 0, 1, 2)
+    p = p_inf * (1 + 0.002 * s(5, 1, 0, 1))
+    return conserved(rho, u, v, w, p)
+
+
+def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_only=False,
+              global_dt_factor=None, n_steps=2, turb_init=None):
+    import numba
+    from autoflowcfd.core.fr_solver import FRSolver
+    from autoflowcfd.core.time_integration import TimeIntegrationScheme
+    from autoflowcfd.postprocess.fr_coefficients import compute_aerodynamic_coefficients_fr
+
+    numba.set_num_threads(min(8, os.cpu_count() or 1))
+    mesh_bc = None
+    if plane_cfg is not None:
+        mesh_bc = {n: ("WALL" if plane_cfg[n]["type"] == "WALL" and plane_cfg[n].get("is_no_slip", True)
+                       else "FARFIELD") for n in boxmesh.PLANE_NAMES}
+    mesh = ref_mesh(box, order, mesh_bc)
+    rho_inf, u_inf, p_inf = free
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name=turb, time_scheme=TimeIntegrationScheme.SSP_RK3,
+                      rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf, mu_molecular=mu,
+                      n_threads=min(8, os.cpu_count() or 1))
+    solver.order_continuation_enabled = False
+    if not box.periodic:
+        solver.boundary_ghost_provider = plane_provider(mesh, box, plane_cfg)
+    N, S = mesh.n_cells, mesh.n_sps_per_cell
+    n_vars = solver.state.n_vars
+    xyz = mesh.sps_coords.reshape(N, S, 3)
+    U = np.zeros((N, S, n_vars))
+    U[:, :, :5] = state_fn(xyz[..., 0], xyz[..., 1], xyz[..., 2])
+
+    out = dict(meta_name=np.array(name), order=np.int32(order), n_cells=np.int32(N), n_prism=np.int32(mesh.n_prism_cells),
+               n_sps=np.int32(S), n_fine=np.int32(mesh.n_sps_per_cell_fine), n_vars=np.int32(n_vars),
+               turb=np.array(turb), mu=np.float64(mu), freestream=np.array(free, float),
+               inviscid_only=np.int32(inviscid_only), periodic=np.int32(box.periodic),
+               global_dt_factor=np.float64(global_dt_factor or 0.0),
+               box_shape=np.array(box.shape), box_lengths=np.array(box.lengths), box_kind=np.array(box.kind))
+    out["det_jacs"] = mesh.jacobians["det_jacs"].reshape(N, S)
+    out["inv_jacs"] = mesh.jacobians["inv_jacs"].reshape(N, S, 3, 3)
+    Fn = mesh.n_sps_per_cell_fine
+    out["det_jacs_fine"] = mesh.jacobians_fine["det_jacs"].reshape(N, Fn)
+    out["inv_jacs_fine"] = mesh.jacobians_fine["inv_jacs"].reshape(N, Fn, 3, 3)
+    out["cell_volumes"] = mesh.get_all_cell_volumes()
+    out["sps_coords"] = xyz
+    out["nodes"] = mesh._node_coords
+    out["conn"] = (mesh._fixed_prism_conn if mesh.n_prism_cells else mesh._fixed_tet_conn).astype(np.int64)
+    out.update(op_tables(solver.ops))
+    out.update(flat_tables(mesh, solver.ops))
+    out.update(bc_tables(solver.boundary_ghost_provider, mesh.face_connectivity.n_faces))
+    out["true_area_weight"] = np.asarray(mesh.face_flux_points.true_area_weight, float)
+    if mesh_bc is not None:
+        from autoflowcfd.grid.connectivity.face_connectivity import tag_boundary_groups
+
+        gcode, name_to_code = tag_boundary_groups(mesh.face_connectivity, mesh.boundary_groups)
+        wall_codes = [c for n, c in name_to_code.items() if mesh.boundary_bc_types.get(n) == "WALL"]
+        out["cd_wall_face"] = np.isin(gcode, wall_codes).astype(np.uint8)
+
+    if turb == "SST":
+        nodes = mesh._node_coords
+        wall = np.flatnonzero(np.abs(nodes[:, 2]) < 1e-12)
+        solver.compute_wall_distance_field(nodes, wall)
+        out["wall_distance"] = solver.wall_distance.copy()
+        k0, w0, nut0 = turb_init(xyz)
+        solver.turb_model.k_field = k0.copy()
+        solver.turb_model.omega_field = w0.copy()
+        solver.turb_model.nu_t = nut0.copy()
+        rho = U[:, :, 0]
+        U[:, :, 5] = rho * k0
+        U[:, :, 6] = rho * w0
+        out["k0"], out["omega0"], out["nu_t0"] = k0, w0, nut0
+    out["U0"] = U.copy()
+
+    orig_dt = solver._compute_local_time_step
+
+    def snapshot():
+        snap = dict(U=solver.state.U.copy())
+        if solver.turb_model is not None:
+            snap.update(k=solver.turb_model.k_field.copy(), w=solver.turb_model.omega_field.copy(),
+                        nut=solver.turb_model.nu_t.copy())
+        return snap
+
+    def restore(snap):
+        solver.state.U = snap["U"].copy()
+        solver.state._update_primitives()
+        if solver.turb_model is not None:
+            solver.turb_model.k_field = snap["k"].copy()
+            solver.turb_model.omega_field = snap["w"].copy()
+            solver.turb_model.nu_t = snap["nut"].copy()
+            if hasattr(solver.turb_model, "_last_beta_blend"):
+                del solver.turb_model._last_beta_blend
+
+    solver.state.U = U.copy()
+    solver.state._update_primitives()
+    s0 = snapshot()
+
+    # --- single evaluations at the initial state ---
+    out["R_inv"] = solver.compute_inviscid_residual().copy()
+    out["R_visc"] = solver.compute_viscous_residual().copy()
+    out["dt_local"] = orig_dt().copy()
+    restore(s0)
+
+    if turb == "SST":
+        import autoflowcfd.core.turbulence.transport as tr
+
+        captured = {}
+        real = tr.compute_turbulence_transport_residual
+
+        def spy(*a, **kw):
+            r = real(*a, **kw)
+            captured["tk"], captured["tw"] = r[0].copy(), r[1].copy()
+            return r
+
+        tr.compute_turbulence_transport_residual = spy
+        try:
+            dtl = orig_dt()
+            Sk, Sw = solver.compute_turbulence_source(dtl)
+        finally:
+            tr.compute_turbulence_transport_residual = real
+        out["sst_Sk"], out["sst_Sw"] = Sk.copy(), Sw.copy()
+        out["sst_tk"], out["sst_tw"] = captured["tk"], captured["tw"]
+        out["sst_k1"] = solver.turb_model.k_field.copy()
+        out["sst_w1"] = solver.turb_model.omega_field.copy()
+        out["sst_nut1"] = solver.turb_model.nu_t.copy()
+        restore(s0)
+
+    # --- full steps ---
+    if global_dt_factor:
+        solver._compute_local_time_step = lambda: np.full((N, S), global_dt_factor * float(np.min(orig_dt())))
+    if inviscid_only:
+        solver.compute_viscous_residual = lambda: np.zeros_like(solver.state.U)
+    norms = []
+    for s in range(n_steps):
+        norms.append(solver.step(1e-3))
+        out[f"U_step{s + 1}"] = solver.state.U.copy()
+        if solver.turb_model is not None:
+            out[f"k_step{s + 1}"] = solver.turb_model.k_field.copy()
+            out[f"w_step{s + 1}"] = solver.turb_model.omega_field.copy()
+            out[f"nut_step{s + 1}"] = solver.turb_model.nu_t.copy()
+    out["norms"] = np.array(norms)
+
+    if not box.periodic and not inviscid_only:
+        coef = compute_aerodynamic_coefficients_fr(solver, reference_area=1.0)
+        out["cd_cl"] = np.array([coef.Cd, coef.Cl, coef.Cs], float)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: N={N} S={S} faces={len(out['owner_cell'])} colors={out['colors'].max() + 1} "
+          f"norms={norms}", flush=True)
+    return out
+
+
+def main(which=None):
+    cases = {}
+
+    def c_tet_p1():
+        L = 1.0
+        box = boxmesh.tet_box(3, 3, 3, (L, L, L), jitter=0.0, periodic=True)
+        rho, p = 1.225, 101325.0
+        u = 0.5 * np.sqrt(GAMMA * p / rho)
+        make_case("tet_p1_vortex", box, 1, "NONE", 1.8e-5, (rho, u, p), None,
+                  lambda x, y, z: vortex_state(x, y, L, L, 0.2 * L, rho, p, u),
+                  inviscid_only=True, global_dt_factor=3.0)
+
+    def c_prism_p2_sst():
+        Ls = (4.0, 2.0, 1.5)
+        box = boxmesh.prism_box(4, 3, 3, Ls, jitter=0.1, seed=7)
+        rho, p = 1.225, 101325.0
+        u = 0.1 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e6
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        k_in = 1.5 * (0.01 * u) ** 2
+        w_in = rho * k_in / (10 * mu)
+
+        def turb_init(xyz):
+            rng = np.random.default_rng(3)
+            N, S = xyz.shape[:2]
+            pert = 1 + 0.2 * np.sin(2 * np.pi * xyz[..., 0] / Ls[0] + 0.3) * np.cos(np.pi * xyz[..., 2] / Ls[2])
+            k = k_in * pert
+            w = w_in * (1 + 0.3 * np.cos(2 * np.pi * xyz[..., 1] / Ls[1]))
+            nut = 10 * mu / rho * (1 + 0.5 * rng.uniform(size=(N, S)))
+            return k, w, nut
+
+        make_case("prism_p2_sst", box, 2, "SST", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 11), turb_init=turb_init)
+
+    def c_prism_p1_ns():
+        Ls = (2.0, 1.0, 1.0)
+        box = boxmesh.prism_box(4, 3, 2, Ls, jitter=0.1, seed=5, bump=(0.05, 1.0, 0.5, 0.3))
+        rho, p = 1.225, 101325.0
+        u = 0.2 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e5
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        cfg["x_min"] = {"type": "INLET", "Q_inlet": Qf}
+        cfg["x_max"] = {"type": "OUTLET", "p_outlet": p}
+        cfg["y_min"] = {"type": "SYMMETRY"}
+        cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
+        make_case("prism_p1_ns", box, 1, "NONE", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 5))
+
+    def c_tet_p3():
+        L = 1.0
+        box = boxmesh.tet_box(2, 2, 2, (L, L, L), jitter=0.05, seed=9, periodic=True)
+        rho, p = 1.225, 101325.0
+        u0 = 0.1 * np.sqrt(GAMMA * p / rho)
+        make_case("tet_p3_tgv", box, 3, "NONE", 1.8e-5, (rho, 0.0, p), None,
+                  lambda x, y, z: tgv_state(x, y, z, L, u0, rho, p), inviscid_only=True, global_dt_factor=3.0,
+                  n_steps=1)
+
+    cases = {"tet_p1_vortex": c_tet_p1, "prism_p2_sst": c_prism_p2_sst, "prism_p1_ns": c_prism_p1_ns,
+             "tet_p3_tgv": c_tet_p3}
+    for k, fn in cases.items():
+        if which and k not in which:
+            continue
+        fn()
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or None)
