@@ -1,0 +1,674 @@
+// C-ABI of the B200 FR residual-and-update library (declared in include/afr_b200.h).
+//
+// afr_create copies the reference's flattened mesh tables to HBM once, builds
+// the per-cell slot lists (every face side that lifts a correction into a
+// cell, in ascending face-color order) and allocates the scratch the step
+// needs.  The step then runs, per RK stage, one gradient pre-pass and one
+// fused per-cell stage kernel (see afr_kernels.cuh), plus the SST kernels once
+// per step (afr_sst.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/afr_b200.h"
+#include "afr_sst.cuh"
+
+using namespace afr;
+
+#define AFR_VERSION 100
+
+struct afr_handle {
+  int N = 0, n_prism = 0, order = 0, S = 0, Fn = 0, P = 0, F = 0, nv = 5;
+  afr_params prm{};
+  Geom g{};
+  Ops ops{};
+  Faces fc{};
+  Bc bc{};
+  // scratch
+  double* grads = nullptr;
+  double* Ua = nullptr;
+  double* Ub = nullptr;
+  double* dt = nullptr;
+  double* norm_part = nullptr;
+  double* red = nullptr;      // reduction results
+  double* pt = nullptr;
+  double* cfp = nullptr;
+  uint8_t* wall_face = nullptr;
+  uint8_t* cd_wall = nullptr;
+  double* area_w = nullptr;
+  int32_t* cd_faces = nullptr;
+  int n_cd_faces = 0;
+  double* cd_part = nullptr;  // (n_cd_faces, 6)
+  unsigned* status = nullptr;
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(afr_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(afr_handle* h, cudaError_t e, const char* what) {
+  return fail(h, AFR_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+int dalloc(afr_handle* h, T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(h, AFR_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  h->allocs.push_back((void*)*p);
+  h->bytes += n * sizeof(T);
+  return AFR_OK;
+}
+
+template <class T>
+int upload(afr_handle* h, T** dst, const T* src, size_t n, cudaStream_t st) {
+  int rc = dalloc(h, dst, n);
+  if (rc) return rc;
+  if (src && n) {
+    cudaError_t e = cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(h, e, "upload");
+  }
+  return AFR_OK;
+}
+
+template <class T>
+int upload_i32(afr_handle* h, int32_t** dst, const T* src, size_t n, cudaStream_t st, std::vector<int32_t>& tmp) {
+  tmp.assign(n, 0);
+  for (size_t i = 0; i < n; ++i) tmp[i] = (int32_t)src[i];
+  int rc = upload(h, dst, tmp.data(), n, st);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(st);  // tmp is reused by the caller
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "upload sync");
+}
+
+__global__ void k_form_adj(const double* det, const double* inv, double* adj, size_t npts) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * 9) return;
+  adj[t] = det[t / 9] * inv[t];  // compute_adj_j, core/fr_operators/volume_contract.py:47-80
+}
+
+__global__ void k_metric_flux_scale(const double* adj, double* mfs, size_t npts) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const double* a = adj + p * 9;
+  double acc = 0.0;  // sum_m |adj[m,:]|, core/fr_solver/solver_geometry.py:18-32
+  for (int m = 0; m < 3; ++m) acc += sqrt(a[m * 3] * a[m * 3] + a[m * 3 + 1] * a[m * 3 + 1] + a[m * 3 + 2] * a[m * 3 + 2]);
+  mfs[p] = acc;
+}
+
+// deterministic single-block reductions (fixed order for a given n)
+__global__ void k_reduce_sum(const double* x, size_t n, double* out) {
+  __shared__ double sh[1024];
+  double acc = 0.0;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) acc += x[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_reduce_min(const double* x, size_t n, double* out) {
+  __shared__ double sh[1024];
+  double acc = INFINITY;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) acc = fmin(acc, x[i]);
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_fill_scaled(double* x, size_t n, const double* v, double factor) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = factor * (*v);
+}
+
+// per wall face: pressure and viscous force partials (postprocess/fr_coefficients.py:105-133)
+template <int S, int NP>
+__global__ void k_force(Geom g, Ops ops, Faces fc, const int32_t* faces, int nf, const double* U, int nv,
+                        const double* grads, const double* nut, const double* area_w, double mu, double* part) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  const int f = faces[t];
+  const int oc = fc.owner[f];
+  const int ct = cell_type(g, oc);
+  const int ax = fc.o_axis[f];
+  const double* E = ops.extrap + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] < 0.0 ? 0 : 1)) * NP * S;
+  double fp[3] = {0, 0, 0}, fv[3] = {0, 0, 0};
+  for (int i = 0; i < NP; ++i) {
+    double pf = 0.0, mt = 0.0, gv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < S; ++s) {
+      const size_t p = (size_t)oc * S + s;
+      const double* u = U + p * nv;
+      const double rho = fmax(u[0], 1e-10);
+      const double ux = u[1] / rho, uy = u[2] / rho, uz = u[3] / rho;
+      const double pr = fmax((u[4] - rho * (0.5 * (ux * ux + uy * uy + uz * uz))) * 0.4, 1.0);
+      const double w = E[i * S + s];
+      pf += w * pr;
+      if (nut) mt += w * (rho * nut[p]);
+      for (int k = 0; k < 9; ++k) gv[k] += w * grads[p * 12 + k];
+    }
+    const double* n = fc.tnormal + ((size_t)f * NP + i) * 3;
+    const double aw = area_w[(size_t)f * NP + i];
+    for (int d = 0; d < 3; ++d) fp[d] += pf * n[d] * aw;
+    const double mtot = mu + mt;
+    const double div = gv[0] + gv[4] + gv[8];
+    for (int r = 0; r < 3; ++r) {
+      double tr = 0.0;
+      for (int c = 0; c < 3; ++c) {
+        const double sij = 0.5 * (gv[r * 3 + c] + gv[c * 3 + r]);
+        const double tau = 2.0 * mtot * sij + ((r == c) ? (-2.0 / 3.0 * mtot) * div : 0.0);
+        tr += tau * n[c];
+      }
+      fv[r] += tr * aw;
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    part[t * 6 + d] = fp[d];
+    part[t * 6 + 3 + d] = fv[d];
+  }
+}
+
+template <int S, int FN, int NP, int N1D>
+struct Launch {
+  static size_t stage_smem() { return sizeof(double) * StageSmem<S, FN, NP>::total; }
+  static cudaError_t grad(afr_handle* h, const double* U, cudaStream_t st) {
+    k_grad<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, h->grads);
+    return cudaGetLastError();
+  }
+  static cudaError_t stage(afr_handle* h, const StageArgs& a, cudaStream_t st) {
+    const size_t smem = stage_smem();
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_stage<S, FN, NP, N1D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr = true;
+    }
+    k_stage<S, FN, NP, N1D><<<h->N, 128, smem, st>>>(h->g, h->ops, h->fc, h->bc, a);
+    return cudaGetLastError();
+  }
+  static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st) {
+    k_sst_point<S><<<h->N, 128, 0, st>>>(h->g, h->ops, a);
+    const int nt = h->F * NP;
+    k_sst_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    k_sst_update<S, NP><<<h->N, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    return cudaGetLastError();
+  }
+  static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
+    if (h->n_cd_faces == 0) return cudaSuccess;
+    k_force<S, NP><<<(h->n_cd_faces + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->cd_faces, h->n_cd_faces, U,
+                                                                 h->nv, h->grads, nut, h->area_w, h->prm.mu,
+                                                                 h->cd_part);
+    return cudaGetLastError();
+  }
+};
+
+template <class Fn>
+cudaError_t dispatch(afr_handle* h, Fn&& fn) {
+  switch (h->order) {
+    case 1: return fn(Launch<8, 27, 4, 2>());
+    case 2: return fn(Launch<27, 64, 9, 3>());
+    case 3: return fn(Launch<64, 64, 16, 4>());
+  }
+  return cudaErrorInvalidValue;
+}
+
+int check_status(afr_handle* h, cudaStream_t st) {
+  unsigned s = 0;
+  cudaError_t e = cudaMemcpyAsync(&s, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "status read");
+  if (s & DS_BAD_INDEX) return fail(h, AFR_EINDEX, "kernel saw an out-of-range table index");
+  if (s & DS_NONFINITE) return fail(h, AFR_ENONFINITE, "non-finite value in the state");
+  return AFR_OK;
+}
+
+StageArgs base_args(afr_handle* h) {
+  StageArgs a{};
+  a.nv = h->nv;
+  a.mu = h->prm.mu;
+  a.inviscid_only = h->prm.inviscid_only;
+  a.status = h->status;
+  a.grads = h->grads;
+  return a;
+}
+
+int compute_dt(afr_handle* h, const double* U, const double* nut, double* dt, cudaStream_t st) {
+  const size_t n = (size_t)h->N * h->S;
+  k_local_dt<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(h->g, h->S, h->order, U, h->nv, nut, h->prm.mu, dt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(h, e, "local dt");
+  if (h->prm.global_dt_factor > 0.0) {
+    k_reduce_min<<<1, 1024, 0, st>>>(dt, n, h->red);
+    k_fill_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dt, n, h->red, h->prm.global_dt_factor);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "global dt");
+  }
+  return AFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int afr_version(void) { return AFR_VERSION; }
+
+const char* afr_status_string(int s) {
+  switch (s) {
+    case AFR_OK: return "ok";
+    case AFR_EINVAL: return "invalid argument";
+    case AFR_ENOMEM: return "out of device memory";
+    case AFR_ECUDA: return "CUDA error";
+    case AFR_ENONFINITE: return "non-finite value";
+    case AFR_EUNSUPPORTED: return "unsupported";
+    case AFR_EINDEX: return "index out of range";
+  }
+  return "unknown status";
+}
+
+const char* afr_last_error(const afr_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int afr_device_bytes(const afr_handle* h, uint64_t* out) {
+  if (!h || !out) return AFR_EINVAL;
+  *out = h->bytes;
+  return AFR_OK;
+}
+
+int afr_destroy(afr_handle* h) {
+  if (!h) return AFR_EINVAL;
+  for (void* p : h->allocs) cudaFree(p);
+  delete h;
+  return AFR_OK;
+}
+
+int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_handle** out) {
+  if (!m || !prm || !out) return AFR_EINVAL;
+  *out = nullptr;
+  afr_handle* h = new afr_handle();
+  auto bail = [&](int rc) {
+    std::string e = h->err;
+    afr_destroy(h);
+    (void)e;
+    return rc;
+  };
+  cudaStream_t st = (cudaStream_t)stream;
+  h->N = m->n_cells;
+  h->n_prism = m->n_prism;
+  h->order = m->order;
+  h->S = m->n_sps;
+  h->Fn = m->n_fine;
+  h->P = m->n_fp;
+  h->F = m->n_faces;
+  h->prm = *prm;
+  h->nv = prm->n_vars;
+  const int n1d = h->order + 1;
+  if (h->order < 1 || h->order > 3) return bail(fail(h, AFR_EUNSUPPORTED, "order must be 1, 2 or 3"));
+  const int fine_1d = std::min(2 * h->order, 3) + 1;
+  if (h->S != n1d * n1d * n1d || h->P != n1d * n1d || h->Fn != fine_1d * fine_1d * fine_1d)
+    return bail(fail(h, AFR_EINVAL, "n_sps/n_fp/n_fine inconsistent with order"));
+  if (h->nv != 5 && h->nv != 7) return bail(fail(h, AFR_EINVAL, "n_vars must be 5 or 7"));
+  if (prm->turb == AFR_TURB_SST && (h->nv != 7 || !m->wall_distance))
+    return bail(fail(h, AFR_EINVAL, "SST needs n_vars=7 and a wall distance field"));
+  if (h->N <= 0 || h->n_prism < 0 || h->n_prism > h->N || h->F <= 0) return bail(fail(h, AFR_EINVAL, "bad sizes"));
+  const size_t N = h->N, S = h->S, Fn = h->Fn, P = h->P, F = h->F;
+  int rc;
+  std::vector<int32_t> tmp;
+
+  // ---- validate face tables on the host (all indices in range) ----
+  for (size_t f = 0; f < F; ++f) {
+    const int64_t o = m->owner_cell[f], nb = m->neighbor_cell[f];
+    const bool bnd = m->is_boundary[f] != 0;
+    if (o < 0 || o >= (int64_t)N || nb < -1 || nb >= (int64_t)N || (!bnd && nb < 0))
+      return bail(fail(h, AFR_EINDEX, "face cell index out of range at face " + std::to_string(f)));
+    if (m->owner_axis[f] < 0 || m->owner_axis[f] > 2 || (!bnd && (m->neighbor_axis[f] < 0 || m->neighbor_axis[f] > 2)))
+      return bail(fail(h, AFR_EINDEX, "face axis out of range at face " + std::to_string(f)));
+    for (int which = 0; which < 2; ++which) {
+      const int64_t c0 = which ? m->ow_src0_cell[f] : m->nb_src0_cell[f];
+      const int64_t i1 = which ? m->ow_src1_idx[f] : m->nb_src1_idx[f];
+      const int64_t n1 = which ? m->n_ow_src1 : m->n_nb_src1;
+      if (c0 < -1 || c0 >= (int64_t)N || i1 < -1 || i1 >= n1)
+        return bail(fail(h, AFR_EINDEX, "face source index out of range at face " + std::to_string(f)));
+      if (i1 >= 0) {
+        const int64_t c1 = which ? m->ow_src1_cell[i1] : m->nb_src1_cell[i1];
+        if (c1 < 0 || c1 >= (int64_t)N) return bail(fail(h, AFR_EINDEX, "second source cell out of range"));
+      }
+    }
+    if (m->bc_group[f] < 0 || m->bc_group[f] >= m->n_bc) return bail(fail(h, AFR_EINDEX, "bc_group out of range"));
+    if (m->colors[f] < 0) return bail(fail(h, AFR_EINVAL, "negative face color"));
+  }
+  for (int i = 0; i < 3 * (int)S; ++i)
+    if (m->dist_fp_of_sp[i] < 0 || m->dist_fp_of_sp[i] >= (int64_t)P || m->dist_axis_coord_of_sp[i] < 0 ||
+        m->dist_axis_coord_of_sp[i] >= n1d)
+      return bail(fail(h, AFR_EINDEX, "distribution map out of range"));
+
+  if ((rc = dalloc(h, &h->status, 1))) return bail(rc);
+  cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+
+  // ---- geometry ----
+  double *det = nullptr, *inv = nullptr, *detf = nullptr, *invf = nullptr;
+  if ((rc = upload(h, &det, m->det_jacs, N * S, st))) return bail(rc);
+  if ((rc = upload(h, &inv, m->inv_jacs, N * S * 9, st))) return bail(rc);
+  double *adj, *adjf, *vol, *mfs, *wd = nullptr;
+  if ((rc = dalloc(h, &adj, N * S * 9))) return bail(rc);
+  if ((rc = dalloc(h, &adjf, N * Fn * 9))) return bail(rc);
+  if ((rc = dalloc(h, &mfs, N * S))) return bail(rc);
+  if ((rc = upload(h, &vol, m->cell_volumes, N, st))) return bail(rc);
+  if (m->wall_distance && (rc = upload(h, &wd, m->wall_distance, N * S, st))) return bail(rc);
+  {
+    // fine-point Jacobians are only needed to form adj_fine: stage them through
+    // a temporary allocation released right after
+    cudaError_t e1 = cudaMalloc((void**)&detf, N * Fn * sizeof(double));
+    cudaError_t e2 = cudaMalloc((void**)&invf, N * Fn * 9 * sizeof(double));
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      cudaFree(detf);
+      cudaFree(invf);
+      return bail(fail(h, AFR_ENOMEM, "cudaMalloc failed for fine Jacobians"));
+    }
+    cudaMemcpyAsync(detf, m->det_jacs_fine, N * Fn * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(invf, m->inv_jacs_fine, N * Fn * 9 * sizeof(double), cudaMemcpyHostToDevice, st);
+    const size_t nf = N * Fn * 9, nc = N * S * 9;
+    k_form_adj<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(detf, invf, adjf, N * Fn);
+    k_form_adj<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(det, inv, adj, N * S);
+    k_metric_flux_scale<<<(unsigned)((N * S + 255) / 256), 256, 0, st>>>(adj, mfs, N * S);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(detf);
+    cudaFree(invf);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "geometry set-up"));
+  }
+  h->g = Geom{h->N, h->n_prism, det, inv, adj, adjf, vol, mfs, wd};
+
+  // ---- operators ----
+  for (int t = 0; t < 2; ++t) {
+    const bool present = t == 0 ? h->n_prism > 0 : h->N > h->n_prism;
+    if (!present) continue;
+    if (!m->D_3d[t] || !m->c2f[t] || !m->D_fine[t] || !m->f2c[t] || !m->filter[t])
+      return bail(fail(h, AFR_EINVAL, "missing operator for a present cell type"));
+    double *d3, *d3g, *c2f, *dfn, *f2c, *flt;
+    if ((rc = upload(h, &d3, m->D_3d[t], S * S * 3, st))) return bail(rc);
+    std::vector<double> g2(3 * S * S);
+    for (size_t s = 0; s < S; ++s)
+      for (int mm = 0; mm < 3; ++mm)
+        for (size_t j = 0; j < S; ++j) g2[(s * 3 + mm) * S + j] = m->D_3d[t][s * 3 * S + j * 3 + mm];
+    if ((rc = upload(h, &d3g, g2.data(), g2.size(), st))) return bail(rc);
+    cudaStreamSynchronize(st);
+    if ((rc = upload(h, &c2f, m->c2f[t], Fn * S, st))) return bail(rc);
+    if ((rc = upload(h, &dfn, m->D_fine[t], Fn * Fn * 3, st))) return bail(rc);
+    if ((rc = upload(h, &f2c, m->f2c[t], S * Fn, st))) return bail(rc);
+    if ((rc = upload(h, &flt, m->filter[t], S * S, st))) return bail(rc);
+    h->ops.D3[t] = d3;
+    h->ops.D3g[t] = d3g;
+    h->ops.c2f[t] = c2f;
+    h->ops.Dfine[t] = dfn;
+    h->ops.f2c[t] = f2c;
+    h->ops.filt[t] = flt;
+  }
+  {
+    double *ex, *gl, *gr;
+    int32_t *dfp, *dco;
+    if ((rc = upload(h, &ex, m->boundary_extrap, 12 * P * S, st))) return bail(rc);
+    if ((rc = upload(h, &gl, m->g_left, (size_t)n1d, st))) return bail(rc);
+    if ((rc = upload(h, &gr, m->g_right, (size_t)n1d, st))) return bail(rc);
+    if ((rc = upload_i32(h, &dfp, m->dist_fp_of_sp, 3 * S, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &dco, m->dist_axis_coord_of_sp, 3 * S, st, tmp))) return bail(rc);
+    h->ops.extrap = ex;
+    h->ops.g_left = gl;
+    h->ops.g_right = gr;
+    h->ops.dist_fp = dfp;
+    h->ops.dist_co = dco;
+  }
+
+  // ---- faces ----
+  Faces& fc = h->fc;
+  fc.F = h->F;
+  {
+    int32_t *own, *nbr, *c0n, *i1n, *c1n, *c0o, *i1o, *c1o, *bcg;
+    int8_t *oax, *nax;
+    uint8_t* isb;
+    double *osd, *nsd, *tn, *m0n, *m1n, *m0o, *m1o;
+    if ((rc = upload_i32(h, &own, m->owner_cell, F, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &nbr, m->neighbor_cell, F, st, tmp))) return bail(rc);
+    std::vector<int8_t> ax8(F);
+    for (size_t f = 0; f < F; ++f) ax8[f] = (int8_t)m->owner_axis[f];
+    if ((rc = upload(h, &oax, ax8.data(), F, st))) return bail(rc);
+    cudaStreamSynchronize(st);
+    for (size_t f = 0; f < F; ++f) ax8[f] = (int8_t)std::max<int64_t>(m->neighbor_axis[f], 0);
+    if ((rc = upload(h, &nax, ax8.data(), F, st))) return bail(rc);
+    cudaStreamSynchronize(st);
+    if ((rc = upload(h, &osd, m->owner_side, F, st))) return bail(rc);
+    if ((rc = upload(h, &nsd, m->neighbor_side, F, st))) return bail(rc);
+    if ((rc = upload(h, &isb, m->is_boundary, F, st))) return bail(rc);
+    if ((rc = upload(h, &tn, m->true_normal, F * P * 3, st))) return bail(rc);
+    if ((rc = upload_i32(h, &c0n, m->nb_src0_cell, F, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &i1n, m->nb_src1_idx, F, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &c1n, m->nb_src1_cell, (size_t)m->n_nb_src1, st, tmp))) return bail(rc);
+    if ((rc = upload(h, &m0n, m->nb_src0_mat, F * P * S, st))) return bail(rc);
+    if ((rc = upload(h, &m1n, m->nb_src1_mat, (size_t)m->n_nb_src1 * P * S, st))) return bail(rc);
+    if ((rc = upload_i32(h, &c0o, m->ow_src0_cell, F, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &i1o, m->ow_src1_idx, F, st, tmp))) return bail(rc);
+    if ((rc = upload_i32(h, &c1o, m->ow_src1_cell, (size_t)m->n_ow_src1, st, tmp))) return bail(rc);
+    if ((rc = upload(h, &m0o, m->ow_src0_mat, F * P * S, st))) return bail(rc);
+    if ((rc = upload(h, &m1o, m->ow_src1_mat, (size_t)m->n_ow_src1 * P * S, st))) return bail(rc);
+    if ((rc = upload(h, &bcg, m->bc_group, F, st))) return bail(rc);
+    fc.owner = own; fc.neighbor = nbr; fc.o_axis = oax; fc.n_axis = nax; fc.o_side = osd; fc.n_side = nsd;
+    fc.is_bnd = isb; fc.tnormal = tn; fc.nb_c0 = c0n; fc.nb_m0 = m0n; fc.nb_i1 = i1n; fc.nb_c1 = c1n; fc.nb_m1 = m1n;
+    fc.ow_c0 = c0o; fc.ow_m0 = m0o; fc.ow_i1 = i1o; fc.ow_c1 = c1o; fc.ow_m1 = m1o; fc.bc_group = bcg;
+  }
+  // slot lists: faces visited in ascending (color, face index)
+  {
+    std::vector<int32_t> order(F);
+    for (size_t f = 0; f < F; ++f) order[f] = (int32_t)f;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return m->colors[a] < m->colors[b]; });
+    auto build = [&](bool transport, int32_t** dptr, int32_t** dslot) -> int {
+      std::vector<int32_t> cnt(N + 1, 0);
+      auto visit = [&](auto&& emit) {
+        for (int32_t f : order) {
+          const bool bnd = m->is_boundary[f] != 0;
+          if (transport) {
+            emit((int32_t)m->owner_cell[f], f * 2);
+            if (m->neighbor_cell[f] >= 0) emit((int32_t)m->neighbor_cell[f], f * 2 + 1);
+          } else {
+            if (m->owner_is_primary[f]) emit((int32_t)m->owner_cell[f], f * 2);
+            if (!bnd && m->neighbor_is_primary[f]) emit((int32_t)m->neighbor_cell[f], f * 2 + 1);
+          }
+        }
+      };
+      visit([&](int32_t c, int32_t) { cnt[c + 1]++; });
+      for (size_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
+      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1), slots(cnt[N]);
+      visit([&](int32_t c, int32_t code) { slots[pos[c]++] = code; });
+      int r = upload(h, dptr, cnt.data(), N + 1, st);
+      if (r) return r;
+      r = upload(h, dslot, slots.data(), slots.size(), st);
+      if (r) return r;
+      return cudaStreamSynchronize(st) == cudaSuccess ? AFR_OK : AFR_ECUDA;
+    };
+    int32_t *sp, *sl, *tp, *tl;
+    if ((rc = build(false, &sp, &sl))) return bail(rc);
+    if ((rc = build(true, &tp, &tl))) return bail(rc);
+    fc.slot_ptr = sp; fc.slot = sl; fc.tslot_ptr = tp; fc.tslot = tl;
+  }
+  // ---- boundary condition table ----
+  {
+    int32_t *bt, *bn;
+    double *bw, *bq, *bp;
+    const size_t nb = (size_t)m->n_bc;
+    if ((rc = upload(h, &bt, m->bc_type, nb, st))) return bail(rc);
+    if ((rc = upload(h, &bn, m->bc_noslip, nb, st))) return bail(rc);
+    if ((rc = upload(h, &bw, m->bc_wall_vel, nb * 3, st))) return bail(rc);
+    if ((rc = upload(h, &bq, m->bc_Q, nb * 5, st))) return bail(rc);
+    if ((rc = upload(h, &bp, m->bc_p_out, nb, st))) return bail(rc);
+    h->bc = Bc{m->n_bc, bt, bn, bw, bq, bp};
+    std::vector<uint8_t> wall(F);
+    for (size_t f = 0; f < F; ++f) wall[f] = (m->is_boundary[f] && m->bc_type[m->bc_group[f]] == AFR_BC_WALL) ? 1 : 0;
+    if ((rc = upload(h, &h->wall_face, wall.data(), F, st))) return bail(rc);
+    cudaStreamSynchronize(st);
+  }
+  if (m->cd_wall_face && m->true_area_weight) {
+    std::vector<int32_t> cdf;
+    for (size_t f = 0; f < F; ++f)
+      if (m->cd_wall_face[f] && m->owner_is_primary[f]) cdf.push_back((int32_t)f);
+    h->n_cd_faces = (int)cdf.size();
+    if ((rc = upload(h, &h->cd_faces, cdf.data(), cdf.size(), st))) return bail(rc);
+    if ((rc = upload(h, &h->area_w, m->true_area_weight, F * P, st))) return bail(rc);
+    if ((rc = dalloc(h, &h->cd_part, cdf.size() * 6))) return bail(rc);
+    cudaStreamSynchronize(st);
+  }
+  // ---- scratch ----
+  if ((rc = dalloc(h, &h->grads, N * S * 12))) return bail(rc);
+  if ((rc = dalloc(h, &h->Ua, N * S * h->nv))) return bail(rc);
+  if ((rc = dalloc(h, &h->Ub, N * S * h->nv))) return bail(rc);
+  if ((rc = dalloc(h, &h->dt, N * S))) return bail(rc);
+  if ((rc = dalloc(h, &h->norm_part, N))) return bail(rc);
+  if ((rc = dalloc(h, &h->red, 4))) return bail(rc);
+  if (prm->turb == AFR_TURB_SST) {
+    if ((rc = dalloc(h, &h->pt, N * S * 5))) return bail(rc);
+    if ((rc = dalloc(h, &h->cfp, F * P * 4))) return bail(rc);
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "afr_create"));
+  *out = h;
+  return AFR_OK;
+}
+
+int afr_inviscid_residual(afr_handle* h, const double* U, double* R, void* stream) {
+  if (!h || !U || !R) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  StageArgs a = base_args(h);
+  a.Ucur = U;
+  a.inviscid_only = 1;
+  a.stage = -1;
+  a.Rinv = R;
+  cudaError_t e = dispatch(h, [&](auto L) { return L.stage(h, a, st); });
+  if (e != cudaSuccess) return cuda_fail(h, e, "inviscid residual");
+  return check_status(h, st);
+}
+
+int afr_viscous_residual(afr_handle* h, const double* U, const double* nu_t, double* R, void* stream) {
+  if (!h || !U || !R) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  StageArgs a = base_args(h);
+  a.Ucur = U;
+  a.inviscid_only = 0;
+  a.stage = -1;
+  a.nut = nu_t;
+  a.Rvisc = R;
+  cudaError_t e = dispatch(h, [&](auto L) {
+    cudaError_t r = L.grad(h, U, st);
+    return r != cudaSuccess ? r : L.stage(h, a, st);
+  });
+  if (e != cudaSuccess) return cuda_fail(h, e, "viscous residual");
+  return check_status(h, st);
+}
+
+int afr_local_dt(afr_handle* h, const double* U, const double* nu_t, double* dt, void* stream) {
+  if (!h || !U || !dt) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = compute_dt(h, U, nu_t, dt, st);
+  return rc ? rc : check_status(h, st);
+}
+
+int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, double* k, double* omega, double* nu_t,
+                   double* diag, void* stream) {
+  if (!h || !U || !dt_local || !k || !omega || !nu_t) return AFR_EINVAL;
+  if (h->prm.turb != AFR_TURB_SST) return fail(h, AFR_EINVAL, "handle was created without SST");
+  cudaStream_t st = (cudaStream_t)stream;
+  SstArgs s{U, dt_local, k, omega, nu_t, h->pt, h->cfp, h->wall_face, diag, h->nv, h->prm.mu};
+  cudaError_t e = dispatch(h, [&](auto L) { return L.sst(h, s, st); });
+  if (e != cudaSuccess) return cuda_fail(h, e, "sst update");
+  return check_status(h, st);
+}
+
+int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
+  if (!h || !U) return AFR_EINVAL;
+  const bool sst = h->prm.turb == AFR_TURB_SST;
+  if (sst && (!k || !omega || !nu_t)) return fail(h, AFR_EINVAL, "SST step needs k, omega and nu_t");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = compute_dt(h, U, sst ? nu_t : nullptr, h->dt, st);
+  if (rc) return rc;
+  const bool visc = !h->prm.inviscid_only;
+  cudaError_t e = dispatch(h, [&](auto L) {
+    cudaError_t r = cudaSuccess;
+    if (sst) {
+      SstArgs s{U, h->dt, k, omega, nu_t, h->pt, h->cfp, h->wall_face, nullptr, h->nv, h->prm.mu};
+      r = L.sst(h, s, st);
+      if (r != cudaSuccess) return r;
+    }
+    const double* cur[3] = {U, h->Ua, h->Ub};
+    double* nxt[3] = {h->Ua, h->Ub, U};
+    for (int stg = 0; stg < 3; ++stg) {
+      if (visc) {
+        r = L.grad(h, cur[stg], st);
+        if (r != cudaSuccess) return r;
+      }
+      StageArgs a = base_args(h);
+      a.Ucur = cur[stg];
+      a.U0 = U;
+      a.Unext = nxt[stg];
+      a.nut = sst ? nu_t : nullptr;
+      a.dt = h->dt;
+      a.norm_part = h->norm_part;
+      a.stage = stg;
+      r = L.stage(h, a, st);
+      if (r != cudaSuccess) return r;
+    }
+    return r;
+  });
+  if (e != cudaSuccess) return cuda_fail(h, e, "step");
+  k_reduce_sum<<<1, 1024, 0, st>>>(h->norm_part, (size_t)h->N, h->red);
+  if (norm_out) {
+    double ss = 0.0;
+    e = cudaMemcpyAsync(&ss, h->red, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(h, e, "norm read");
+    *norm_out = std::sqrt(ss) / std::sqrt((double)h->N * h->S * h->nv);
+    return check_status(h, st);
+  }
+  return AFR_OK;
+}
+
+int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3, void* stream) {
+  if (!h || !U || !out3) return AFR_EINVAL;
+  if (!h->cd_faces) return fail(h, AFR_EINVAL, "handle was created without wall-face force tables");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = dispatch(h, [&](auto L) {
+    cudaError_t r = L.grad(h, U, st);
+    return r != cudaSuccess ? r : L.force(h, U, nu_t, st);
+  });
+  if (e != cudaSuccess) return cuda_fail(h, e, "force");
+  std::vector<double> part((size_t)h->n_cd_faces * 6);
+  e = cudaMemcpyAsync(part.data(), h->cd_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "force read");
+  double Fp[3] = {0, 0, 0}, Fv[3] = {0, 0, 0};
+  for (int i = 0; i < h->n_cd_faces; ++i)
+    for (int d = 0; d < 3; ++d) {
+      Fp[d] += part[i * 6 + d];
+      Fv[d] += -part[i * 6 + 3 + d];
+    }
+  const double q = 0.5 * h->prm.rho_inf * h->prm.vel_inf * h->prm.vel_inf;
+  const double den = std::max(q * reference_area, 1e-300);
+  out3[0] = (Fp[0] + Fv[0]) / den;
+  out3[1] = (Fp[2] + Fv[2]) / den;
+  out3[2] = (Fp[1] + Fv[1]) / den;
+  return AFR_OK;
+}
+
+}  // extern "C"

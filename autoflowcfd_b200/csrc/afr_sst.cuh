@@ -1,0 +1,383 @@
+// SST k-omega source, transport and point-implicit update, and the local time
+// step.  Restates (paths relative to the reference's src/autoflowcfd):
+//   compute_turbulence_source          core/fr_solver/turbulence.py:178-330
+//   SSTModelFR.compute_source_terms    core/turbulence/sst.py:241-354
+//   SSTModelFR.update_fields           core/turbulence/sst.py:382-479
+//   compute_turbulence_transport_residual core/turbulence/transport.py:367-522
+//   transport face kernels             core/turbulence/transport_kernel.py:25-327
+//   compute_local_time_step            core/fr_solver/cfl.py:12-147
+#pragma once
+#include "afr_kernels.cuh"
+
+namespace afr {
+
+struct SstArgs {
+  const double* U;      // (N,S,nv) step-start state
+  const double* dt;     // (N,S)
+  double* k;            // (N,S) in/out
+  double* w;            // (N,S) in/out
+  double* nut;          // (N,S) in/out (kinematic eddy viscosity)
+  double* pt;           // (N,S,5) scratch: Sk, Sw, beta_blend, gamma_k, gamma_w
+  double* cfp;          // (F,P,4) scratch: conv_k, diff_k, conv_w, diff_w face corrections
+  const uint8_t* wall_face;  // (F) WALL boundary faces (k Dirichlet-zero ghost)
+  double* dbg;          // optional (N,S,4): Sk, Sw, transport_k, transport_w
+  int nv;
+  double mu;            // molecular viscosity of the mean flow
+};
+
+constexpr double SST_SK1 = 0.85, SST_SK2 = 1.0, SST_SW1 = 0.5, SST_SW2 = 0.856;
+constexpr double SST_B1 = 0.075, SST_B2 = 0.0828, SST_A1 = 0.31, SST_KAPPA = 0.41, SST_BSTAR = 0.09;
+constexpr double SST_TVR = 1.0e5;
+constexpr double MU_SOURCE = 1.8e-5;  // hard-coded in core/fr_solver/turbulence.py:230
+
+__device__ __forceinline__ double dfinite(double x) { return isfinite(x) ? x : 0.0; }
+
+__device__ __forceinline__ double sst_F1(double k, double w, double d, double nu, double rho, double CD) {
+  w = fmax(w, 1e-10);
+  k = fmax(k, 1e-10);
+  d = fmax(d, 1e-10);
+  const double sk = sqrt(k);
+  const double t1 = sk / (SST_BSTAR * w * d);
+  const double t2 = 500.0 * nu / (d * d * w);
+  const double t3 = 4.0 * rho * SST_SW2 * k / (fmax(CD, 1e-10) * (d * d));
+  double a = fmin(fmax(t1, t2), t3);
+  if (!isfinite(a)) a = 1e75;
+  a = fmin(a, 1e75);
+  return tanh(pow(a, 4.0));
+}
+
+__device__ __forceinline__ double sst_F2(double k, double w, double d, double nu) {
+  w = fmax(w, 1e-10);
+  k = fmax(k, 1e-10);
+  d = fmax(d, 1e-10);
+  const double sk = sqrt(k);
+  double a = fmax(2.0 * sk / (SST_BSTAR * w * d), 500.0 * nu / (d * d * w));
+  if (!isfinite(a)) a = 1e150;
+  a = fmin(a, 1e150);
+  return tanh(a * a);
+}
+
+// per cell: gradients of (rho u, rho v, rho w, k, omega), pointwise SST terms
+template <int S>
+__global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a) {
+  __shared__ double f[S * 5];
+  __shared__ double gc[S * 3 * 5];
+  const int e = blockIdx.x;
+  const int ct = cell_type(g, e);
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const double* u = a.U + ((size_t)e * S + s) * a.nv;
+    f[s * 5 + 0] = u[1];
+    f[s * 5 + 1] = u[2];
+    f[s * 5 + 2] = u[3];
+    f[s * 5 + 3] = a.k[(size_t)e * S + s];
+    f[s * 5 + 4] = a.w[(size_t)e * S + s];
+  }
+  __syncthreads();
+  block_gemm<S * 3, 5, S>(gc, 5, ops.D3g[ct], S, f, 5);
+  __syncthreads();
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const size_t p = (size_t)e * S + s;
+    const double* inv = g.inv + p * 9;
+    double gp[5][3];
+    for (int q = 0; q < 5; ++q)
+      for (int n = 0; n < 3; ++n) {
+        double acc = 0.0;
+        for (int m = 0; m < 3; ++m) acc += gc[(s * 3 + m) * 5 + q] * inv[m * 3 + n];
+        gp[q][n] = acc;
+      }
+    // |grad| <= 1e6 clip of grad k, grad omega
+    for (int q = 3; q < 5; ++q) {
+      const double mag = sqrt(gp[q][0] * gp[q][0] + gp[q][1] * gp[q][1] + gp[q][2] * gp[q][2]);
+      if (mag > 1e6) {
+        double sc = 1e6 / fmax(mag, 1e-10);
+        sc = fmin(fmax(sc, 0.0), 1.0);
+        for (int n = 0; n < 3; ++n) gp[q][n] *= sc;
+      }
+    }
+    const double* u = a.U + p * a.nv;
+    const double rho = fmax(u[0], 1e-10);
+    const double kf = a.k[p], wf = a.w[p];
+    const double d = g.wall_dist[p];
+    // strain magnitude of the conserved-momentum gradient
+    double ss = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const double sij = 0.5 * (gp[i][j] + gp[j][i]);
+        ss += sij * sij;
+      }
+    const double Sm = sqrt(2.0 * ss);
+    const double gd = gp[3][0] * gp[4][0] + gp[3][1] * gp[4][1] + gp[3][2] * gp[4][2];
+    // --- compute_source_terms ---
+    const double nu = MU_SOURCE / fmax(rho, 1e-10);
+    const double k_s = fmin(kf, 1e40);
+    const double w_s = fmax(fmin(wf, 1e40), 1e-10);
+    const double CD = fmax(2.0 * rho * SST_SW2 / w_s * gd, 1e-10);
+    const double F1 = sst_F1(k_s, w_s, d, nu, rho, CD);
+    const double F2 = sst_F2(k_s, w_s, d, nu);
+    const double beta = F1 * SST_B1 + (1.0 - F1) * SST_B2;
+    double nut = SST_A1 * fmax(k_s, 1e-10) / fmax(SST_A1 * fmax(w_s, 1e-10), F2 * fmax(Sm, 1e-10));
+    nut = fmin(nut, SST_TVR * MU_SOURCE / fmax(rho, 1e-10));
+    if (!isfinite(nut)) nut = 0.0;
+    double Pk = nut * rho * (Sm * Sm);
+    Pk = fmin(Pk, 10.0 * SST_BSTAR * rho * k_s * w_s);
+    const double Dk = rho * SST_BSTAR * k_s * w_s;
+    const double g1 = SST_B1 / SST_BSTAR - SST_SW1 * SST_KAPPA * SST_KAPPA / sqrt(SST_BSTAR);
+    const double g2 = SST_B2 / SST_BSTAR - SST_SW2 * SST_KAPPA * SST_KAPPA / sqrt(SST_BSTAR);
+    const double gam = F1 * g1 + (1.0 - F1) * g2;
+    const double Pw = rho * gam * (Sm * Sm);
+    const double Dw = rho * beta * (w_s * w_s);
+    const double CDw = 2.0 * rho * (1.0 - F1) * SST_SW2 / w_s * gd;
+    const double Sk = dfinite(Pk - Dk);
+    const double Sw = dfinite(Pw - Dw + CDw);
+    // --- transport diffusion coefficients (mu = molecular viscosity of the mean flow) ---
+    const double nu_m = a.mu / fmax(rho, 1e-10);
+    const double CD2 = fmax(2.0 * rho * SST_SW2 / fmax(wf, 1e-10) * gd, 1e-10);
+    const double F1t = sst_F1(kf, wf, d, nu_m, rho, CD2);
+    const double sk = F1t * SST_SK1 + (1.0 - F1t) * SST_SK2;
+    const double sw = F1t * SST_SW1 + (1.0 - F1t) * SST_SW2;
+    const double rnut = rho * nut;
+    a.nut[p] = nut;
+    double* o = a.pt + p * 5;
+    o[0] = Sk;
+    o[1] = Sw;
+    o[2] = beta;
+    o[3] = a.mu + sk * rnut;
+    o[4] = a.mu + sw * rnut;
+  }
+}
+
+// per face flux point: upwind convection and BR1-style diffusion corrections
+template <int S, int NP>
+__global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= fc.F * NP) return;
+  const int f = t / NP, i = t % NP;
+  const int oc = fc.owner[f];
+  const int ct = cell_type(g, oc);
+  const int ax = fc.o_axis[f];
+  const double* E = ops.extrap + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * NP * S + i * S;
+  // owner side: rho, rho u (3), k, w, gamma_k, gamma_w
+  double po[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int s = 0; s < S; ++s) {
+    const size_t p = (size_t)oc * S + s;
+    const double* u = a.U + p * a.nv;
+    const double rho = fmax(u[0], 1e-10);
+    const double we = __ldg(E + s);
+    po[0] += we * rho;
+    po[1] += we * (u[1] / rho);
+    po[2] += we * (u[2] / rho);
+    po[3] += we * (u[3] / rho);
+    po[4] += we * a.k[p];
+    po[5] += we * a.w[p];
+    po[6] += we * a.pt[p * 5 + 3];
+    po[7] += we * a.pt[p * 5 + 4];
+  }
+  // neighbour side: k, w, gamma_k, gamma_w
+  double pn[4];
+  const int c0 = fc.nb_c0[f], i1 = fc.nb_i1[f];
+  if (c0 < 0 && i1 < 0) {
+    const bool wz = a.wall_face[f] != 0;
+    pn[0] = wz ? -po[4] : po[4];
+    pn[1] = po[5];
+    pn[2] = po[6];
+    pn[3] = po[7];
+  } else {
+    for (int q = 0; q < 4; ++q) pn[q] = 0.0;
+    if (c0 >= 0) {
+      const double* M = fc.nb_m0 + ((size_t)f * NP + i) * S;
+      for (int q = 0; q < 4; ++q) {
+        double acc = 0.0;
+        for (int s = 0; s < S; ++s) {
+          const size_t p = (size_t)c0 * S + s;
+          const double x = q == 0 ? a.k[p] : q == 1 ? a.w[p] : a.pt[p * 5 + 1 + q];
+          acc += __ldg(M + s) * x;
+        }
+        pn[q] = acc;
+      }
+    }
+    if (i1 >= 0) {
+      const int c1 = fc.nb_c1[i1];
+      const double* M = fc.nb_m1 + ((size_t)i1 * NP + i) * S;
+      for (int q = 0; q < 4; ++q) {
+        double acc = 0.0;
+        for (int s = 0; s < S; ++s) {
+          const size_t p = (size_t)c1 * S + s;
+          const double x = q == 0 ? a.k[p] : q == 1 ? a.w[p] : a.pt[p * 5 + 1 + q];
+          acc += __ldg(M + s) * x;
+        }
+        pn[q] += acc;
+      }
+    }
+  }
+  const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
+  const double mflux = ((po[0] * po[1]) * tn[0] + (po[0] * po[2]) * tn[1]) + (po[0] * po[3]) * tn[2];
+  double* o = a.cfp + ((size_t)f * NP + i) * 4;
+  const double upk = mflux >= 0.0 ? po[4] : pn[0];
+  const double upw = mflux >= 0.0 ? po[5] : pn[1];
+  o[0] = mflux * (upk - po[4]);
+  o[1] = (0.5 * (po[6] + pn[2])) * (0.5 * (po[4] + pn[0]) - po[4]);
+  o[2] = mflux * (upw - po[5]);
+  o[3] = (0.5 * (po[7] + pn[3])) * (0.5 * (po[5] + pn[1]) - po[5]);
+}
+
+// per cell: volume transport terms, gather of the face corrections, outlier
+// suppression and the point-implicit k / omega update
+template <int S, int NP>
+__global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a) {
+  __shared__ double fl[S * 4];       // k, w, gamma_k, gamma_w
+  __shared__ double gc[S * 3 * 2];   // reference-space grads of k, w
+  __shared__ double Ft[S * 3 * 4];   // contravariant fluxes: conv k, diff k, conv w, diff w
+  __shared__ double R[S * 4];        // volume residuals
+  __shared__ double C[S * 4];        // interface corrections
+  __shared__ double T[S * 5];        // transport k, w (+ padding for the outlier helper)
+  __shared__ double Ref[S * 5];
+  __shared__ double work[24];
+  const int e = blockIdx.x;
+  const int ct = cell_type(g, e);
+  const double* det = g.det + (size_t)e * S;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const size_t p = (size_t)e * S + s;
+    fl[s * 4 + 0] = a.k[p];
+    fl[s * 4 + 1] = a.w[p];
+    fl[s * 4 + 2] = a.pt[p * 5 + 3];
+    fl[s * 4 + 3] = a.pt[p * 5 + 4];
+    for (int q = 0; q < 4; ++q) C[s * 4 + q] = 0.0;
+  }
+  __syncthreads();
+  // grad k, grad w in reference space (D3g rows s*3+m)
+  for (int t = threadIdx.x; t < S * 3 * 2; t += blockDim.x) {
+    const int r = t / 2, q = t % 2;
+    const double* Dr = ops.D3g[ct] + (size_t)r * S;
+    double acc = 0.0;
+    for (int j = 0; j < S; ++j) acc += __ldg(Dr + j) * fl[j * 4 + q];
+    gc[r * 2 + q] = acc;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const size_t p = (size_t)e * S + s;
+    const double* inv = g.inv + p * 9;
+    const double* adj = g.adj + p * 9;
+    const double* u = a.U + p * a.nv;
+    const double rho = fmax(u[0], 1e-10);
+    const double vel[3] = {u[1] / rho, u[2] / rho, u[3] / rho};
+    for (int q = 0; q < 2; ++q) {
+      double gphys[3];
+      for (int n = 0; n < 3; ++n) {
+        double acc = 0.0;
+        for (int m = 0; m < 3; ++m) acc += gc[(s * 3 + m) * 2 + q] * inv[m * 3 + n];
+        gphys[n] = acc;
+      }
+      const double phi = fl[s * 4 + q];
+      const double gam = fl[s * 4 + 2 + q];
+      double Fc[3], Fd[3];
+      for (int d = 0; d < 3; ++d) {
+        Fc[d] = (rho * vel[d]) * phi;
+        Fd[d] = gam * gphys[d];
+      }
+      for (int m = 0; m < 3; ++m) {
+        Ft[(s * 3 + m) * 4 + 2 * q] = adj[m * 3 + 0] * Fc[0] + adj[m * 3 + 1] * Fc[1] + adj[m * 3 + 2] * Fc[2];
+        Ft[(s * 3 + m) * 4 + 2 * q + 1] = adj[m * 3 + 0] * Fd[0] + adj[m * 3 + 1] * Fd[1] + adj[m * 3 + 2] * Fd[2];
+      }
+    }
+  }
+  __syncthreads();
+  // divergence: sum over m of (sum_j Ft[j,m] D[s,j,m])
+  for (int t = threadIdx.x; t < S * 4; t += blockDim.x) {
+    const int s = t / 4, q = t % 4;
+    const double* Dr = ops.D3[ct] + (size_t)s * S * 3;
+    double div = 0.0;
+    for (int m = 0; m < 3; ++m) {
+      double acc = 0.0;
+      for (int j = 0; j < S; ++j) acc += Ft[(j * 3 + m) * 4 + q] * __ldg(Dr + j * 3 + m);
+      div += acc;
+    }
+    R[t] = -div / det[s];
+  }
+  __syncthreads();
+  // face corrections in ascending color order (every face side)
+  const int b = fc.tslot_ptr[e], en = fc.tslot_ptr[e + 1];
+  for (int si = b; si < en; ++si) {
+    const int code = fc.tslot[si];
+    const int f = code >> 1;
+    const bool is_owner = (code & 1) == 0;
+    const int ax = is_owner ? fc.o_axis[f] : fc.n_axis[f];
+    const double side = is_owner ? fc.o_side[f] : fc.n_side[f];
+    const double* gp = side > 0.0 ? ops.g_right : ops.g_left;
+    for (int t = threadIdx.x; t < S * 4; t += blockDim.x) {
+      const int s = t / 4, q = t % 4;
+      const int fp = ops.dist_fp[ax * S + s];
+      const double contrib = gp[ops.dist_co[ax * S + s]] * a.cfp[((size_t)f * NP + fp) * 4 + q];
+      if (is_owner) C[t] -= contrib / det[s];
+      else C[t] += contrib / det[s];
+    }
+    __syncthreads();
+  }
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const double rho = fmax(a.U[((size_t)e * S + s) * a.nv], 1e-10);
+    const double conv_k = R[s * 4 + 0] + C[s * 4 + 0];
+    const double diff_k = R[s * 4 + 1] - C[s * 4 + 1];
+    const double conv_w = R[s * 4 + 2] + C[s * 4 + 2];
+    const double diff_w = R[s * 4 + 3] - C[s * 4 + 3];
+    T[s * 5 + 0] = (conv_k + diff_k) / fmax(rho, 1e-10);
+    T[s * 5 + 1] = (conv_w + diff_w) / fmax(rho, 1e-10);
+    T[s * 5 + 2] = 0.0; T[s * 5 + 3] = 0.0; T[s * 5 + 4] = 0.0;
+    Ref[s * 5 + 0] = fl[s * 4 + 0];
+    Ref[s * 5 + 1] = fl[s * 4 + 1];
+    Ref[s * 5 + 2] = 0.0; Ref[s * 5 + 3] = 0.0; Ref[s * 5 + 4] = 0.0;
+  }
+  __syncthreads();
+  suppress_outliers<S>(T, Ref, 5, work);
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const size_t p = (size_t)e * S + s;
+    const double rho = fmax(a.U[p * a.nv], 1e-10);
+    const double tk = dfinite(T[s * 5 + 0]);
+    const double tw = dfinite(T[s * 5 + 1]);
+    const double* pt = a.pt + p * 5;
+    const double dts = a.dt[p];
+    const double kf = fl[s * 4 + 0], wf = fl[s * 4 + 1];
+    const double wo = fmax(wf, 1e-10);
+    const double dkd = dfinite((pt[0] / fmax(rho, 1e-10)) / (1.0 + dts * (SST_BSTAR * wo)));
+    const double dwd = dfinite((pt[1] / fmax(rho, 1e-10)) / (1.0 + dts * (pt[2] * wo)));
+    const double kt = dfinite(dkd + tk);
+    const double wt = dfinite(dwd + tw);
+    double kn = kf + dts * kt;
+    double wn = wf + dts * wt;
+    if (!isfinite(kn)) kn = 1e-12;
+    if (!isfinite(wn)) wn = 1e-12;
+    a.k[p] = fmax(kn, 1e-12);
+    a.w[p] = fmax(wn, 1e-12);
+    if (a.dbg) {
+      a.dbg[p * 4 + 0] = pt[0];
+      a.dbg[p * 4 + 1] = pt[1];
+      a.dbg[p * 4 + 2] = tk;
+      a.dbg[p * 4 + 3] = tw;
+    }
+  }
+}
+
+// local time step per solution point (core/fr_solver/cfl.py:12-147)
+__global__ void k_local_dt(Geom g, int S, int order, const double* __restrict__ U, int nv,
+                           const double* __restrict__ nut, double mu, double* __restrict__ dt) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (size_t)g.N * S) return;
+  const int e = (int)(p / S);
+  const double* u = U + p * nv;
+  const double rho = fmax(u[0], 1e-10);
+  const double ux = u[1] / rho, uy = u[2] / rho, uz = u[3] / rho;
+  const double ke = 0.5 * (ux * ux + uy * uy + uz * uz);
+  const double pr = fmax((u[4] - rho * ke) * 0.4, 1.0);
+  const double a = sqrt(fmax(1.4 * pr / fmax(rho, 1e-10), 1e-10));
+  const double vm = sqrt(ux * ux + uy * uy + uz * uz);
+  const double wave = fmax(vm + a, 1e-10);
+  const double h = pow(fabs(g.volume[e]), 1.0 / 3.0);
+  const double CFL = 0.1;
+  const double fa = 1.0 / (2 * order + 1);
+  const double fv = 1.0 / ((2 * order + 1) * (2 * order + 1));
+  const double dt_adv = CFL * fa * h / wave;
+  const double mu_eff = nut ? mu + rho * nut[p] : mu;
+  const double dt_visc = 0.25 * CFL * fv * rho * (h * h) / fmax(mu_eff, 1e-30);
+  const double dt_geo = CFL * fabs(g.det[p]) / fmax(g.mfs[p] * wave, 1e-300);
+  dt[p] = fmin(fmin(dt_adv, dt_visc), dt_geo);
+}
+
+}  // namespace afr

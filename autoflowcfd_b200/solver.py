@@ -1,0 +1,221 @@
+"""Host-side mirror of the reference's residual / time-step seam on one B200.
+
+``B200FRSolver`` exposes the method surface of the reference's ``FRSolver``
+residual seam (core/fr_solver/solver.py:329-446) and of the ``--backend gpu``
+``GPUFRSolver`` (core/gpu/gpu_solver.py:36-453, core/gpu/gpu_solver_io.py:20-84)
+with the same names, argument meaning and error behaviour, but every numeric
+operation runs in ``libafr_b200.so`` on the device.  PyTorch provides device
+memory and the current CUDA stream only; there is no CPU fallback.
+
+State layouts are the reference's: U (n_cells, n_sps, n_vars) float64, k /
+omega / nu_t (n_cells, n_sps) float64.
+"""
+
+import ctypes
+from dataclasses import dataclass
+from typing import Dict, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import LIB, check
+
+GAMMA = 1.4
+
+
+def _dev_ptr(t: Optional[torch.Tensor]):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise ValueError("device arrays must be contiguous float64 CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class SolverResult:
+    """core/fr_solver/state.py:12-17."""
+
+    converged: bool
+    iterations: int
+    final_residual: float
+
+
+class B200FRSolver:
+    """One FR case resident on the GPU.
+
+    Args:
+        case: mapping with the reference's flattened mesh tables, operators and
+            boundary tables (the keys written by ``tests/golden/make_golden.py``
+            or produced by ``autoflowcfd_b200.boxgeom``).
+        turb_model_name: "SST" or "NONE" (core/fr_solver/turbulence.py:23-47).
+        mu_molecular: molecular viscosity (FRSolver ``mu_molecular``).
+        rho_inf, vel_inf, p_inf: free stream (FRSolver ctor).
+        inviscid_only: Euler runs (the viscous residual is zero).
+        global_dt_factor: > 0 selects time-accurate global stepping
+            dt = factor * min(dt_local).
+        device: CUDA device.
+    """
+
+    def __init__(self, case: Dict[str, np.ndarray], turb_model_name: str = "NONE", mu_molecular: float = 1.8e-5,
+                 rho_inf: float = 1.225, vel_inf: float = 33.33, p_inf: float = 101325.0,
+                 inviscid_only: bool = False, global_dt_factor: float = 0.0, device="cuda:0"):
+        name = turb_model_name.upper()
+        if name not in ("SST", "NONE"):
+            raise ValueError(f"Unknown turbulence model: {turb_model_name}")
+        self.device = torch.device(device)
+        self.turb_model_name = name
+        self.n_cells = int(case["n_cells"])
+        self.n_sps = int(case["n_sps"])
+        self.order = int(case["order"])
+        self.n_vars = 7 if name == "SST" else 5
+        self.mu_molecular = float(mu_molecular)
+        self.freestream = {"rho_inf": rho_inf, "vel_inf": vel_inf, "p_inf": p_inf}
+        self._tables = _lib.MeshTables(case)
+        prm = _lib.AfrParams()
+        prm.n_vars = self.n_vars
+        prm.turb = _lib.AFR_TURB_SST if name == "SST" else _lib.AFR_TURB_NONE
+        prm.inviscid_only = 1 if inviscid_only else 0
+        prm.mu, prm.rho_inf, prm.vel_inf, prm.p_inf = self.mu_molecular, rho_inf, vel_inf, p_inf
+        prm.global_dt_factor = float(global_dt_factor)
+        self._prm = prm
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(LIB.afr_create(ctypes.byref(self._tables.desc), ctypes.byref(prm), _stream(), ctypes.byref(h)))
+        self._h = h
+        N, S = self.n_cells, self.n_sps
+        self.U = torch.zeros((N, S, self.n_vars), dtype=torch.float64, device=self.device)
+        self.k = self.omega = self.nu_t = None
+        if name == "SST":
+            # SSTModelFR initial fields, core/turbulence/sst.py:46-49
+            self.k = torch.full((N, S), 1e-6, dtype=torch.float64, device=self.device)
+            self.omega = torch.ones((N, S), dtype=torch.float64, device=self.device)
+            self.nu_t = torch.zeros((N, S), dtype=torch.float64, device=self.device)
+        self.initialize_uniform(rho_inf, vel_inf, 0.0, 0.0, p_inf)
+        self.residual_history = []
+
+    # ------------------------------------------------------------------ state
+    def initialize_uniform(self, rho=1.0, u=0.0, v=0.0, w=0.0, p=1.0, k=1e-6, omega=1e-2):
+        """FRState.initialize_uniform, core/fr_solver/state.py:50-74."""
+        e = p / ((GAMMA - 1.0) * rho) + 0.5 * (u**2 + v**2 + w**2)
+        vals = [rho, rho * u, rho * v, rho * w, rho * e]
+        if self.n_vars > 5:
+            vals += [rho * k, rho * omega]
+        self.U[...] = torch.tensor(vals, dtype=torch.float64, device=self.device)
+
+    def set_state_from_cpu(self, U: np.ndarray):
+        """GPUFRSolver.set_state_from_cpu (core/gpu/gpu_solver_io.py:20-35)."""
+        U = np.asarray(U, dtype=np.float64)
+        if U.shape != tuple(self.U.shape):
+            raise ValueError(f"state shape {U.shape} != {tuple(self.U.shape)}")
+        self.U.copy_(torch.from_numpy(np.ascontiguousarray(U)))
+
+    def get_state_cpu(self) -> np.ndarray:
+        return self.U.cpu().numpy()
+
+    def set_turbulence(self, k: np.ndarray, omega: np.ndarray, nu_t: np.ndarray):
+        if self.k is None:
+            raise ValueError("solver was built without SST")
+        for dst, src in ((self.k, k), (self.omega, omega), (self.nu_t, nu_t)):
+            dst.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=np.float64)))
+
+    # -------------------------------------------------------------- residuals
+    def compute_inviscid_residual(self, U_trial: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """FRSolver.compute_inviscid_residual (core/fr_solver/solver.py:351-400)."""
+        U = self.U if U_trial is None else U_trial
+        R = torch.empty_like(U)
+        check(LIB.afr_inviscid_residual(self._h, _dev_ptr(U), _dev_ptr(R), _stream()), self._h)
+        return R
+
+    def compute_viscous_residual(self, U_trial: Optional[torch.Tensor] = None,
+                                 mu_t_field: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """FRSolver.compute_viscous_residual (core/fr_solver/solver.py:402-432).
+
+        ``mu_t_field`` here is the kinematic eddy viscosity nu_t; the library
+        forms mu_t = max(rho, 1e-10) * nu_t as the reference does."""
+        U = self.U if U_trial is None else U_trial
+        nut = self.nu_t if mu_t_field is None else mu_t_field
+        R = torch.empty_like(U)
+        check(LIB.afr_viscous_residual(self._h, _dev_ptr(U), _dev_ptr(nut), _dev_ptr(R), _stream()), self._h)
+        return R
+
+    # GPUFRSolver spellings
+    compute_inviscid_residual_gpu = compute_inviscid_residual
+    compute_viscous_residual_gpu = compute_viscous_residual
+
+    def _compute_local_time_step(self) -> torch.Tensor:
+        """core/fr_solver/cfl.py:12-147 (global min when global_dt_factor > 0)."""
+        dt = torch.empty((self.n_cells, self.n_sps), dtype=torch.float64, device=self.device)
+        check(LIB.afr_local_dt(self._h, _dev_ptr(self.U), _dev_ptr(self.nu_t), _dev_ptr(dt), _stream()), self._h)
+        return dt
+
+    def compute_turbulence_source(self, dt_local: torch.Tensor, diag: bool = False):
+        """core/fr_solver/turbulence.py:178-330: updates k, omega, nu_t in place;
+        returns (Sk, S_omega, transport_k, transport_omega) when ``diag``."""
+        if self.k is None:
+            return None
+        d = torch.empty((self.n_cells, self.n_sps, 4), dtype=torch.float64, device=self.device) if diag else None
+        check(LIB.afr_sst_update(self._h, _dev_ptr(self.U), _dev_ptr(dt_local), _dev_ptr(self.k),
+                                 _dev_ptr(self.omega), _dev_ptr(self.nu_t), _dev_ptr(d), _stream()), self._h)
+        if diag:
+            return d[..., 0], d[..., 1], d[..., 2], d[..., 3]
+        return None
+
+    # ------------------------------------------------------------------- step
+    def step(self, dt: float = 1e-3, want_norm: bool = True) -> float:
+        """FRSolver.step / GPUFRSolver.step: one SSP-RK3 step with local time
+        stepping (the ``dt`` argument is ignored, as in the reference's
+        steady SSP-RK mode, core/fr_solver/step.py:47-58)."""
+        norm = ctypes.c_double(0.0)
+        check(LIB.afr_step(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega), _dev_ptr(self.nu_t),
+                           ctypes.byref(norm) if want_norm else None, _stream()), self._h)
+        if want_norm:
+            self.residual_history.append(norm.value)
+            return norm.value
+        return float("nan")
+
+    def solve(self, max_iter: int = 1000, dt: float = 1e-3, tol: float = 1e-6, output_interval: int = 0) -> dict:
+        """GPUFRSolver.solve (core/gpu/gpu_solver.py:403-453): stops on tol or a
+        non-finite norm."""
+        res = float("inf")
+        it = 0
+        converged = False
+        for it in range(1, max_iter + 1):
+            res = self.step(dt)
+            if output_interval and it % output_interval == 0:
+                print(f"Iteration {it}: Residual = {res:.6e}")
+            if not np.isfinite(res):
+                break
+            if res < tol:
+                converged = True
+                break
+        return {"converged": converged, "iterations": it, "final_residual": res,
+                "residual_history": list(self.residual_history)}
+
+    def compute_aerodynamic_coefficients(self, reference_area: float = 1.0) -> Dict[str, float]:
+        """compute_aerodynamic_coefficients_fr (postprocess/fr_coefficients.py:27-152)."""
+        out = (ctypes.c_double * 3)()
+        check(LIB.afr_cd_cl(self._h, _dev_ptr(self.U), _dev_ptr(self.nu_t), float(reference_area), out, _stream()),
+              self._h)
+        return {"Cd": out[0], "Cl": out[1], "Cs": out[2]}
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_uint64(0)
+        check(LIB.afr_device_bytes(self._h, ctypes.byref(v)), self._h)
+        return int(v.value)
+
+    def cleanup(self):
+        """GPUFRSolver.cleanup (core/gpu/gpu_solver_io.py)."""
+        if getattr(self, "_h", None) is not None and self._h.value:
+            LIB.afr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.cleanup()
+        except Exception:
+            pass

@@ -1,0 +1,158 @@
+/*
+ * afr_b200.h -- C-ABI of the B200 (sm_100a) FR residual-and-update library.
+ *
+ * The library replaces, behind one C-ABI, the reference solver's residual /
+ * time-step seam for the explicit Flux-Reconstruction path of AutoFlowCFD.
+ * Reference interfaces replaced (paths relative to the reference's
+ * src/autoflowcfd):
+ *
+ *   afr_create              HighOrderMesh + FRSolver set-up consumed by the path:
+ *                           core/fr_solver/solver.py:58-243 (ctor),
+ *                           core/fr_operators/face_kernels.py:228-369 (FlatFaceGeometry),
+ *                           boundary/fr_ghost_state.py:144-189 (ghost provider tables),
+ *                           core/gpu/gpu_solver.py:51-157 (GPUFRSolver.__init__ upload)
+ *   afr_inviscid_residual   FRSolver.compute_inviscid_residual, core/fr_solver/solver.py:351-400
+ *                           (GPU form: core/gpu/gpu_inviscid.py:31 compute_inviscid_residual_fr_gpu)
+ *   afr_viscous_residual    FRSolver.compute_viscous_residual, core/fr_solver/solver.py:402-432
+ *                           (GPU form: core/gpu/gpu_viscous.py:36)
+ *   afr_local_dt            FRSolver._compute_local_time_step, core/fr_solver/cfl.py:12-147
+ *                           (GPU form: core/gpu/gpu_solver.py:251-293)
+ *   afr_sst_update          FRSolver.compute_turbulence_source, core/fr_solver/turbulence.py:178-330
+ *   afr_step                FRSolver.step, core/fr_solver/step.py:15-221
+ *                           (GPU form: GPUFRSolver.step, core/gpu/gpu_solver.py:295-401)
+ *   afr_cd_cl               compute_aerodynamic_coefficients_fr, postprocess/fr_coefficients.py:27-152
+ *   afr_destroy             GPUFRSolver.cleanup, core/gpu/gpu_solver_io.py:20-35
+ *
+ * Conventions: every call returns an int status (AFR_OK = 0).  Arrays passed
+ * to afr_create are HOST pointers that are copied; arrays passed to the other
+ * calls are DEVICE pointers owned by the caller (contiguous, row-major, the
+ * reference's own layouts: U is (n_cells, n_sps, n_vars) float64, fields are
+ * (n_cells, n_sps) float64).  The library never frees caller memory.  Calls
+ * on one handle are not thread safe.  `stream` is a cudaStream_t (0 = the
+ * legacy default stream).  Kernels never trap: device-side problems are
+ * reported through a status word read back by the call (AFR_ENONFINITE,
+ * AFR_EINDEX).
+ */
+#ifndef AFR_B200_H
+#define AFR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  AFR_OK = 0,
+  AFR_EINVAL = 1,       /* bad argument / inconsistent tables */
+  AFR_ENOMEM = 2,       /* device allocation failed */
+  AFR_ECUDA = 3,        /* CUDA runtime error */
+  AFR_ENONFINITE = 4,   /* non-finite value detected by a kernel */
+  AFR_EUNSUPPORTED = 5, /* order / feature not built into this library */
+  AFR_EINDEX = 6        /* a table index out of range */
+};
+
+enum { AFR_TURB_NONE = 0, AFR_TURB_SST = 1 };
+enum { AFR_BC_WALL = 0, AFR_BC_FARFIELD = 1, AFR_BC_INLET = 2, AFR_BC_OUTLET = 3, AFR_BC_SYMMETRY = 4 };
+
+typedef struct afr_handle afr_handle;
+
+/* Mesh, operators and face tables, as flattened by the reference
+ * (core/fr_operators/face_kernels.py:124-187).  All host pointers. */
+typedef struct afr_mesh_desc {
+  int32_t n_cells, n_prism, order, n_sps, n_fine, n_fp, n_faces;
+  int32_t n_nb_src1, n_ow_src1; /* rows of the compact second-source tables */
+  /* geometry */
+  const double* det_jacs;       /* (N,S) */
+  const double* inv_jacs;       /* (N,S,3,3) */
+  const double* det_jacs_fine;  /* (N,Fn) */
+  const double* inv_jacs_fine;  /* (N,Fn,3,3) */
+  const double* cell_volumes;   /* (N) Gauss-Legendre volume (high_order_mesh.py:335-354) */
+  const double* wall_distance;  /* (N,S) or NULL (required for SST) */
+  /* operators, index 0 = prism, 1 = tet (may be NULL for an absent type) */
+  const double* D_3d[2];        /* (S,S,3) */
+  const double* c2f[2];         /* (Fn,S) */
+  const double* D_fine[2];      /* (Fn,Fn,3) */
+  const double* f2c[2];         /* (S,Fn) */
+  const double* filter[2];      /* (S,S) */
+  const double* boundary_extrap;/* (2,3,2,P,S) */
+  const double* g_left;         /* (order+1) */
+  const double* g_right;
+  const int64_t* dist_fp_of_sp;         /* (3,S) */
+  const int64_t* dist_axis_coord_of_sp; /* (3,S) */
+  /* face records */
+  const int64_t* owner_cell;    /* (F) */
+  const int64_t* neighbor_cell; /* (F), -1 on boundary */
+  const int64_t* owner_axis;
+  const int64_t* neighbor_axis;
+  const double* owner_side;
+  const double* neighbor_side;
+  const uint8_t* is_boundary;
+  const uint8_t* owner_is_primary;
+  const uint8_t* neighbor_is_primary;
+  const double* true_normal;    /* (F,P,3) */
+  const int64_t* nb_src0_cell; const double* nb_src0_mat; /* (F), (F,P,S) */
+  const int64_t* nb_src1_idx;  const int64_t* nb_src1_cell; const double* nb_src1_mat;
+  const int64_t* ow_src0_cell; const double* ow_src0_mat;
+  const int64_t* ow_src1_idx;  const int64_t* ow_src1_cell; const double* ow_src1_mat;
+  const int32_t* colors;        /* (F) greedy face color (core/utils/face_coloring.py:124-176) */
+  /* boundary conditions: row bc_group[f] of the table for boundary face f */
+  int32_t n_bc;
+  const int32_t* bc_group;      /* (F) */
+  const int32_t* bc_type;       /* (n_bc) AFR_BC_* */
+  const int32_t* bc_noslip;     /* (n_bc) */
+  const double* bc_wall_vel;    /* (n_bc,3) */
+  const double* bc_Q;           /* (n_bc,5) free-stream / inlet primitive state */
+  const double* bc_p_out;       /* (n_bc) */
+  /* force integration (optional) */
+  const uint8_t* cd_wall_face;      /* (F) or NULL */
+  const double* true_area_weight;   /* (F,P) or NULL */
+} afr_mesh_desc;
+
+typedef struct afr_params {
+  int32_t n_vars;           /* 5, or 7 with SST (columns 5:7 carried, zero residual) */
+  int32_t turb;             /* AFR_TURB_* */
+  int32_t inviscid_only;    /* 1: viscous residual is zero (Euler) */
+  int32_t reserved;
+  double mu;                /* molecular viscosity of the mean flow (FRSolver mu_molecular) */
+  double rho_inf, vel_inf, p_inf;
+  double global_dt_factor;  /* >0: dt = factor * min(dt_local) everywhere (time-accurate runs) */
+} afr_params;
+
+int afr_create(const afr_mesh_desc* mesh, const afr_params* params, void* stream, afr_handle** out);
+int afr_destroy(afr_handle* h);
+const char* afr_last_error(const afr_handle* h);
+const char* afr_status_string(int status);
+int afr_version(void);
+
+/* Residuals of the state U (device, (N,S,n_vars)), written to R (device, same
+ * shape, turbulence columns zero).  nu_t (device (N,S) or NULL) is the
+ * kinematic eddy viscosity; mu_t = max(rho,1e-10) * nu_t. */
+int afr_inviscid_residual(afr_handle* h, const double* U, double* R, void* stream);
+int afr_viscous_residual(afr_handle* h, const double* U, const double* nu_t, double* R, void* stream);
+
+/* Local time step (device (N,S)). */
+int afr_local_dt(afr_handle* h, const double* U, const double* nu_t, double* dt, void* stream);
+
+/* SST source + transport + point-implicit update of k, omega (in place) and
+ * nu_t (overwritten with the new eddy viscosity).  diag (device (N,S,4) or
+ * NULL) receives Sk, S_omega, transport_k, transport_omega. */
+int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, double* k, double* omega,
+                   double* nu_t, double* diag, void* stream);
+
+/* One SSP-RK3 step in place on U (and k, omega, nu_t with SST; pass NULL
+ * otherwise).  *norm_out (host) receives the RMS of dU/dt at stage 0. */
+int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out,
+             void* stream);
+
+/* Wall force coefficients (Cd, Cl, Cs) of state U into out3 (host). */
+int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3,
+              void* stream);
+
+/* Bytes of device memory the handle owns (tables + scratch). */
+int afr_device_bytes(const afr_handle* h, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFR_B200_H */
