@@ -43,6 +43,9 @@ class AfrMeshDesc(ctypes.Structure):
         ("n_bc", ctypes.c_int32), ("bc_group", _P_I32), ("bc_type", _P_I32), ("bc_noslip", _P_I32),
         ("bc_wall_vel", _P_D), ("bc_Q", _P_D), ("bc_p_out", _P_D),
         ("cd_wall_face", _P_U8), ("true_area_weight", _P_D),
+        ("n_src_mats", ctypes.c_int32), ("src_mat_table", _P_D),
+        ("nb_src0_mat_index", _P_I32), ("nb_src1_mat_index", _P_I32),
+        ("ow_src0_mat_index", _P_I32), ("ow_src1_mat_index", _P_I32),
     ]
 
 
@@ -70,6 +73,9 @@ SIGNATURES = {
     "afr_cd_cl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                  ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "afr_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "afr_step_profile": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                                                  ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
+    "afr_greedy_face_coloring": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, _P_I64, _P_I64, _P_U8, _P_I32]),
 }
 
 
@@ -93,6 +99,18 @@ class AfrError(RuntimeError):
         self.status = status
 
 
+def greedy_face_coloring(owner, neighbor, is_boundary, n_cells):
+    """Face colors by the reference's greedy rule (C++ in libafr_b200.so)."""
+    owner = np.ascontiguousarray(owner, np.int64)
+    neighbor = np.ascontiguousarray(neighbor, np.int64)
+    isb = np.ascontiguousarray(is_boundary, np.uint8)
+    out = np.empty(owner.shape[0], np.int32)
+    check(LIB.afr_greedy_face_coloring(owner.shape[0], int(n_cells), _ptr(owner, ctypes.c_int64),
+                                       _ptr(neighbor, ctypes.c_int64), _ptr(isb, ctypes.c_uint8),
+                                       _ptr(out, ctypes.c_int32)))
+    return out
+
+
 def check(status, handle=None):
     if status != AFR_OK:
         msg = LIB.afr_last_error(handle).decode() if handle else ""
@@ -110,8 +128,8 @@ class MeshTables:
     C-ABI expects, plus the ``afr_mesh_desc`` that points into them."""
 
     F64 = ["det_jacs", "inv_jacs", "det_jacs_fine", "inv_jacs_fine", "cell_volumes", "boundary_extrap",
-           "g_left", "g_right", "owner_side", "neighbor_side", "true_normal", "nb_src0_mat", "nb_src1_mat",
-           "ow_src0_mat", "ow_src1_mat", "bc_wall_vel", "bc_Q", "bc_p_out"]
+           "g_left", "g_right", "owner_side", "neighbor_side", "true_normal", "bc_wall_vel", "bc_Q", "bc_p_out"]
+    MATS = ["nb_src0_mat", "nb_src1_mat", "ow_src0_mat", "ow_src1_mat"]
     I64 = ["dist_fp_of_sp", "dist_axis_coord_of_sp", "owner_cell", "neighbor_cell", "owner_axis", "neighbor_axis",
            "nb_src0_cell", "nb_src1_idx", "nb_src1_cell", "ow_src0_cell", "ow_src1_idx", "ow_src1_cell"]
     U8 = ["is_boundary", "owner_is_primary", "neighbor_is_primary"]
@@ -127,6 +145,14 @@ class MeshTables:
             c[k] = np.ascontiguousarray(case[k], dtype=np.uint8)
         for k in self.I32:
             c[k] = np.ascontiguousarray(case[k], dtype=np.int32)
+        indexed = case.get("src_mat_table") is not None
+        if indexed:
+            c["src_mat_table"] = np.ascontiguousarray(case["src_mat_table"], dtype=np.float64)
+            for k in self.MATS:
+                c[k + "_index"] = np.ascontiguousarray(case[k + "_index"], dtype=np.int32)
+        else:
+            for k in self.MATS:
+                c[k] = np.ascontiguousarray(case[k], dtype=np.float64)
         for t in ("prism", "tet"):
             for k in ("D_3d_", "c2f_", "Dfine_", "f2c_", "filter_"):
                 if k + t in case and case[k + t] is not None:
@@ -147,6 +173,14 @@ class MeshTables:
         d.n_ow_src1 = int(c["ow_src1_cell"].shape[0])
         for k in self.F64:
             setattr(d, k, _ptr(c[k], ctypes.c_double))
+        if indexed:
+            d.n_src_mats = int(c["src_mat_table"].shape[0])
+            d.src_mat_table = _ptr(c["src_mat_table"], ctypes.c_double)
+            for k in self.MATS:
+                setattr(d, k + "_index", _ptr(c[k + "_index"], ctypes.c_int32))
+        else:
+            for k in self.MATS:
+                setattr(d, k, _ptr(c[k], ctypes.c_double))
         for k in self.I64:
             setattr(d, k, _ptr(c[k], ctypes.c_int64))
         for k in self.U8:

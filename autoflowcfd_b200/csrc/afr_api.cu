@@ -95,6 +95,12 @@ int upload_i32(afr_handle* h, int32_t** dst, const T* src, size_t n, cudaStream_
   return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "upload sync");
 }
 
+__global__ void k_expand_mats(const double* table, const int32_t* index, size_t n, size_t per, double* out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * per) return;
+  out[t] = table[(size_t)index[t / per] * per + t % per];
+}
+
 __global__ void k_form_adj(const double* det, const double* inv, double* adj, size_t npts) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * 9) return;
@@ -188,6 +194,15 @@ __global__ void k_force(Geom g, Ops ops, Faces fc, const int32_t* faces, int nf,
   }
 }
 
+// Optional event recorder for afr_step_profile: an event after every launch group.
+struct StepTimer {
+  cudaEvent_t ev[24];
+  int n = 0;
+  void mark(cudaStream_t st) {
+    if (n < 24) cudaEventRecord(ev[n++], st);
+  }
+};
+
 template <int S, int FN, int NP, int N1D>
 struct Launch {
   static size_t stage_smem() { return sizeof(double) * StageSmem<S, FN, NP>::total; }
@@ -205,11 +220,14 @@ struct Launch {
     k_stage<S, FN, NP, N1D><<<h->N, 128, smem, st>>>(h->g, h->ops, h->fc, h->bc, a);
     return cudaGetLastError();
   }
-  static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st) {
+  static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
     k_sst_point<S><<<h->N, 128, 0, st>>>(h->g, h->ops, a);
+    if (tm) tm->mark(st);
     const int nt = h->F * NP;
     k_sst_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    if (tm) tm->mark(st);
     k_sst_update<S, NP><<<h->N, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    if (tm) tm->mark(st);
     return cudaGetLastError();
   }
   static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
@@ -285,6 +303,47 @@ const char* afr_status_string(int s) {
 }
 
 const char* afr_last_error(const afr_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* owner, const int64_t* neighbor,
+                             const uint8_t* is_boundary, int32_t* colors) {
+  if (n_faces < 0 || n_cells < 0 || !owner || !neighbor || !is_boundary || !colors) return AFR_EINVAL;
+  // cell -> faces touching it (owner always, neighbour of interior faces)
+  std::vector<int64_t> cnt(n_cells + 1, 0);
+  for (int64_t f = 0; f < n_faces; ++f) {
+    if (owner[f] < 0 || owner[f] >= n_cells) return AFR_EINDEX;
+    cnt[owner[f] + 1]++;
+    if (!is_boundary[f] && neighbor[f] >= 0) {
+      if (neighbor[f] >= n_cells) return AFR_EINDEX;
+      cnt[neighbor[f] + 1]++;
+    }
+  }
+  for (int64_t c = 0; c < n_cells; ++c) cnt[c + 1] += cnt[c];
+  std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1), lst(cnt[n_cells]);
+  for (int64_t f = 0; f < n_faces; ++f) {
+    lst[pos[owner[f]]++] = f;
+    if (!is_boundary[f] && neighbor[f] >= 0) lst[pos[neighbor[f]]++] = f;
+  }
+  for (int64_t f = 0; f < n_faces; ++f) colors[f] = -1;
+  std::vector<uint8_t> used;
+  for (int64_t f = 0; f < n_faces; ++f) {
+    used.assign(used.size(), 0);
+    const int64_t cells[2] = {owner[f], (!is_boundary[f] && neighbor[f] >= 0) ? neighbor[f] : -1};
+    for (int64_t c : cells) {
+      if (c < 0) continue;
+      for (int64_t i = cnt[c]; i < cnt[c + 1]; ++i) {
+        const int32_t col = colors[lst[i]];
+        if (lst[i] != f && col >= 0) {
+          if ((size_t)col >= used.size()) used.resize(col + 1, 0);
+          used[col] = 1;
+        }
+      }
+    }
+    int32_t c = 0;
+    while ((size_t)c < used.size() && used[c]) ++c;
+    colors[f] = c;
+  }
+  return AFR_OK;
+}
 
 int afr_device_bytes(const afr_handle* h, uint64_t* out) {
   if (!h || !out) return AFR_EINVAL;
@@ -459,13 +518,43 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload_i32(h, &c0n, m->nb_src0_cell, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &i1n, m->nb_src1_idx, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &c1n, m->nb_src1_cell, (size_t)m->n_nb_src1, st, tmp))) return bail(rc);
-    if ((rc = upload(h, &m0n, m->nb_src0_mat, F * P * S, st))) return bail(rc);
-    if ((rc = upload(h, &m1n, m->nb_src1_mat, (size_t)m->n_nb_src1 * P * S, st))) return bail(rc);
+    const bool indexed = m->src_mat_table != nullptr;
+    double* table = nullptr;
+    auto mats = [&](double** dst, const double* dense, const int32_t* index, size_t n) -> int {
+      if (!indexed) return upload(h, dst, dense, n * P * S, st);
+      for (size_t i = 0; i < n; ++i)
+        if (index[i] < 0 || index[i] >= m->n_src_mats) return fail(h, AFR_EINDEX, "matrix index out of range");
+      int r = dalloc(h, dst, n * P * S);
+      if (r) return r;
+      int32_t* di = nullptr;
+      if (cudaMalloc((void**)&di, std::max<size_t>(n, 1) * sizeof(int32_t)) != cudaSuccess)
+        return fail(h, AFR_ENOMEM, "index staging");
+      cudaMemcpyAsync(di, index, n * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+      const size_t tot = n * P * S;
+      if (tot) k_expand_mats<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(table, di, n, P * S, *dst);
+      cudaError_t e = cudaStreamSynchronize(st);
+      cudaFree(di);
+      return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "matrix expansion");
+    };
+    if (indexed) {
+      if (m->n_src_mats <= 0) return bail(fail(h, AFR_EINVAL, "empty matrix table"));
+      if (cudaMalloc((void**)&table, (size_t)m->n_src_mats * P * S * sizeof(double)) != cudaSuccess)
+        return bail(fail(h, AFR_ENOMEM, "matrix table staging"));
+      cudaMemcpyAsync(table, m->src_mat_table, (size_t)m->n_src_mats * P * S * sizeof(double),
+                      cudaMemcpyHostToDevice, st);
+    }
+    int rm = mats(&m0n, m->nb_src0_mat, m->nb_src0_mat_index, F);
+    if (!rm) rm = mats(&m1n, m->nb_src1_mat, m->nb_src1_mat_index, (size_t)m->n_nb_src1);
+    if (!rm) rm = mats(&m0o, m->ow_src0_mat, m->ow_src0_mat_index, F);
+    if (!rm) rm = mats(&m1o, m->ow_src1_mat, m->ow_src1_mat_index, (size_t)m->n_ow_src1);
+    if (table) {
+      cudaStreamSynchronize(st);
+      cudaFree(table);
+    }
+    if (rm) return bail(rm);
     if ((rc = upload_i32(h, &c0o, m->ow_src0_cell, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &i1o, m->ow_src1_idx, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &c1o, m->ow_src1_cell, (size_t)m->n_ow_src1, st, tmp))) return bail(rc);
-    if ((rc = upload(h, &m0o, m->ow_src0_mat, F * P * S, st))) return bail(rc);
-    if ((rc = upload(h, &m1o, m->ow_src1_mat, (size_t)m->n_ow_src1 * P * S, st))) return bail(rc);
     if ((rc = upload(h, &bcg, m->bc_group, F, st))) return bail(rc);
     fc.owner = own; fc.neighbor = nbr; fc.o_axis = oax; fc.n_axis = nax; fc.o_side = osd; fc.n_side = nsd;
     fc.is_bnd = isb; fc.tnormal = tn; fc.nb_c0 = c0n; fc.nb_m0 = m0n; fc.nb_i1 = i1n; fc.nb_c1 = c1n; fc.nb_m1 = m1n;
@@ -596,19 +685,24 @@ int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, doubl
   return check_status(h, st);
 }
 
-int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
+static int step_impl(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out,
+                     cudaStream_t st, StepTimer* tm, int* launches) {
   if (!h || !U) return AFR_EINVAL;
   const bool sst = h->prm.turb == AFR_TURB_SST;
   if (sst && (!k || !omega || !nu_t)) return fail(h, AFR_EINVAL, "SST step needs k, omega and nu_t");
-  cudaStream_t st = (cudaStream_t)stream;
+  int nl = 0;
+  if (tm) tm->mark(st);
   int rc = compute_dt(h, U, sst ? nu_t : nullptr, h->dt, st);
   if (rc) return rc;
+  nl += h->prm.global_dt_factor > 0.0 ? 3 : 1;
+  if (tm) tm->mark(st);
   const bool visc = !h->prm.inviscid_only;
   cudaError_t e = dispatch(h, [&](auto L) {
     cudaError_t r = cudaSuccess;
     if (sst) {
       SstArgs s{U, h->dt, k, omega, nu_t, h->pt, h->cfp, h->wall_face, nullptr, h->nv, h->prm.mu};
-      r = L.sst(h, s, st);
+      r = L.sst(h, s, st, tm);
+      nl += 3;
       if (r != cudaSuccess) return r;
     }
     const double* cur[3] = {U, h->Ua, h->Ub};
@@ -616,8 +710,10 @@ int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, d
     for (int stg = 0; stg < 3; ++stg) {
       if (visc) {
         r = L.grad(h, cur[stg], st);
+        nl += 1;
         if (r != cudaSuccess) return r;
       }
+      if (tm) tm->mark(st);
       StageArgs a = base_args(h);
       a.Ucur = cur[stg];
       a.U0 = U;
@@ -627,12 +723,17 @@ int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, d
       a.norm_part = h->norm_part;
       a.stage = stg;
       r = L.stage(h, a, st);
+      nl += 1;
+      if (tm) tm->mark(st);
       if (r != cudaSuccess) return r;
     }
     return r;
   });
   if (e != cudaSuccess) return cuda_fail(h, e, "step");
   k_reduce_sum<<<1, 1024, 0, st>>>(h->norm_part, (size_t)h->N, h->red);
+  nl += 1;
+  if (tm) tm->mark(st);
+  if (launches) *launches = nl;
   if (norm_out) {
     double ss = 0.0;
     e = cudaMemcpyAsync(&ss, h->red, sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -642,6 +743,32 @@ int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, d
     return check_status(h, st);
   }
   return AFR_OK;
+}
+
+int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
+  return step_impl(h, U, k, omega, nu_t, norm_out, (cudaStream_t)stream, nullptr, nullptr);
+}
+
+int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* ms_out, int n_ms,
+                     int* launches, void* stream) {
+  if (!h || !ms_out || n_ms < 1) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  StepTimer tm;
+  for (int i = 0; i < 24; ++i) cudaEventCreate(&tm.ev[i]);
+  int rc = step_impl(h, U, k, omega, nu_t, nullptr, st, &tm, launches);
+  if (rc == AFR_OK) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "profile sync");
+  }
+  for (int i = 0; i < n_ms; ++i) ms_out[i] = -1.0;
+  if (rc == AFR_OK)
+    for (int i = 0; i + 1 < tm.n && i < n_ms; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, tm.ev[i], tm.ev[i + 1]);
+      ms_out[i] = ms;
+    }
+  for (int i = 0; i < 24; ++i) cudaEventDestroy(tm.ev[i]);
+  return rc;
 }
 
 int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3, void* stream) {

@@ -1,0 +1,29 @@
+"""Per-kernel device timing of one step (CUDA events recorded by the library
+between its launch groups, afr_step_profile)."""
+
+import ctypes
+
+from ._lib import LIB, check
+
+
+def step_breakdown(solver):
+    """Run one step with events; returns per-kernel-group milliseconds."""
+    import torch
+
+    from .solver import _dev_ptr, _stream
+
+    ms = (ctypes.c_double * 24)()
+    nl = ctypes.c_int(0)
+    check(LIB.afr_step_profile(solver._h, _dev_ptr(solver.U), _dev_ptr(solver.k), _dev_ptr(solver.omega),
+                               _dev_ptr(solver.nu_t), ms, 24, ctypes.byref(nl), _stream()), solver._h)
+    torch.cuda.synchronize()
+    vals = [v for v in ms if v >= 0]
+    sst = solver.k is not None
+    names = ["local_dt"] + (["sst_point", "sst_face", "sst_update"] if sst else [])
+    for stg in range(3):
+        names += [f"grad{stg}", f"stage{stg}"]
+    names += ["norm"]
+    per = dict(zip(names, vals))
+    stage_ms = [per[f"stage{i}"] for i in range(3) if f"stage{i}" in per]
+    return {"per_kernel_ms": per, "launches_per_step": int(nl.value),
+            "k_stage_ms_per_launch": sum(stage_ms) / len(stage_ms) if stage_ms else None}

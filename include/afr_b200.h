@@ -107,6 +107,16 @@ typedef struct afr_mesh_desc {
   /* force integration (optional) */
   const uint8_t* cd_wall_face;      /* (F) or NULL */
   const double* true_area_weight;   /* (F,P) or NULL */
+  /* optional indexed form of the interpolation matrices: when src_mat_table
+   * is non-NULL the four *_mat arrays above are ignored and record f's
+   * matrix is src_mat_table[*_mat_index[f]]; the library expands them to the
+   * same dense per-record device layout */
+  int32_t n_src_mats;
+  const double* src_mat_table;      /* (n_src_mats,P,S) */
+  const int32_t* nb_src0_mat_index; /* (F) */
+  const int32_t* nb_src1_mat_index; /* (n_nb_src1) */
+  const int32_t* ow_src0_mat_index; /* (F) */
+  const int32_t* ow_src1_mat_index; /* (n_ow_src1) */
 } afr_mesh_desc;
 
 typedef struct afr_params {
@@ -145,9 +155,22 @@ int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, doubl
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out,
              void* stream);
 
+/* afr_step with a CUDA event after every launch group; ms_out[i] receives the
+ * device time of group i: local dt, [SST point, SST face, SST update],
+ * then per RK stage (gradient pre-pass, fused stage kernel), the norm
+ * reduction.  *launches receives the kernel launches of the step. */
+int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* ms_out, int n_ms,
+                     int* launches, void* stream);
+
 /* Wall force coefficients (Cd, Cl, Cs) of state U into out3 (host). */
 int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3,
               void* stream);
+
+/* Host utility (no GPU): greedy face coloring in face order, the smallest
+ * color not used by any earlier face sharing a cell (owner, and neighbour of
+ * interior faces).  Restates core/utils/face_coloring.py:124-176. */
+int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* owner_cell,
+                             const int64_t* neighbor_cell, const uint8_t* is_boundary, int32_t* colors_out);
 
 /* Bytes of device memory the handle owns (tables + scratch). */
 int afr_device_bytes(const afr_handle* h, uint64_t* out);
