@@ -30,7 +30,7 @@ struct afr_handle {
   Faces fc{};
   Bc bc{};
   // scratch
-  double* grads = nullptr;
+  double* PF = nullptr;       // (N,S,18) point fields of the state being evaluated
   double* Ua = nullptr;
   double* Ub = nullptr;
   double* dt = nullptr;
@@ -151,7 +151,7 @@ __global__ void k_fill_scaled(double* x, size_t n, const double* v, double facto
 // per wall face: pressure and viscous force partials (postprocess/fr_coefficients.py:105-133)
 template <int S, int NP>
 __global__ void k_force(Geom g, Ops ops, Faces fc, const int32_t* faces, int nf, const double* U, int nv,
-                        const double* grads, const double* nut, const double* area_w, double mu, double* part) {
+                        const double* PF, const double* nut, const double* area_w, double mu, double* part) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nf) return;
   const int f = faces[t];
@@ -171,7 +171,7 @@ __global__ void k_force(Geom g, Ops ops, Faces fc, const int32_t* faces, int nf,
       const double w = E[i * S + s];
       pf += w * pr;
       if (nut) mt += w * (rho * nut[p]);
-      for (int k = 0; k < 9; ++k) gv[k] += w * grads[p * 12 + k];
+      for (int k = 0; k < 9; ++k) gv[k] += w * PF[p * PFW + 5 + k];
     }
     const double* n = fc.tnormal + ((size_t)f * NP + i) * 3;
     const double aw = area_w[(size_t)f * NP + i];
@@ -206,18 +206,18 @@ struct StepTimer {
 template <int S, int FN, int NP, int N1D>
 struct Launch {
   static size_t stage_smem() { return sizeof(double) * StageSmem<S, FN, NP>::total; }
-  static cudaError_t grad(afr_handle* h, const double* U, cudaStream_t st) {
-    k_grad<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, h->grads);
+  static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
+    k_pre<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
     return cudaGetLastError();
   }
   static cudaError_t stage(afr_handle* h, const StageArgs& a, cudaStream_t st) {
     const size_t smem = stage_smem();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(k_stage<S, FN, NP, N1D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_stage<S, FN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       attr = true;
     }
-    k_stage<S, FN, NP, N1D><<<h->N, 128, smem, st>>>(h->g, h->ops, h->fc, h->bc, a);
+    k_stage<S, FN, NP><<<h->N, STAGE_THREADS, smem, st>>>(h->g, h->ops, h->fc, h->bc, a);
     return cudaGetLastError();
   }
   static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
@@ -233,7 +233,7 @@ struct Launch {
   static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
     if (h->n_cd_faces == 0) return cudaSuccess;
     k_force<S, NP><<<(h->n_cd_faces + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->cd_faces, h->n_cd_faces, U,
-                                                                 h->nv, h->grads, nut, h->area_w, h->prm.mu,
+                                                                 h->nv, h->PF, nut, h->area_w, h->prm.mu,
                                                                  h->cd_part);
     return cudaGetLastError();
   }
@@ -265,7 +265,7 @@ StageArgs base_args(afr_handle* h) {
   a.mu = h->prm.mu;
   a.inviscid_only = h->prm.inviscid_only;
   a.status = h->status;
-  a.grads = h->grads;
+  a.PF = h->PF;
   return a;
 }
 
@@ -472,6 +472,18 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload(h, &dfn, m->D_fine[t], Fn * Fn * 3, st))) return bail(rc);
     if ((rc = upload(h, &f2c, m->f2c[t], S * Fn, st))) return bail(rc);
     if ((rc = upload(h, &flt, m->filter[t], S * S, st))) return bail(rc);
+    // W = f2c * D_fine (S x 3Fn), summed in ascending fine-point order
+    std::vector<double> Wh(S * 3 * Fn, 0.0);
+    for (size_t r = 0; r < S; ++r)
+      for (size_t k = 0; k < 3 * Fn; ++k) {
+        double acc = 0.0;
+        for (size_t i = 0; i < Fn; ++i) acc += m->f2c[t][r * Fn + i] * m->D_fine[t][i * 3 * Fn + k];
+        Wh[r * 3 * Fn + k] = acc;
+      }
+    double* wdev;
+    if ((rc = upload(h, &wdev, Wh.data(), Wh.size(), st))) return bail(rc);
+    cudaStreamSynchronize(st);
+    h->ops.W[t] = wdev;
     h->ops.D3[t] = d3;
     h->ops.D3g[t] = d3g;
     h->ops.c2f[t] = c2f;
@@ -580,6 +592,9 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
         }
       };
       visit([&](int32_t c, int32_t) { cnt[c + 1]++; });
+      if (!transport)
+        for (size_t i = 0; i < N; ++i)
+          if (cnt[i + 1] > NSLOT) return fail(h, AFR_EUNSUPPORTED, "a cell has more than 6 face slots");
       for (size_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
       std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1), slots(cnt[N]);
       visit([&](int32_t c, int32_t code) { slots[pos[c]++] = code; });
@@ -621,7 +636,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     cudaStreamSynchronize(st);
   }
   // ---- scratch ----
-  if ((rc = dalloc(h, &h->grads, N * S * 12))) return bail(rc);
+  if ((rc = dalloc(h, &h->PF, N * S * PFW))) return bail(rc);
   if ((rc = dalloc(h, &h->Ua, N * S * h->nv))) return bail(rc);
   if ((rc = dalloc(h, &h->Ub, N * S * h->nv))) return bail(rc);
   if ((rc = dalloc(h, &h->dt, N * S))) return bail(rc);
@@ -645,7 +660,10 @@ int afr_inviscid_residual(afr_handle* h, const double* U, double* R, void* strea
   a.inviscid_only = 1;
   a.stage = -1;
   a.Rinv = R;
-  cudaError_t e = dispatch(h, [&](auto L) { return L.stage(h, a, st); });
+  cudaError_t e = dispatch(h, [&](auto L) {
+    cudaError_t r = L.pre(h, U, nullptr, false, st);
+    return r != cudaSuccess ? r : L.stage(h, a, st);
+  });
   if (e != cudaSuccess) return cuda_fail(h, e, "inviscid residual");
   return check_status(h, st);
 }
@@ -660,7 +678,7 @@ int afr_viscous_residual(afr_handle* h, const double* U, const double* nu_t, dou
   a.nut = nu_t;
   a.Rvisc = R;
   cudaError_t e = dispatch(h, [&](auto L) {
-    cudaError_t r = L.grad(h, U, st);
+    cudaError_t r = L.pre(h, U, nu_t, true, st);
     return r != cudaSuccess ? r : L.stage(h, a, st);
   });
   if (e != cudaSuccess) return cuda_fail(h, e, "viscous residual");
@@ -708,11 +726,9 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
     const double* cur[3] = {U, h->Ua, h->Ub};
     double* nxt[3] = {h->Ua, h->Ub, U};
     for (int stg = 0; stg < 3; ++stg) {
-      if (visc) {
-        r = L.grad(h, cur[stg], st);
-        nl += 1;
-        if (r != cudaSuccess) return r;
-      }
+      r = L.pre(h, cur[stg], sst ? nu_t : nullptr, visc, st);
+      nl += 1;
+      if (r != cudaSuccess) return r;
       if (tm) tm->mark(st);
       StageArgs a = base_args(h);
       a.Ucur = cur[stg];
@@ -776,7 +792,7 @@ int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double referen
   if (!h->cd_faces) return fail(h, AFR_EINVAL, "handle was created without wall-face force tables");
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = dispatch(h, [&](auto L) {
-    cudaError_t r = L.grad(h, U, st);
+    cudaError_t r = L.pre(h, U, nu_t, true, st);
     return r != cudaSuccess ? r : L.force(h, U, nu_t, st);
   });
   if (e != cudaSuccess) return cuda_fail(h, e, "force");

@@ -33,6 +33,7 @@ struct Ops {
   const double* c2f[2];     // (Fn, S)
   const double* Dfine[2];   // (Fn, Fn*3)
   const double* f2c[2];     // (S, Fn)
+  const double* W[2];       // (S, 3Fn) = f2c * D_fine, folded once at create
   const double* filt[2];    // (S, S)
   const double* extrap;     // (2, 3, 2, P, S)
   const double* g_left;     // (n1d)
