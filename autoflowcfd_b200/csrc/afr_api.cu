@@ -31,6 +31,8 @@ struct afr_handle {
   Bc bc{};
   // scratch
   double* PF = nullptr;       // (N,S,18) point fields of the state being evaluated
+  double* J = nullptr;        // (n_slots,P,10) face jumps of the residual slots
+  SlotTable slots{};
   double* Ua = nullptr;
   double* Ub = nullptr;
   double* dt = nullptr;
@@ -205,19 +207,34 @@ struct StepTimer {
 
 template <int S, int FN, int NP, int N1D>
 struct Launch {
-  static size_t stage_smem() { return sizeof(double) * StageSmem<S, FN, NP>::total; }
+  static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 2 : 1);
+  static size_t cell_smem() { return sizeof(double) * CellSmem<S, FN, CPB>::total; }
   static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
     k_pre<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
     return cudaGetLastError();
   }
-  static cudaError_t stage(afr_handle* h, const StageArgs& a, cudaStream_t st) {
-    const size_t smem = stage_smem();
+  static cudaError_t stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm = nullptr) {
+    const int nt = h->slots.n * NP;
+    if (nt > 0)
+      k_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->bc, h->slots, h->PF, h->prm.mu,
+                                                      a.inviscid_only ? 0 : 1, h->J);
+    if (tm) tm->mark(st);
+    const size_t smem = cell_smem();
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(k_stage<S, FN, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_cell<S, FN, NP, CPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       attr = true;
     }
-    k_stage<S, FN, NP><<<h->N, STAGE_THREADS, smem, st>>>(h->g, h->ops, h->fc, h->bc, a);
+    a.N = h->N;
+    a.slot_flags = h->slots.flags;
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      a.cell_base = ranges[r];
+      a.cell_end = ranges[r + 1];
+      const int n = a.cell_end - a.cell_base;
+      if (n <= 0) continue;
+      k_cell<S, FN, NP, CPB><<<(n + CPB - 1) / CPB, CELL_THREADS, smem, st>>>(h->g, h->ops, h->fc, a, h->J);
+    }
     return cudaGetLastError();
   }
   static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
@@ -261,6 +278,7 @@ int check_status(afr_handle* h, cudaStream_t st) {
 
 StageArgs base_args(afr_handle* h) {
   StageArgs a{};
+  a.N = h->N;
   a.nv = h->nv;
   a.mu = h->prm.mu;
   a.inviscid_only = h->prm.inviscid_only;
@@ -592,9 +610,6 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
         }
       };
       visit([&](int32_t c, int32_t) { cnt[c + 1]++; });
-      if (!transport)
-        for (size_t i = 0; i < N; ++i)
-          if (cnt[i + 1] > NSLOT) return fail(h, AFR_EUNSUPPORTED, "a cell has more than 6 face slots");
       for (size_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
       std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1), slots(cnt[N]);
       visit([&](int32_t c, int32_t code) { slots[pos[c]++] = code; });
@@ -608,6 +623,36 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = build(false, &sp, &sl))) return bail(rc);
     if ((rc = build(true, &tp, &tl))) return bail(rc);
     fc.slot_ptr = sp; fc.slot = sl; fc.tslot_ptr = tp; fc.tslot = tl;
+    // slot table of the residual slots, in the same (cell, color) order
+    std::vector<int32_t> ptr(N + 1), codes;
+    cudaMemcpy(ptr.data(), sp, (N + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    codes.resize(ptr[N]);
+    cudaMemcpy(codes.data(), sl, codes.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    const size_t ns = codes.size();
+    std::vector<int32_t> sf(ns), sc(ns), sflg(ns), s0(ns), s1(ns), si1(ns);
+    for (size_t c = 0; c < N; ++c)
+      for (int32_t k = ptr[c]; k < ptr[c + 1]; ++k) {
+        const int f = codes[k] >> 1;
+        const bool nbside = (codes[k] & 1) != 0;
+        const bool bnd = m->is_boundary[f] != 0;
+        const int ax = (int)(nbside ? m->neighbor_axis[f] : m->owner_axis[f]);
+        const double side = nbside ? m->neighbor_side[f] : m->owner_side[f];
+        sf[k] = f;
+        sc[k] = (int32_t)c;
+        sflg[k] = (nbside ? 1 : 0) | (bnd ? 2 : 0) | (ax << 2) | (side > 0.0 ? 16 : 0);
+        const int64_t i1 = nbside ? m->ow_src1_idx[f] : m->nb_src1_idx[f];
+        s0[k] = bnd ? -1 : (int32_t)(nbside ? m->ow_src0_cell[f] : m->nb_src0_cell[f]);
+        si1[k] = (int32_t)i1;
+        s1[k] = (bnd || i1 < 0) ? -1 : (int32_t)(nbside ? m->ow_src1_cell[i1] : m->nb_src1_cell[i1]);
+      }
+    int32_t *d_f, *d_c, *d_fl, *d_0, *d_1, *d_i1;
+    if ((rc = upload(h, &d_f, sf.data(), ns, st)) || (rc = upload(h, &d_c, sc.data(), ns, st)) ||
+        (rc = upload(h, &d_fl, sflg.data(), ns, st)) || (rc = upload(h, &d_0, s0.data(), ns, st)) ||
+        (rc = upload(h, &d_1, s1.data(), ns, st)) || (rc = upload(h, &d_i1, si1.data(), ns, st)))
+      return bail(rc);
+    cudaStreamSynchronize(st);
+    h->slots = SlotTable{(int32_t)ns, d_f, d_c, d_fl, d_0, d_1, d_i1};
+    if ((rc = dalloc(h, &h->J, ns * P * 10))) return bail(rc);
   }
   // ---- boundary condition table ----
   {
@@ -738,8 +783,8 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
       a.dt = h->dt;
       a.norm_part = h->norm_part;
       a.stage = stg;
-      r = L.stage(h, a, st);
-      nl += 1;
+      r = L.stage(h, a, st, tm);
+      nl += 2;
       if (tm) tm->mark(st);
       if (r != cudaSuccess) return r;
     }

@@ -30,6 +30,9 @@ struct StageArgs {
   int inviscid_only;
   double mu;
   unsigned* status;
+  int N;                     // cells
+  const int32_t* slot_flags; // (n_slots) flags of the residual slots (see SlotTable)
+  int cell_base, cell_end;   // cell range of this launch (one cell type)
 };
 
 __device__ __forceinline__ int cell_type(const Geom& g, int e) { return e < g.n_prism ? 0 : 1; }
@@ -132,54 +135,171 @@ __global__ void __launch_bounds__(128) k_pre(Geom g, Ops ops, const double* __re
 }
 
 // ---------------------------------------------------------------------------
-// fused stage kernel, one cell per CTA: volume terms, every face slot of the
-// cell (own-side extrapolation, neighbour-side gather, AUSM+up / BR1 fluxes),
-// correction lifting in ascending color order, outlier suppression, then
-// (stage >= 0) the SSP-RK3 Shu-Osher combination, positivity projection and
-// modal filter (core/time_integration/base.py:250-335,
-// core/time_integration/positivity.py:13-45, core/fr_solver/filter.py:29-42).
-// The inviscid volume divergence uses W = f2c * D_fine folded at create time.
+// face kernel: one thread per (slot, flux point).  A slot is one side of one
+// face record whose own extrapolation + correction lifting lands on a cell
+// (core/fr_residual/inviscid_kernel_colored.py:86-157 owner side, :159-236
+// neighbour side; core/fr_residual/viscous_flux_kernel.py:335-520).  Writes
+// the inviscid and viscous flux jumps J (n_slots, NP, 10).
+// Slot flags: bit0 neighbour side, bit1 boundary face, bits2-3 axis, bit4 side>0.
 // ---------------------------------------------------------------------------
-constexpr int NSLOT = 5;   // a prism has 5 cube faces, a tet 4: one primary slot each
-constexpr int NSRC = 2 * NSLOT;
-constexpr int STAGE_THREADS = 256;
-
-// interpolation sources staged in shared memory per cell (the rest is read
-// from global memory): all of them at P1/P2, four at P3
-template <int S>
-struct Staging {
-  static constexpr int src = S >= 64 ? 4 : NSRC;
+struct SlotTable {
+  int32_t n;                // number of slots
+  const int32_t* face;      // (n)
+  const int32_t* cell;      // (n) cell the slot lifts into
+  const int32_t* flags;     // (n)
+  const int32_t* c0;        // (n) first interpolation source cell, -1 if none
+  const int32_t* c1;        // (n) second source cell, -1 if none
+  const int32_t* i1;        // (n) row of the compact second-source table
 };
 
-template <int S, int FN, int NP>
-struct StageSmem {
-  static constexpr int oPF = 0;                   // S*18 own point fields
-  static constexpr int oAdj = oPF + S * PFW;      // S*9
-  static constexpr int oU = oAdj + S * 9;         // S*8 own state rows
-  static constexpr int oDet = oU + S * 8;         // S
-  static constexpr int oRi = oDet + S;            // S*5
-  static constexpr int oRv = oRi + S * 5;         // S*5
-  static constexpr int oJ = oRv + S * 5;          // NSLOT*NP*10 face jumps
-  static constexpr int oBig = oJ + NSLOT * NP * 10;
-  // slot phase: own extrapolation (21) and neighbour gather (18) per flux point
-  static constexpr int sOwn = 0;
-  static constexpr int sOth = sOwn + NSLOT * NP * 21;
-  static constexpr int sEnd = sOth + NSLOT * NP * 18;
-  // volume phase (aliases the slot scratch)
-  static constexpr int vQf = 0;                   // FN*5
-  static constexpr int vFt = vQf + FN * 5;        // FN*15
-  static constexpr int vGt = vFt + FN * 15;       // S*15
-  static constexpr int vEnd = vGt + S * 15;
-  static constexpr int big = sEnd > vEnd ? sEnd : vEnd;
-  static constexpr int work = oBig + big;         // 24 doubles for reductions
-  static constexpr int oSM = work + 24;           // staged source matrices
-  static constexpr int oSC = oSM + Staging<S>::src * NP * S;  // staged neighbour point fields
-  static constexpr int total = oSC + Staging<S>::src * S * PFW;
+__device__ __forceinline__ void ld18(const double* __restrict__ p, double x[18]) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const double2 v = __ldg(q + j);
+    x[2 * j] = v.x;
+    x[2 * j + 1] = v.y;
+  }
+}
+
+template <int S, int NP>
+__global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc bc, SlotTable st,
+                                                 const double* __restrict__ PF, double mu, int visc,
+                                                 double* __restrict__ J) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= st.n * NP) return;
+  const int sl = t / NP, i = t % NP;
+  const int f = st.face[sl];
+  const int e = st.cell[sl];
+  const int fl = st.flags[sl];
+  const bool is_owner = (fl & 1) == 0;
+  const bool bnd = (fl & 2) != 0;
+  const int ax = (fl >> 2) & 3;
+  const double side = (fl & 16) ? 1.0 : -1.0;
+  const int ct = cell_type(g, e);
+  // own-side extrapolation: q(5), adjugate row of this axis(3), grads+mu_t(13)
+  double ow[21];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) ow[k] = 0.0;
+  {
+    const double* Er = ops.extrap + ((((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * NP + i) * S;
+    const double* pf = PF + (size_t)e * S * PFW;
+    const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
+    for (int s = 0; s < S; ++s) {
+      const double w = __ldg(Er + s);
+      double x[18];
+      ld18(pf + s * PFW, x);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) ow[k] += w * x[k];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) ow[5 + d] += w * __ldg(ad + s * 9 + d);
+      if (visc) {
+#pragma unroll
+        for (int k = 0; k < 13; ++k) ow[8 + k] += w * x[5 + k];
+      }
+    }
+  }
+  // other side: interpolation sources (sum src0 then src1, zero weights skipped)
+  double ot[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) ot[k] = 0.0;
+  const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
+  if (bnd) {
+    double qo[5], n[3], gq[5];
+    for (int v = 0; v < 5; ++v) qo[v] = ow[v];
+    for (int d = 0; d < 3; ++d) n[d] = tn[d];
+    ghost_state(bc, fc.bc_group[f], qo, n, gq);
+    for (int v = 0; v < 5; ++v) ot[v] = gq[v];
+    for (int k = 0; k < 13; ++k) ot[5 + k] = ow[8 + k];
+  } else {
+    for (int src = 0; src < 2; ++src) {
+      const int c = src == 0 ? st.c0[sl] : st.c1[sl];
+      if (c < 0) continue;
+      const double* M = src == 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S
+                                 : (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S;
+      const double* pf = PF + (size_t)c * S * PFW;
+      for (int s = 0; s < S; ++s) {
+        const double w = __ldg(M + s);
+        if (w == 0.0) continue;  // the reference skips zero weights (inviscid_kernel_colored.py:117-121)
+        double x[18];
+        ld18(pf + s * PFW, x);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) ot[k] += w * x[k];
+        if (visc) {
+#pragma unroll
+          for (int k = 0; k < 13; ++k) ot[5 + k] += w * x[5 + k];
+        }
+      }
+    }
+  }
+  // pointwise fluxes
+  const double a0 = ow[5], a1 = ow[6], a2 = ow[7];
+  double mag = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+  if (mag < 1e-300) mag = 1e-300;
+  double dir[3] = {a0 / mag * side, a1 / mag * side, a2 / mag * side};
+  const double sg = is_owner ? 1.0 : -1.0;
+  const double t0 = sg * tn[0], t1 = sg * tn[1], t2 = sg * tn[2];
+  if (dir[0] * t0 + dir[1] * t1 + dir[2] * t2 < 0.5) { dir[0] = t0; dir[1] = t1; dir[2] = t2; }
+  double Fc[5], Fp[3][5];
+  ausm_up(ow, ot, dir, Fc);
+  euler_flux(ow, Fp);
+  double* Jo = J + (size_t)t * 10;
+  for (int v = 0; v < 5; ++v) Jo[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
+  if (visc) {
+    double qa[5], ga[13];
+    for (int v = 0; v < 5; ++v) qa[v] = 0.5 * (ow[v] + ot[v]);
+    for (int k = 0; k < 13; ++k) ga[k] = 0.5 * (ow[8 + k] + ot[5 + k]);
+    double Gc[3][5], Go[3][5];
+    viscous_flux(qa, ga, ga + 9, mu, ga[12], Gc);
+    viscous_flux(ow, ow + 8, ow + 17, mu, ow[20], Go);
+    double jv[5];
+    for (int v = 0; v < 5; ++v)
+      jv[v] = (a0 * Gc[0][v] + a1 * Gc[1][v] + a2 * Gc[2][v]) - (a0 * Go[0][v] + a1 * Go[1][v] + a2 * Go[2][v]);
+    if (bnd) {
+      // interior-penalty term on boundary faces (core/fr_operators/flux_kernels.py:140-200);
+      // cell volume scale = mean of det over the cell's points (viscous_flux_kernel.py:344-347)
+      double vol_o = 0.0;
+      for (int s = 0; s < S; ++s) vol_o += g.det[(size_t)e * S + s];
+      vol_o /= S;
+      double h = pow(vol_o, 1.0 / 3.0);
+      if (h < 1e-300) h = 1e-300;
+      const double eta = C_IP * (mu + ow[20]) / h;
+      const double scale = eta * sqrt(a0 * a0 + a1 * a1 + a2 * a2) * side;
+      for (int v = 1; v < 4; ++v) jv[v] += -scale * (ow[v] - ot[v]);
+    }
+    for (int v = 0; v < 5; ++v) Jo[5 + v] = jv[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cell kernel: CPB cells per CTA.  Volume terms (inviscid over-integrated
+// divergence with W = f2c * D_fine folded at create, viscous divergence),
+// lifting of the face jumps of each cell's slots in ascending color order,
+// outlier suppression, then (stage >= 0) the SSP-RK3 Shu-Osher combination,
+// positivity projection and modal filter (core/time_integration/base.py:250-335,
+// core/time_integration/positivity.py:13-45, core/fr_solver/filter.py:29-42).
+// ---------------------------------------------------------------------------
+constexpr int CELL_THREADS = 256;
+
+template <int S, int FN, int CPB>
+struct CellSmem {
+  static constexpr int oPF = 0;                    // CPB*S*18
+  static constexpr int oAdj = oPF + CPB * S * PFW; // CPB*S*9
+  static constexpr int oU = oAdj + CPB * S * 9;    // CPB*S*8
+  static constexpr int oDet = oU + CPB * S * 8;    // CPB*S
+  static constexpr int oRi = oDet + CPB * S;       // CPB*S*5
+  static constexpr int oRv = oRi + CPB * S * 5;    // CPB*S*5
+  static constexpr int oQf = oRv + CPB * S * 5;    // CPB*FN*5
+  static constexpr int oFt = oQf + CPB * FN * 5;   // CPB*FN*15
+  static constexpr int oGt = oFt + CPB * FN * 15;  // CPB*S*15
+  static constexpr int work = oGt + CPB * S * 15;  // CPB*24
+  static constexpr int total = work + CPB * 24;
 };
 
-template <int S, int FN, int NP>
-__global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(Geom g, Ops ops, Faces fc, Bc bc, StageArgs a) {
-  using L = StageSmem<S, FN, NP>;
+template <int S, int FN, int NP, int CPB>
+__global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces fc, StageArgs a,
+                                                          const double* __restrict__ J) {
+  using L = CellSmem<S, FN, CPB>;
   extern __shared__ double sm[];
   double* sPF = sm + L::oPF;
   double* sAdj = sm + L::oAdj;
@@ -187,309 +307,152 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(Geom g, Ops ops, Fac
   double* sDet = sm + L::oDet;
   double* sRi = sm + L::oRi;
   double* sRv = sm + L::oRv;
-  double* sJ = sm + L::oJ;
-  double* big = sm + L::oBig;
+  double* sQf = sm + L::oQf;
+  double* sFt = sm + L::oFt;
+  double* sGt = sm + L::oGt;
   double* work = sm + L::work;
-  __shared__ int slF[NSLOT], slAx[NSLOT], slOwn[NSLOT], slBnd[NSLOT];
-  __shared__ double slSide[NSLOT];
-  __shared__ const double* slE[NSLOT];
-  __shared__ int slSrc[NSLOT + 1];                 // sources of slot sl: [slSrc[sl], slSrc[sl+1])
-  __shared__ const double* srcM[NSRC];             // source matrix (global)
-  __shared__ int srcCell[NSRC], srcStage[NSRC];    // neighbour cell, staged cell slot or -1
-  __shared__ int n_src, n_ucell;
-  __shared__ int ucell[NSRC];
-  constexpr int MAXST = Staging<S>::src;
-  double* sMs = sm + L::oSM;
-  double* sNs = sm + L::oSC;
-
-  const int e = blockIdx.x;
-  const int ct = cell_type(g, e);
+  const int e0 = a.cell_base + blockIdx.x * CPB;
+  const int nc = min(CPB, a.cell_end - e0);
+  const int ct = cell_type(g, e0);  // a launch covers cells of one type
   const int nv = a.nv;
   const bool visc = !a.inviscid_only;
   const int tid = threadIdx.x;
-  const int s_beg = fc.slot_ptr[e];
-  const int nsl = min(fc.slot_ptr[e + 1] - s_beg, NSLOT);
 
-  // ---- phase 0: own cell, slot metadata, staged sources ----
-  {
-    const double* pf = a.PF + (size_t)e * S * PFW;
-    for (int t = tid; t < S * PFW; t += blockDim.x) sPF[t] = pf[t];
-    const double* ad = g.adj + (size_t)e * S * 9;
-    for (int t = tid; t < S * 9; t += blockDim.x) sAdj[t] = ad[t];
-    const double* u = a.Ucur + (size_t)e * S * nv;
-    for (int t = tid; t < S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = u[t];
-    for (int t = tid; t < S; t += blockDim.x) sDet[t] = g.det[(size_t)e * S + t];
-    if (tid == 0) {
-      if (fc.slot_ptr[e + 1] - s_beg > NSLOT) atomicOr(a.status, DS_BAD_INDEX);
-      int k = 0, nu = 0;
-      for (int sl = 0; sl < nsl; ++sl) {
-        const int code = fc.slot[s_beg + sl];
-        const int f = code >> 1;
-        const bool own = (code & 1) == 0;
-        const int ax = own ? fc.o_axis[f] : fc.n_axis[f];
-        const double side = own ? fc.o_side[f] : fc.n_side[f];
-        slF[sl] = f;
-        slOwn[sl] = own;
-        slAx[sl] = ax;
-        slSide[sl] = side;
-        slBnd[sl] = fc.is_bnd[f];
-        slE[sl] = ops.extrap + (((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * NP * S;
-        slSrc[sl] = k;
-        if (slBnd[sl]) continue;
-        const int c0 = own ? fc.nb_c0[f] : fc.ow_c0[f];
-        const int i1 = own ? fc.nb_i1[f] : fc.ow_i1[f];
-        for (int src = 0; src < 2; ++src) {
-          const int c = src == 0 ? c0 : (i1 >= 0 ? (own ? fc.nb_c1[i1] : fc.ow_c1[i1]) : -1);
-          if (c < 0) continue;
-          srcM[k] = src == 0 ? (own ? fc.nb_m0 : fc.ow_m0) + (size_t)f * NP * S
-                             : (own ? fc.nb_m1 : fc.ow_m1) + (size_t)i1 * NP * S;
-          srcCell[k] = c;
-          int st = -1;
-          for (int j = 0; j < nu; ++j)
-            if (ucell[j] == c) st = j;
-          if (st < 0 && nu < MAXST) {
-            ucell[nu] = c;
-            st = nu++;
-          }
-          srcStage[k] = st;
-          ++k;
-        }
-      }
-      slSrc[nsl] = k;
-      n_src = k;
-      n_ucell = nu;
-    }
-  }
-  __syncthreads();
-  {
-    const int nm = min(n_src, MAXST);
-    for (int t = tid; t < nm * NP * S; t += blockDim.x) {
-      const int k = t / (NP * S), r = t % (NP * S);
-      sMs[t] = __ldg(srcM[k] + r);
-    }
-    for (int t = tid; t < n_ucell * S * PFW; t += blockDim.x) {
-      const int j = t / (S * PFW), r = t % (S * PFW);
-      sNs[t] = __ldg(a.PF + (size_t)ucell[j] * S * PFW + r);
-    }
-  }
+  // ---- load ----
+  for (int t = tid; t < nc * S * PFW; t += blockDim.x) sPF[t] = a.PF[(size_t)e0 * S * PFW + t];
+  for (int t = tid; t < nc * S * 9; t += blockDim.x) sAdj[t] = g.adj[(size_t)e0 * S * 9 + t];
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
+  for (int t = tid; t < nc * S; t += blockDim.x) sDet[t] = g.det[(size_t)e0 * S + t];
   __syncthreads();
 
-  // ---- phase 1: own extrapolations and neighbour gathers of every slot ----
-  double* own = big + L::sOwn;  // [sl][i][21]: q(5) adj row(3) grads+mu_t(13)
-  double* oth = big + L::sOth;  // [sl][i][18]: q(5) grads+mu_t(13)
-  {
-    const int nown3 = visc ? 7 : 3;
-    const int noth3 = visc ? 6 : 2;
-    const int n_own = nsl * NP * nown3;
-    const int n_all = n_own + nsl * NP * noth3;
-    for (int t = tid; t < n_all; t += blockDim.x) {
-      if (t < n_own) {
-        const int sl = t / (NP * nown3), r = t % (NP * nown3), i = r / nown3, c0 = (r % nown3) * 3;
-        const double* Er = slE[sl] + i * S;
-        const int ax = slAx[sl];
-        double acc[3] = {0.0, 0.0, 0.0};
-        for (int s = 0; s < S; ++s) {
-          const double w = __ldg(Er + s);
+  // ---- Q at fine points (c2f) and viscous contravariant fluxes ----
+  for (int t = tid; t < FN * 5; t += blockDim.x) {
+    const int i = t / 5, v = t % 5;
+    const double* c = ops.c2f[ct] + i * S;
+    double acc[CPB];
 #pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            const int c = c0 + j;
-            const double x = c < 5 ? sPF[s * PFW + c] : (c < 8 ? sAdj[s * 9 + ax * 3 + c - 5] : sPF[s * PFW + c - 3]);
-            acc[j] += w * x;
-          }
-        }
-        double* o = own + (sl * NP + i) * 21 + c0;
-        for (int j = 0; j < 3; ++j) o[j] = acc[j];
-      } else {
-        const int u = t - n_own;
-        const int sl = u / (NP * noth3), r = u % (NP * noth3), i = r / noth3, k0 = (r % noth3) * 3;
-        if (slBnd[sl]) continue;
-        double acc[3] = {0.0, 0.0, 0.0};
-        for (int k = slSrc[sl]; k < slSrc[sl + 1]; ++k) {
-          const double* Mr = (k < MAXST ? sMs + k * NP * S : srcM[k]) + i * S;
-          const int st = srcStage[k];
-          const double* pf = (st >= 0 ? sNs + st * S * PFW : a.PF + (size_t)srcCell[k] * S * PFW) + k0;
-          for (int s = 0; s < S; ++s) {
-            const double w = Mr[s];
-            // the reference skips zero weights (inviscid_kernel_colored.py:117-121)
+    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+    for (int s = 0; s < S; ++s) {
+      const double w = __ldg(c + s);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) acc[j] += (w != 0.0) ? w * pf[s * PFW + j] : 0.0;
-          }
-        }
-        double* o = oth + (sl * NP + i) * 18 + k0;
-        for (int j = 0; j < 3; ++j) o[j] = acc[j];
-      }
+      for (int b = 0; b < CPB; ++b) acc[b] += w * sPF[(b * S + s) * PFW + v];
     }
+#pragma unroll
+    for (int b = 0; b < CPB; ++b)
+      if (b < nc) sQf[(b * FN + i) * 5 + v] = acc[b];
   }
-  __syncthreads();
-
-  // ---- phase 2: pointwise interface fluxes at every (slot, flux point) ----
-  double vol_o = 0.0;
   if (visc) {
-    for (int s = 0; s < S; ++s) vol_o += sDet[s];
-    vol_o /= S;
-  }
-  for (int t = tid; t < nsl * NP; t += blockDim.x) {
-    const int sl = t / NP, i = t % NP;
-    const double* ow = own + (sl * NP + i) * 21;
-    double* ot = oth + (sl * NP + i) * 18;
-    const int f = slF[sl];
-    const double side = slSide[sl];
-    const bool is_owner = slOwn[sl] != 0;
-    const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
-    if (slBnd[sl]) {
-      double qo[5], n[3], gq[5];
-      for (int v = 0; v < 5; ++v) qo[v] = ow[v];
-      for (int d = 0; d < 3; ++d) n[d] = tn[d];
-      ghost_state(bc, fc.bc_group[f], qo, n, gq);
-      for (int v = 0; v < 5; ++v) ot[v] = gq[v];
-      for (int k = 0; k < 13; ++k) ot[5 + k] = ow[8 + k];
-    }
-    const double a0 = ow[5], a1 = ow[6], a2 = ow[7];
-    double mag = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
-    if (mag < 1e-300) mag = 1e-300;
-    double dir[3] = {a0 / mag * side, a1 / mag * side, a2 / mag * side};
-    const double sg = is_owner ? 1.0 : -1.0;
-    const double t0 = sg * tn[0], t1 = sg * tn[1], t2 = sg * tn[2];
-    if (dir[0] * t0 + dir[1] * t1 + dir[2] * t2 < 0.5) { dir[0] = t0; dir[1] = t1; dir[2] = t2; }
-    double qo[5], qn[5], Fc[5], Fp[3][5];
-    for (int v = 0; v < 5; ++v) { qo[v] = ow[v]; qn[v] = ot[v]; }
-    ausm_up(qo, qn, dir, Fc);
-    euler_flux(qo, Fp);
-    double* J = sJ + (sl * NP + i) * 10;
-    for (int v = 0; v < 5; ++v) J[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
-    if (visc) {
-      double qa[5], ga[13];
-      for (int v = 0; v < 5; ++v) qa[v] = 0.5 * (qo[v] + qn[v]);
-      for (int k = 0; k < 13; ++k) ga[k] = 0.5 * (ow[8 + k] + ot[5 + k]);
-      double Gc[3][5], Go[3][5];
-      viscous_flux(qa, ga, ga + 9, a.mu, ga[12], Gc);
-      viscous_flux(qo, ow + 8, ow + 17, a.mu, ow[20], Go);
-      double jv[5];
-      for (int v = 0; v < 5; ++v)
-        jv[v] = (a0 * Gc[0][v] + a1 * Gc[1][v] + a2 * Gc[2][v]) - (a0 * Go[0][v] + a1 * Go[1][v] + a2 * Go[2][v]);
-      if (slBnd[sl]) {
-        // interior-penalty term on boundary faces (core/fr_operators/flux_kernels.py:140-200)
-        double h = pow(vol_o, 1.0 / 3.0);
-        if (h < 1e-300) h = 1e-300;
-        const double eta = C_IP * (a.mu + ow[20]) / h;
-        const double scale = eta * sqrt(a0 * a0 + a1 * a1 + a2 * a2) * side;
-        for (int v = 1; v < 4; ++v) jv[v] += -scale * (qo[v] - qn[v]);
-      }
-      for (int v = 0; v < 5; ++v) J[5 + v] = jv[v];
-    }
-  }
-  __syncthreads();
-
-  // ---- phase 3: volume terms ----
-  {
-    double* Qf = big + L::vQf;
-    double* Ft = big + L::vFt;
-    double* Gt = big + L::vGt;
-    // Q at fine points (c2f), own Q is sPF[s*18 + 0..4]
-    for (int t = tid; t < FN * 5; t += blockDim.x) {
-      const int i = t / 5, v = t % 5;
-      const double* c = ops.c2f[ct] + i * S;
-      double acc = 0.0;
-      for (int s = 0; s < S; ++s) acc += __ldg(c + s) * sPF[s * PFW + v];
-      Qf[t] = acc;
-    }
-    if (visc) {
-      for (int s = tid; s < S; s += blockDim.x) {
-        double q[5], G[3][5];
-        const double* p = sPF + s * PFW;
-        for (int v = 0; v < 5; ++v) q[v] = p[v];
-        viscous_flux(q, p + 5, p + 14, a.mu, p[17], G);
-        const double* am = sAdj + s * 9;
-        for (int m = 0; m < 3; ++m)
-          for (int v = 0; v < 5; ++v)
-            Gt[(s * 3 + m) * 5 + v] = am[m * 3 + 0] * G[0][v] + am[m * 3 + 1] * G[1][v] + am[m * 3 + 2] * G[2][v];
-      }
-    }
-    __syncthreads();
-    for (int i = tid; i < FN; i += blockDim.x) {
-      double q[5], F[3][5];
-      for (int v = 0; v < 5; ++v) q[v] = Qf[i * 5 + v];
-      euler_flux(q, F);
-      const double* ad = g.adj_fine + ((size_t)e * FN + i) * 9;
-      double am[9];
-      for (int k = 0; k < 9; ++k) am[k] = __ldg(ad + k);
+    for (int t = tid; t < nc * S; t += blockDim.x) {
+      double q[5], G[3][5];
+      const double* p = sPF + t * PFW;
+      for (int v = 0; v < 5; ++v) q[v] = p[v];
+      viscous_flux(q, p + 5, p + 14, a.mu, p[17], G);
+      const double* am = sAdj + t * 9;
       for (int m = 0; m < 3; ++m)
         for (int v = 0; v < 5; ++v)
-          Ft[(i * 3 + m) * 5 + v] = am[m * 3 + 0] * F[0][v] + am[m * 3 + 1] * F[1][v] + am[m * 3 + 2] * F[2][v];
-    }
-    __syncthreads();
-    // inviscid divergence W (S x 3FN) and viscous divergence D3 (S x 3S)
-    const int n_i = S * 5, n_all = visc ? 2 * S * 5 : S * 5;
-    for (int t = tid; t < n_all; t += blockDim.x) {
-      if (t < n_i) {
-        const int s = t / 5, v = t % 5;
-        const double* w = ops.W[ct] + (size_t)s * FN * 3;
-        double acc = 0.0;
-#pragma unroll 4
-        for (int k = 0; k < FN * 3; ++k) acc += __ldg(w + k) * Ft[k * 5 + v];
-        sRi[t] = -acc / sDet[s];
-      } else {
-        const int u = t - n_i, s = u / 5, v = u % 5;
-        const double* d = ops.D3[ct] + (size_t)s * S * 3;
-        double acc = 0.0;
-#pragma unroll 4
-        for (int k = 0; k < S * 3; ++k) acc += __ldg(d + k) * Gt[k * 5 + v];
-        sRv[u] = acc / sDet[s];
-      }
+          sGt[(t * 3 + m) * 5 + v] = am[m * 3 + 0] * G[0][v] + am[m * 3 + 1] * G[1][v] + am[m * 3 + 2] * G[2][v];
     }
   }
   __syncthreads();
-
-  // ---- phase 4: lift corrections, slots in ascending color order ----
-  for (int t = tid; t < S * 5; t += blockDim.x) {
-    const int s = t / 5, v = t % 5;
+  // ---- Euler fluxes at fine points, contravariant with adj_fine ----
+  for (int t = tid; t < nc * FN; t += blockDim.x) {
+    const int b = t / FN, i = t % FN;
+    double q[5], F[3][5];
+    for (int v = 0; v < 5; ++v) q[v] = sQf[t * 5 + v];
+    euler_flux(q, F);
+    const double* ad = g.adj_fine + ((size_t)(e0 + b) * FN + i) * 9;
+    double am[9];
+    for (int k = 0; k < 9; ++k) am[k] = __ldg(ad + k);
+    for (int m = 0; m < 3; ++m)
+      for (int v = 0; v < 5; ++v)
+        sFt[(t * 3 + m) * 5 + v] = am[m * 3 + 0] * F[0][v] + am[m * 3 + 1] * F[1][v] + am[m * 3 + 2] * F[2][v];
+  }
+  __syncthreads();
+  // ---- divergences: inviscid W (S x 3FN), viscous D3 (S x 3S) ----
+  {
+    const int n_i = S * 5, n_all = visc ? 2 * S * 5 : S * 5;
+    for (int t = tid; t < n_all; t += blockDim.x) {
+      const bool inv = t < n_i;
+      const int u = inv ? t : t - n_i;
+      const int s = u / 5, v = u % 5;
+      const int K = inv ? FN * 3 : S * 3;
+      const double* w = inv ? ops.W[ct] + (size_t)s * FN * 3 : ops.D3[ct] + (size_t)s * S * 3;
+      const double* X = inv ? sFt : sGt;
+      const int ldb = inv ? FN * 15 : S * 15;
+      double acc[CPB];
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < K; ++k) {
+        const double wk = __ldg(w + k);
+#pragma unroll
+        for (int b = 0; b < CPB; ++b) acc[b] += wk * X[b * ldb + k * 5 + v];
+      }
+#pragma unroll
+      for (int b = 0; b < CPB; ++b)
+        if (b < nc) {
+          const double dj = sDet[b * S + s];
+          if (inv) sRi[(b * S + s) * 5 + v] = -acc[b] / dj;
+          else sRv[(b * S + s) * 5 + v] = acc[b] / dj;
+        }
+    }
+  }
+  __syncthreads();
+  // ---- lift the face jumps of each cell's slots, ascending color order ----
+  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
+    const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    const int e = e0 + b;
+    const double dj = sDet[b * S + s];
     double ci = 0.0, cv = 0.0;
-    for (int sl = 0; sl < nsl; ++sl) {
-      const int ax = slAx[sl];
+    for (int k = fc.slot_ptr[e]; k < fc.slot_ptr[e + 1]; ++k) {
+      const int fl = a.slot_flags[k];
+      const int ax = (fl >> 2) & 3;
       const int fp = ops.dist_fp[ax * S + s];
-      const double gw = (slSide[sl] < 0.0 ? ops.g_left : ops.g_right)[ops.dist_co[ax * S + s]];
-      const double* J = sJ + (sl * NP + fp) * 10;
-      ci += -(gw * J[v]) / sDet[s];
-      if (visc) cv += (gw * J[5 + v]) / sDet[s];
+      const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
+      const double* Jk = J + ((size_t)k * NP + fp) * 10;
+      ci += -(gw * Jk[v]) / dj;
+      if (visc) cv += (gw * Jk[5 + v]) / dj;
     }
     sRi[t] = sRi[t] + ci;
     if (visc) sRv[t] = sRv[t] + cv;
   }
   __syncthreads();
-  suppress_outliers<S>(sRi, sU, 8, work);
-  if (visc) suppress_outliers<S>(sRv, sU, 8, work);
+  for (int b = 0; b < nc; ++b) {
+    suppress_outliers<S>(sRi + b * S * 5, sU + b * S * 8, 8, work);
+    if (visc) suppress_outliers<S>(sRv + b * S * 5, sU + b * S * 8, 8, work);
+  }
 
   if (a.stage < 0) {
-    for (int t = tid; t < S * nv; t += blockDim.x) {
-      const int s = t / nv, v = t % nv;
-      if (a.Rinv) a.Rinv[(size_t)e * S * nv + t] = v < 5 ? sRi[s * 5 + v] : 0.0;
-      if (a.Rvisc) a.Rvisc[(size_t)e * S * nv + t] = (v < 5 && visc) ? sRv[s * 5 + v] : 0.0;
+    for (int t = tid; t < nc * S * nv; t += blockDim.x) {
+      const int p = t / nv, v = t % nv;
+      if (a.Rinv) a.Rinv[(size_t)e0 * S * nv + t] = v < 5 ? sRi[p * 5 + v] : 0.0;
+      if (a.Rvisc) a.Rvisc[(size_t)e0 * S * nv + t] = (v < 5 && visc) ? sRv[p * 5 + v] : 0.0;
     }
     return;
   }
 
-  // ---- phase 5: RK stage combination + positivity (per point) ----
-  double* Up = big;  // (S, 8)
-  double part = 0.0;
-  for (int s = tid; s < S; s += blockDim.x) {
-    double L[8], un[8];
-    for (int v = 0; v < nv; ++v) L[v] = v < 5 ? sRi[s * 5 + v] + (visc ? sRv[s * 5 + v] : 0.0) : 0.0;
-    if (a.stage == 0)
-      for (int v = 0; v < nv; ++v) part += L[v] * L[v];
-    const double dts = a.dt[(size_t)e * S + s];
-    const double* u0 = a.U0 + ((size_t)e * S + s) * nv;
-    const double* uc = sU + s * 8;
+  // ---- RK stage combination + positivity (per point) ----
+  double* Up = sQf;  // (CPB*S, 8) reuses the fine-point scratch
+  double* part = sGt;  // (CPB*S) squared dU/dt per point (stage 0)
+  for (int p = tid; p < nc * S; p += blockDim.x) {
+    double Lr[8], un[8];
+    double sq_sum = 0.0;
+    for (int v = 0; v < nv; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
+    for (int v = 0; v < nv; ++v) sq_sum += Lr[v] * Lr[v];
+    const size_t gp = (size_t)e0 * S + p;
+    const double dts = a.dt[gp];
+    const double* u0 = a.U0 + gp * nv;
+    const double* uc = sU + p * 8;
     if (a.stage == 0) {
-      for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * L[v];
+      for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
     } else if (a.stage == 1) {
-      for (int v = 0; v < nv; ++v) un[v] = (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * L[v];
+      for (int v = 0; v < nv; ++v) un[v] = (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v];
     } else {
       // 1/3 U0 + 0 U1 + 2/3 U2 + 2/3 dt L; the 0*U1 term is dropped: it can only
       // turn a finite value into NaN where U1 is non-finite, and U2 (filtered
       // from U1) is then non-finite at the same cell already.
-      for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * L[v];
+      for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v];
     }
-    // enforce_positivity (p_floor = 1)
     const double rho = fmax(un[0], 1e-6);
     un[0] = rho;
     double vel[3] = {un[1] / rho, un[2] / rho, un[3] / rho};
@@ -499,37 +462,33 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2) k_stage(Geom g, Ops ops, Fac
       for (int d = 0; d < 3; ++d) { vel[d] *= cf; un[1 + d] = rho * vel[d]; }
     }
     const double ke = 0.5 * rho * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
-    const double p = (GAMMA - 1.0) * (un[4] - ke);
-    if (p < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
+    const double pr = (GAMMA - 1.0) * (un[4] - ke);
+    if (pr < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
     if (nv > 5) un[5] = fmax(un[5], 0.0);
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
-    for (int v = 0; v < nv; ++v) Up[s * 8 + v] = un[v];
+    for (int v = 0; v < nv; ++v) Up[p * 8 + v] = un[v];
+    part[p] = sq_sum;
   }
   __syncthreads();
   // modal filter on the first five variables
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < S * nv; t += blockDim.x) {
-    const int s = t / nv, v = t % nv;
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) {
+    const int p = t / nv, v = t % nv;
+    const int b = p / S, s = p % S;
     double val;
     if (v < 5) {
       double acc = 0.0;
-      for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[j * 8 + v];
+      for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * 8 + v];
       val = acc;
     } else {
-      val = Up[s * 8 + v];
+      val = Up[p * 8 + v];
     }
-    a.Unext[(size_t)e * S * nv + t] = val;
+    a.Unext[(size_t)e0 * S * nv + t] = val;
   }
-  if (a.stage == 0) {
-    // deterministic per-cell partial of sum(dU/dt^2)
-    for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
-    if ((tid & 31) == 0) work[tid >> 5] = part;
-    __syncthreads();
-    if (tid == 0) {
-      double acc = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += work[w];
-      a.norm_part[e] = acc;
-    }
+  if (a.stage == 0 && tid < nc) {
+    double acc = 0.0;  // fixed order per cell: points ascending
+    for (int s = 0; s < S; ++s) acc += part[tid * S + s];
+    a.norm_part[e0 + tid] = acc;
   }
 }
 

@@ -21,9 +21,11 @@ def step_breakdown(solver):
     sst = solver.k is not None
     names = ["local_dt"] + (["sst_point", "sst_face", "sst_update"] if sst else [])
     for stg in range(3):
-        names += [f"grad{stg}", f"stage{stg}"]
+        names += [f"pre{stg}", f"face{stg}", f"cell{stg}"]
     names += ["norm"]
     per = dict(zip(names, vals))
-    stage_ms = [per[f"stage{i}"] for i in range(3) if f"stage{i}" in per]
+    face = [per[f"face{i}"] for i in range(3) if f"face{i}" in per]
+    cell = [per[f"cell{i}"] for i in range(3) if f"cell{i}" in per]
     return {"per_kernel_ms": per, "launches_per_step": int(nl.value),
-            "k_stage_ms_per_launch": sum(stage_ms) / len(stage_ms) if stage_ms else None}
+            "k_face_ms_per_launch": sum(face) / len(face) if face else None,
+            "k_cell_ms_per_launch": sum(cell) / len(cell) if cell else None}

@@ -90,24 +90,26 @@ def initial_state(case, spec):
     return U, k, om, nut, mu
 
 
-def algorithmic_stage_bytes(case, nv=7):
-    """Bytes one fused stage launch must move at minimum (each array once):
-    state in/out and step-start state, gradients, metrics, fine metrics, dt,
-    eddy viscosity, and per residual slot its interpolation matrix, normals
-    and record metadata."""
+def algorithmic_bytes(case, nv=7):
+    """Minimum bytes each per-stage kernel must move (every array once).
+
+    k_face: point fields of every cell (18 doubles per point), adjugates, the
+    interpolation matrices of every residual slot, normals, slot metadata, and
+    the jumps it writes (10 doubles per slot flux point).
+    k_cell: point fields, adjugates, fine-point adjugates, det, dt, current and
+    step-start state, the state it writes, and the jumps it reads."""
     N, S, Fn = int(case["n_cells"]), int(case["n_sps"]), int(case["n_fine"])
     P = case["true_normal"].shape[1]
     isb = case["is_boundary"].astype(bool)
     opr = case["owner_is_primary"].astype(bool)
     npr = case["neighbor_is_primary"].astype(bool)
-    own_slots = int(np.sum(opr))
-    nb_slots = int(np.sum(~isb & npr))
-    interior_own = int(np.sum(opr & ~isb))
-    mats = interior_own + nb_slots + int(np.sum(case["nb_src1_idx"][opr & ~isb] >= 0)) + \
-        int(np.sum(case["ow_src1_idx"][~isb & npr] >= 0))
-    slots = own_slots + nb_slots
-    per_cell = S * 8 * (3 * nv + 12 + 1 + 9 + 1 + 1) + Fn * 9 * 8
-    return N * per_cell + mats * P * S * 8 + slots * (P * 3 * 8 + 40)
+    slots = int(np.sum(opr)) + int(np.sum(~isb & npr))
+    mats = int(np.sum(opr & ~isb)) + int(np.sum(~isb & npr)) + \
+        int(np.sum(case["nb_src1_idx"][opr & ~isb] >= 0)) + int(np.sum(case["ow_src1_idx"][~isb & npr] >= 0))
+    jumps = slots * P * 10 * 8
+    face = N * S * 8 * (18 + 9) + mats * P * S * 8 + slots * (P * 3 * 8 + 24) + jumps
+    cell = N * S * 8 * (18 + 9 + 1 + 1 + 3 * nv) + N * Fn * 9 * 8 + jumps + slots * 4
+    return {"k_face": face, "k_cell": cell}
 
 
 def clocks_sampler(path):
@@ -230,7 +232,7 @@ def main():
     U, k, om, nut, mu = initial_state(case, spec)
     rho, u, p, *_ = flow_conditions()
     t_gen = time.perf_counter() - t_gen
-    alg_bytes = algorithmic_stage_bytes(case)
+    alg_bytes = algorithmic_bytes(case)
     s = B200FRSolver(case, turb_model_name="SST", mu_molecular=mu, rho_inf=rho, vel_inf=u, p_inf=p,
                      device=f"cuda:{local}")
     del case
@@ -296,14 +298,18 @@ def main():
         dist.all_reduce(ts, op=dist.ReduceOp.MAX)
     ms, ms_e2e = float(ts[0]), float(ts[1])
     value = world * dofs_per_step / (ms * 1e-3)
-    stage_ms = breakdown.get("k_stage_ms_per_launch")
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9 if stage_ms else None
+    kern_ms = {"k_face": breakdown.get("k_face_ms_per_launch"), "k_cell": breakdown.get("k_cell_ms_per_launch")}
+    dom = max(kern_ms, key=lambda k: kern_ms[k] or 0.0)
+    per_kernel = {k: {"ms_per_launch": kern_ms[k], "algorithmic_bytes": alg_bytes[k],
+                      "achieved_gbs": alg_bytes[k] / (kern_ms[k] * 1e-3) / 1e9 if kern_ms[k] else None}
+                  for k in kern_ms}
+    achieved = per_kernel[dom]["achieved_gbs"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -317,9 +323,9 @@ def main():
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
-                     "kernel": "k_stage (fused residual + RK stage)", "algorithmic_bytes_per_launch": alg_bytes,
+                     "kernel": dom, "algorithmic_bytes_per_launch": alg_bytes[dom], "per_kernel": per_kernel,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                     "fp64_note": "the plain FP64 form is FP64-pipe bound, not HBM bound"},
+                     "fp64_note": "the plain FP64 form is latency / FP64-pipe bound, not HBM bound"},
         "gpu_launches": breakdown.get("launches_per_step", 0) * args.steps,
         "breakdown_ms_per_step": breakdown.get("per_kernel_ms"),
         "device_bytes": s.device_bytes(),
