@@ -75,6 +75,7 @@ SIGNATURES = {
     "afr_device_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "afr_step_profile": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
+    "afr_rms_norm_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
     "afr_greedy_face_coloring": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, _P_I64, _P_I64, _P_U8, _P_I32]),
 }
 

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -303,7 +304,75 @@ int compute_dt(afr_handle* h, const double* U, const double* nut, double* dt, cu
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Allocation-free RMS norm.  Its per-block partial sums live in a fixed
+// file-scope device array instead of handle scratch, so the call needs no
+// cudaMalloc.  Every GPU that loads the library keeps these 32 KiB until exit.
+// ---------------------------------------------------------------------------
+constexpr int NOALLOC_PARTIALS = 4096;         // blocks, one partial each
+constexpr int NOALLOC_THREADS = 256;
+constexpr int64_t NOALLOC_CHUNK = 65536;       // elements summed per block
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_PARTIALS];
+
+namespace {
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[256] = {nullptr};        // per device ordinal
+
+__global__ void k_sumsq_chunks(const double* __restrict__ x, int64_t n, double* __restrict__ partials) {
+  __shared__ double sh[NOALLOC_THREADS];
+  const int64_t beg = (int64_t)blockIdx.x * NOALLOC_CHUNK;
+  const int64_t end = min(beg + NOALLOC_CHUNK, n);
+  double acc = 0.0;
+  for (int64_t i = beg + threadIdx.x; i < end; i += NOALLOC_THREADS) acc += x[i] * x[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = NOALLOC_THREADS / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+__global__ void k_rms_finish(const double* __restrict__ partials, int nb, int64_t n, double* out) {
+  __shared__ double sh[1024];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) acc += partials[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = n > 0 ? sqrt(sh[0]) / sqrt((double)n) : 0.0;
+}
+}  // namespace
+
 extern "C" {
+
+int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream) {
+  if (n < 0 || !out || (n > 0 && !x)) return AFR_EINVAL;
+  if (n > (int64_t)NOALLOC_PARTIALS * NOALLOC_CHUNK) return AFR_EINVAL;  // beyond the fixed scratch
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return AFR_ECUDA;
+  double* partials = nullptr;
+  {
+    // once per device, with that device current: the device address of the
+    // static array (its host-side name is only a stand-in)
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      if (cudaGetSymbolAddress((void**)&g_noalloc_ptr[dev], g_noalloc_partials) != cudaSuccess) {
+        g_noalloc_ptr[dev] = nullptr;
+        return AFR_ECUDA;
+      }
+    }
+    partials = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (int)((n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK);
+  if (nb > 0) k_sumsq_chunks<<<nb, NOALLOC_THREADS, 0, st>>>(x, n, partials);
+  k_rms_finish<<<1, 1024, 0, st>>>(partials, nb, n, out);
+  return cudaGetLastError() == cudaSuccess ? AFR_OK : AFR_ECUDA;
+}
 
 int afr_version(void) { return AFR_VERSION; }
 

@@ -172,6 +172,23 @@ int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double referen
 int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* owner_cell,
                              const int64_t* neighbor_cell, const uint8_t* is_boundary, int32_t* colors_out);
 
+/* RMS norm sqrt(sum(x^2) / n) of a device array x of n doubles, written to
+ * the device double *out, without allocating any memory.  No counterpart in
+ * the reference: it is the step's residual-norm reduction offered on its own
+ * for callers that may not allocate at call time -- code running while a CUDA
+ * graph is being captured (cudaMalloc is not a stream operation and breaks the
+ * capture), real-time step loops where an allocation would synchronise the
+ * device, and host applications that own all device memory through their own
+ * pool.  Its scratch is a fixed 32 KiB file-scope device array (4096 block
+ * partials); n may be at most 4096 * 65536 = 268,435,456, larger n returns
+ * AFR_EINVAL.  The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress, with the device current) and should come
+ * before any stream capture.  Every call shares the array: calls that overlap
+ * on the GPU (different streams, no ordering between them) race.  Each call
+ * writes every partial it reads, so nothing needs clearing between calls.
+ * The sum order is fixed for a given n, so results are bitwise repeatable. */
+int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream);
+
 /* Bytes of device memory the handle owns (tables + scratch). */
 int afr_device_bytes(const afr_handle* h, uint64_t* out);
 
