@@ -209,7 +209,7 @@ struct StepTimer {
 template <int S, int FN, int NP, int N1D>
 struct Launch {
   static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 2 : 1);
-  static size_t cell_smem() { return sizeof(double) * CellSmem<S, FN, CPB>::total; }
+  static size_t cell_smem() { return sizeof(double) * CellSmem<S, FN, CPB, NP>::total; }
   static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
     k_pre<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
     return cudaGetLastError();

@@ -92,6 +92,51 @@ __device__ void suppress_outliers(double* R, const double* Uref, int ldU, double
   __syncthreads();
 }
 
+// The same zeroing for the inviscid and viscous residuals of nc cells at once
+// (one rank pass, one threshold pass): block b < nc is sRi of cell b, block
+// nc + b is sRv of cell b; cell rows of the reference field at sU + b*S*8.
+// work >= 20 doubles per block.
+template <int S>
+__device__ void suppress_outliers_cells(double* sRi, double* sRv, const double* sU, int nc, bool visc, double* work) {
+  const int nb = nc * (visc ? 2 : 1);
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    const double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
+    const double x = fabs(R[s * 5 + v]);
+    int rank = 0;
+    for (int j = 0; j < S; ++j) {
+      const double y = fabs(R[j * 5 + v]);
+      rank += (y < x) || (y == x && j < s);
+    }
+    double* w = work + bb * 20;
+    if (S & 1) {
+      if (rank == S / 2) w[v] = x;
+    } else {
+      if (rank == S / 2 - 1) w[10 + v] = x;
+      if (rank == S / 2) w[15 + v] = x;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * 5; t += blockDim.x) {
+    const int bb = t / 5, v = t % 5;
+    double* w = work + bb * 20;
+    if (!(S & 1)) w[v] = 0.5 * (w[10 + v] + w[15 + v]);
+    const double* Ur = sU + (bb % nc) * S * 8;
+    double acc = 0.0;
+    for (int s = 0; s < S; ++s) acc += fabs(Ur[s * 8 + v]);
+    w[5 + v] = acc / S;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int bb = t / (S * 5), r = t % (S * 5), v = r % 5;
+    double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
+    const double* w = work + bb * 20;
+    const double ref = fmax(fmax(w[v], 1e-9 * w[5 + v]), 1e-300);
+    if (fabs(R[r]) > 1e4 * ref) R[r] = 0.0;
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // per-point pre-pass: PF (N,S,18) = primitive q(5) (no pressure floor,
 // core/fr_residual/inviscid.py:38-47), grads of u,v,w (9) and T (3)
@@ -185,6 +230,7 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
     const double* Er = ops.extrap + ((((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * NP + i) * S;
     const double* pf = PF + (size_t)e * S * PFW;
     const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
+#pragma unroll 3
     for (int s = 0; s < S; ++s) {
       const double w = __ldg(Er + s);
       double x[18];
@@ -218,16 +264,19 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
       const double* M = src == 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S
                                  : (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S;
       const double* pf = PF + (size_t)c * S * PFW;
+#pragma unroll 3
       for (int s = 0; s < S; ++s) {
         const double w = __ldg(M + s);
-        if (w == 0.0) continue;  // the reference skips zero weights (inviscid_kernel_colored.py:117-121)
+        // the reference skips zero weights (inviscid_kernel_colored.py:117-121):
+        // a zero weight adds exactly nothing, even next to a non-finite value
+        const bool nz = w != 0.0;
         double x[18];
         ld18(pf + s * PFW, x);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) ot[k] += w * x[k];
+        for (int k = 0; k < 5; ++k) ot[k] += nz ? w * x[k] : 0.0;
         if (visc) {
 #pragma unroll
-          for (int k = 0; k < 13; ++k) ot[5 + k] += w * x[5 + k];
+          for (int k = 0; k < 13; ++k) ot[5 + k] += nz ? w * x[5 + k] : 0.0;
         }
       }
     }
@@ -280,8 +329,9 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
 // core/time_integration/positivity.py:13-45, core/fr_solver/filter.py:29-42).
 // ---------------------------------------------------------------------------
 constexpr int CELL_THREADS = 256;
+constexpr int CELL_MAXSLOT = 6;  // slots per cell staged in shared memory (more: read from global)
 
-template <int S, int FN, int CPB>
+template <int S, int FN, int CPB, int NPMAX>
 struct CellSmem {
   static constexpr int oPF = 0;                    // CPB*S*18
   static constexpr int oAdj = oPF + CPB * S * PFW; // CPB*S*9
@@ -292,14 +342,16 @@ struct CellSmem {
   static constexpr int oQf = oRv + CPB * S * 5;    // CPB*FN*5
   static constexpr int oFt = oQf + CPB * FN * 5;   // CPB*FN*15
   static constexpr int oGt = oFt + CPB * FN * 15;  // CPB*S*15
-  static constexpr int work = oGt + CPB * S * 15;  // CPB*24
-  static constexpr int total = work + CPB * 24;
+  static constexpr int oJ = oGt + CPB * S * 15;    // staged jumps of the CTA's slots
+  static constexpr int oWp = oJ + CPB * CELL_MAXSLOT * NPMAX * 10;  // 2 halves of the W divergence
+  static constexpr int work = oWp + 2 * CPB * S * 5;  // CPB*2*20 (outliers) + 32
+  static constexpr int total = work + CPB * 40 + 32;
 };
 
 template <int S, int FN, int NP, int CPB>
-__global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces fc, StageArgs a,
+__global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces fc, StageArgs a,
                                                           const double* __restrict__ J) {
-  using L = CellSmem<S, FN, CPB>;
+  using L = CellSmem<S, FN, CPB, NP>;
   extern __shared__ double sm[];
   double* sPF = sm + L::oPF;
   double* sAdj = sm + L::oAdj;
@@ -323,6 +375,12 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces
   for (int t = tid; t < nc * S * 9; t += blockDim.x) sAdj[t] = g.adj[(size_t)e0 * S * 9 + t];
   for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
   for (int t = tid; t < nc * S; t += blockDim.x) sDet[t] = g.det[(size_t)e0 * S + t];
+  // the jumps of this CTA's slots are contiguous (slots are stored cell-major)
+  const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
+  const bool staged = (k_end - k_beg) <= CPB * CELL_MAXSLOT;
+  double* sJ = sm + L::oJ;
+  if (staged)
+    for (int t = tid; t < (k_end - k_beg) * NP * 10; t += blockDim.x) sJ[t] = J[(size_t)k_beg * NP * 10 + t];
   __syncthreads();
 
   // ---- Q at fine points (c2f) and viscous contravariant fluxes ----
@@ -368,16 +426,19 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces
         sFt[(t * 3 + m) * 5 + v] = am[m * 3 + 0] * F[0][v] + am[m * 3 + 1] * F[1][v] + am[m * 3 + 2] * F[2][v];
   }
   __syncthreads();
-  // ---- divergences: inviscid W (S x 3FN), viscous D3 (S x 3S) ----
+  // ---- divergences: inviscid W (S x 3FN) in two K halves, viscous D3 (S x 3S) ----
   {
-    const int n_i = S * 5, n_all = visc ? 2 * S * 5 : S * 5;
+    double* sWp = sm + L::oWp;  // [half][b][s*5+v]
+    constexpr int KH = FN * 3 / 2;  // first half [0, KH), second [KH, 3FN) (3FN is odd at P1)
+    const int n_w = 2 * S * 5, n_all = visc ? 3 * S * 5 : 2 * S * 5;
     for (int t = tid; t < n_all; t += blockDim.x) {
-      const bool inv = t < n_i;
-      const int u = inv ? t : t - n_i;
+      const bool inv = t < n_w;
+      const int u = inv ? t % (S * 5) : t - n_w;
+      const int half = inv ? t / (S * 5) : 0;
       const int s = u / 5, v = u % 5;
-      const int K = inv ? FN * 3 : S * 3;
-      const double* w = inv ? ops.W[ct] + (size_t)s * FN * 3 : ops.D3[ct] + (size_t)s * S * 3;
-      const double* X = inv ? sFt : sGt;
+      const int K = inv ? (half == 0 ? KH : FN * 3 - KH) : S * 3;
+      const double* w = inv ? ops.W[ct] + (size_t)s * FN * 3 + half * KH : ops.D3[ct] + (size_t)s * S * 3;
+      const double* X = inv ? sFt + half * KH * 5 : sGt;
       const int ldb = inv ? FN * 15 : S * 15;
       double acc[CPB];
 #pragma unroll
@@ -391,10 +452,14 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces
 #pragma unroll
       for (int b = 0; b < CPB; ++b)
         if (b < nc) {
-          const double dj = sDet[b * S + s];
-          if (inv) sRi[(b * S + s) * 5 + v] = -acc[b] / dj;
-          else sRv[(b * S + s) * 5 + v] = acc[b] / dj;
+          if (inv) sWp[(half * CPB + b) * S * 5 + u] = acc[b];
+          else sRv[(b * S + s) * 5 + v] = acc[b] / sDet[b * S + s];
         }
+    }
+    __syncthreads();
+    for (int t = tid; t < nc * S * 5; t += blockDim.x) {
+      const int b = t / (S * 5), u = t % (S * 5);
+      sRi[t] = -(sWp[b * S * 5 + u] + sWp[(CPB + b) * S * 5 + u]) / sDet[b * S + u / 5];
     }
   }
   __syncthreads();
@@ -409,7 +474,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces
       const int ax = (fl >> 2) & 3;
       const int fp = ops.dist_fp[ax * S + s];
       const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
-      const double* Jk = J + ((size_t)k * NP + fp) * 10;
+      const double* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : J + ((size_t)k * NP + fp) * 10;
       ci += -(gw * Jk[v]) / dj;
       if (visc) cv += (gw * Jk[5 + v]) / dj;
     }
@@ -417,10 +482,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) k_cell(Geom g, Ops ops, Faces
     if (visc) sRv[t] = sRv[t] + cv;
   }
   __syncthreads();
-  for (int b = 0; b < nc; ++b) {
-    suppress_outliers<S>(sRi + b * S * 5, sU + b * S * 8, 8, work);
-    if (visc) suppress_outliers<S>(sRv + b * S * 5, sU + b * S * 8, 8, work);
-  }
+  suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
 
   if (a.stage < 0) {
     for (int t = tid; t < nc * S * nv; t += blockDim.x) {
