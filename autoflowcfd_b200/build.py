@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libafr_b200.so")
-SOURCES = ["afr_api.cu"]
+SOURCES = ["afr_api.cu", "afr_tc_check.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

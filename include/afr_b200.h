@@ -189,6 +189,14 @@ int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* ow
  * The sum order is fixed for a given n, so results are bitwise repeatable. */
 int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream);
 
+/* Tensor-core self-check: D[128 x n] = A[128 x k] * B[n x k]^T on the
+ * calling device with tcgen05.mma, A and B row-major BF16 bit patterns and D
+ * row-major FP32, all device memory; 16 <= n, k <= 256, both multiples of 16.
+ * It runs the shared-memory layout, descriptors and bounded waits of the
+ * mixed-precision kernels on one CTA and synchronises the stream.  No
+ * counterpart in the reference (diagnostic for the mixed-precision form). */
+int afr_tc_check(int n, int k, const void* A, const void* B, float* D, void* stream);
+
 /* Bytes of device memory the handle owns (tables + scratch). */
 int afr_device_bytes(const afr_handle* h, uint64_t* out);
 
