@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libafr_b200.so")
 
 AFR_OK, AFR_EINVAL, AFR_ENOMEM, AFR_ECUDA, AFR_ENONFINITE, AFR_EUNSUPPORTED, AFR_EINDEX = range(7)
 AFR_TURB_NONE, AFR_TURB_SST = 0, 1
+AFR_PREC_FP64, AFR_PREC_MIXED = 0, 1
 
 _P_D = ctypes.POINTER(ctypes.c_double)
 _P_I64 = ctypes.POINTER(ctypes.c_int64)
@@ -52,7 +53,7 @@ class AfrMeshDesc(ctypes.Structure):
 class AfrParams(ctypes.Structure):
     _fields_ = [
         ("n_vars", ctypes.c_int32), ("turb", ctypes.c_int32), ("inviscid_only", ctypes.c_int32),
-        ("reserved", ctypes.c_int32), ("mu", ctypes.c_double), ("rho_inf", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("mu", ctypes.c_double), ("rho_inf", ctypes.c_double),
         ("vel_inf", ctypes.c_double), ("p_inf", ctypes.c_double), ("global_dt_factor", ctypes.c_double),
     ]
 
@@ -116,7 +117,8 @@ def greedy_face_coloring(owner, neighbor, is_boundary, n_cells):
 
 def check(status, handle=None):
     if status != AFR_OK:
-        msg = LIB.afr_last_error(handle).decode() if handle else ""
+        # with no handle, afr_last_error reports the last failed afr_create of this thread
+        msg = LIB.afr_last_error(handle).decode()
         raise AfrError(status, msg)
 
 

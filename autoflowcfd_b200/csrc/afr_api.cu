@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/afr_b200.h"
+#include "afr_mixed.cuh"
 #include "afr_sst.cuh"
 
 using namespace afr;
@@ -48,12 +49,20 @@ struct afr_handle {
   int n_cd_faces = 0;
   double* cd_part = nullptr;  // (n_cd_faces, 6)
   unsigned* status = nullptr;
+  // mixed-precision form (prec == AFR_PREC_MIXED)
+  int prec = AFR_PREC_FP64;
+  MxOps mo{};
+  MxFace mf{};
+  MxBuf mb{};
+  int mx_pre_blocks = 0, mx_cell_blocks = 0;  // resident CTAs of the persistent kernels
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   std::string err;
 };
 
 namespace {
+
+thread_local std::string g_create_error;  // message of the last failed afr_create on this thread
 
 int fail(afr_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -238,6 +247,90 @@ struct Launch {
     }
     return cudaGetLastError();
   }
+  // ---- mixed-precision form ----
+  static constexpr int MXC = S <= 27 ? 24 : 16;            // cells per volume-kernel tile
+  static constexpr int MXU = S <= 8 ? 16 : (S <= 27 ? 4 : 2);  // cells per update-kernel CTA
+  static size_t mx_pre_smem() { return MxPreSmem<S, NP>::total; }
+  static size_t mx_vol_smem() { return MxVolSmem<S, FN, MXC>::total; }
+  static size_t mx_upd_smem() { return MxUpdSmem<S, NP, MXU>::total; }
+  // resident CTAs per SM of the persistent kernels, capped by tensor memory (512 columns per SM)
+  static cudaError_t mx_grids(afr_handle* h) {
+    int dev = 0, sms = 0, bp = 0, bc = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_pre<S, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_pre_smem());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_vol<S, FN, MXC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_vol_smem());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_update<S, NP, MXU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)mx_upd_smem());
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_mx_pre<S, NP>, MX_THREADS, mx_pre_smem());
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, k_mx_vol<S, FN, MXC>, MX_VOL_THREADS, mx_vol_smem());
+    if (e != cudaSuccess) return e;
+    bp = std::min(bp, 512 / MxPreSmem<S, NP>::NCOL);
+    bc = std::min(bc, 512 / MxVolSmem<S, FN, MXC>::NCOL);
+    if (bp < 1 || bc < 1) return cudaErrorInvalidConfiguration;
+    h->mx_pre_blocks = bp * sms;
+    h->mx_cell_blocks = bc * sms;
+    return cudaSuccess;
+  }
+  static int n_ranges(const afr_handle* h) { return (h->n_prism > 0 ? 1 : 0) + (h->N > h->n_prism ? 1 : 0); }
+  static cudaError_t mx_pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n <= 0) continue;
+      const int tiles = (n + MX_PRE_CELLS - 1) / MX_PRE_CELLS;
+      k_mx_pre<S, NP><<<std::min(tiles, h->mx_pre_blocks), MX_THREADS, mx_pre_smem(), st>>>(
+          h->g, h->mo, h->mb, U, h->nv, nut, grads ? 1 : 0, ranges[r], ranges[r + 1], h->status);
+    }
+    return cudaGetLastError();
+  }
+  static cudaError_t mx_stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm) {
+    const int nt = h->slots.n * NP;
+    if (nt > 0)
+      k_mx_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell,
+                                                         (float)h->prm.mu, a.inviscid_only ? 0 : 1);
+    if (tm) tm->mark(st);
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n <= 0) continue;
+      const int tiles = (n + MXC - 1) / MXC;
+      k_mx_vol<S, FN, MXC><<<std::min(tiles, h->mx_cell_blocks), MX_VOL_THREADS, mx_vol_smem(), st>>>(
+          h->g, h->mo, a.Ucur, h->nv, a.inviscid_only, (float)h->prm.mu, h->mb.PFm, h->mb.RV, ranges[r],
+          ranges[r + 1], h->status);
+    }
+    if (tm) tm->mark(st);
+    a.N = h->N;
+    a.slot_flags = h->slots.flags;
+    for (int r = 0; r < 2; ++r) {
+      a.cell_base = ranges[r];
+      a.cell_end = ranges[r + 1];
+      const int n = a.cell_end - a.cell_base;
+      if (n <= 0) continue;
+      k_mx_update<S, NP, MXU><<<(n + MXU - 1) / MXU, MX_UPD_THREADS, mx_upd_smem(), st>>>(h->g, h->ops, h->fc, a,
+                                                                                        h->mb.RV, h->mb.Jm);
+    }
+    return cudaGetLastError();
+  }
+  // one residual evaluation of either form: pre-pass, face kernel, cell kernel;
+  // adds the number of kernel launches to *nl
+  static cudaError_t eval(afr_handle* h, StageArgs a, const double* U, const double* nut, bool grads,
+                          cudaStream_t st, StepTimer* tm = nullptr, int* nl = nullptr) {
+    const bool mx = h->prec == AFR_PREC_MIXED;
+    cudaError_t r = mx ? mx_pre(h, U, nut, grads, st) : pre(h, U, nut, grads, st);
+    if (r != cudaSuccess) return r;
+    if (tm) tm->mark(st);
+    if (nl) *nl += (mx ? n_ranges(h) : 1) + (h->slots.n > 0 ? 1 : 0) + (mx ? 2 : 1) * n_ranges(h);
+    if (mx) return mx_stage(h, a, st, tm);
+    r = stage(h, a, st, tm);
+    if (tm) tm->mark(st);  // the plain form has no separate update kernel: an empty interval
+    return r;
+  }
   static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
     k_sst_point<S><<<h->N, 128, 0, st>>>(h->g, h->ops, a);
     if (tm) tm->mark(st);
@@ -257,6 +350,35 @@ struct Launch {
   }
 };
 
+// ---- host-side BF16 hi+lo operator images for the mixed form ----
+uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even (operators are finite)
+  return (uint16_t)(u >> 16);
+}
+float bf16_value(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+// R x K matrix -> [hi | lo] images in the K-major canonical layout
+template <class Get>
+std::vector<uint16_t> kmajor_image(int R, int K, Get get) {
+  std::vector<uint16_t> img(2 * (size_t)R * K, 0);
+  for (int r = 0; r < R; ++r)
+    for (int k = 0; k < K; ++k) {
+      const double x = get(r, k);
+      const uint16_t hi = bf16_bits((float)x);
+      const uint16_t lo = bf16_bits((float)(x - (double)bf16_value(hi)));
+      const size_t idx = ((size_t)(k >> 3) * R + r) * 8 + (k & 7);
+      img[idx] = hi;
+      img[(size_t)R * K + idx] = lo;
+    }
+  return img;
+}
+
 template <class Fn>
 cudaError_t dispatch(afr_handle* h, Fn&& fn) {
   switch (h->order) {
@@ -274,6 +396,7 @@ int check_status(afr_handle* h, cudaStream_t st) {
   if (e != cudaSuccess) return cuda_fail(h, e, "status read");
   if (s & DS_BAD_INDEX) return fail(h, AFR_EINDEX, "kernel saw an out-of-range table index");
   if (s & DS_NONFINITE) return fail(h, AFR_ENONFINITE, "non-finite value in the state");
+  if (s & DS_TC_TIMEOUT) return fail(h, AFR_ECUDA, "a tensor-core completion wait timed out");
   return AFR_OK;
 }
 
@@ -389,7 +512,7 @@ const char* afr_status_string(int s) {
   return "unknown status";
 }
 
-const char* afr_last_error(const afr_handle* h) { return h ? h->err.c_str() : "null handle"; }
+const char* afr_last_error(const afr_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
 int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* owner, const int64_t* neighbor,
                              const uint8_t* is_boundary, int32_t* colors) {
@@ -445,14 +568,132 @@ int afr_destroy(afr_handle* h) {
   return AFR_OK;
 }
 
+// Tables of the mixed-precision form: operator images, metric divergence,
+// interior-penalty lengths, per-slot adjugate rows and the conforming-face
+// match of the other side's face point.
+static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<double>* Wkeep, cudaStream_t st) {
+  const int S = h->S, Fn = h->Fn, P = h->P;
+  const size_t N = h->N;
+  if (h->order == 3 && !h->prm.inviscid_only)
+    return fail(h, AFR_EUNSUPPORTED, "the mixed form has viscous terms up to P2");
+  const int Sq = pad16(S), Fq = pad16(Fn);
+  int rc;
+  // Conditioning: a contraction accumulated in FP32 carries an absolute error
+  // of about 2^-24 * (row l1 norm of the operator) * |x|.  The collapsed-tet
+  // operators grow with the order (row l1 norms ~2e4 at P1, ~2e11 at P2 and
+  // ~2e8 at P3 for the reference's nodal sets), so those cell types stay in
+  // the FP64 form.
+  constexpr double MAX_ROW_L1 = 1e6;
+  for (int t = 0; t < 2; ++t) {
+    if (Wkeep[t].empty()) continue;
+    auto row_l1 = [](const double* a, size_t rows, size_t cols, size_t rs, size_t cs) {
+      double mx = 0.0;
+      for (size_t r = 0; r < rows; ++r) {
+        double acc = 0.0;
+        for (size_t c = 0; c < cols; ++c) acc += std::fabs(a[r * rs + c * cs]);
+        mx = std::max(mx, acc);
+      }
+      return mx;
+    };
+    double l1 = row_l1(Wkeep[t].data(), S, 3 * Fn, 3 * Fn, 1);
+    l1 = std::max(l1, row_l1(m->c2f[t], Fn, S, S, 1));
+    for (int mm = 0; mm < 3; ++mm) l1 = std::max(l1, row_l1(m->D_3d[t] + mm, S, S, 3 * S, 3));
+    l1 = std::max(l1, row_l1(m->boundary_extrap + (size_t)t * 6 * P * S, 6 * P, S, S, 1));
+    if (l1 > MAX_ROW_L1)
+      return fail(h, AFR_EUNSUPPORTED,
+                  std::string("the mixed form needs operators with row l1 norms <= 1e6 (FP32 accumulation); the ") +
+                      (t == 0 ? "prism" : "tet") + " operators of this order reach " + std::to_string(l1));
+  }
+  for (int t = 0; t < 2; ++t) {
+    if (Wkeep[t].empty()) continue;
+    const double* c2f = m->c2f[t];
+    const double* D3 = m->D_3d[t];
+    const double* Wt = Wkeep[t].data();
+    const double* ex = m->boundary_extrap;
+    auto i_c2f = kmajor_image(Fq, Sq, [&](int i, int s) { return (i < Fn && s < S) ? c2f[i * S + s] : 0.0; });
+    auto i_W = kmajor_image(Sq, 3 * Fq, [&](int s, int k) {
+      const int mm = k / Fq, i = k % Fq;
+      return (s < S && i < Fn) ? Wt[(size_t)s * 3 * Fn + i * 3 + mm] : 0.0;
+    });
+    auto i_D3 = kmajor_image(Sq, 3 * Sq, [&](int s, int k) {
+      const int mm = k / Sq, j = k % Sq;
+      return (s < S && j < S) ? D3[(size_t)s * 3 * S + j * 3 + mm] : 0.0;
+    });
+    auto i_D3g = kmajor_image(3 * Sq, Sq, [&](int n, int j) {
+      const int mm = n / Sq, s = n % Sq;
+      return (s < S && j < S) ? D3[(size_t)s * 3 * S + j * 3 + mm] : 0.0;
+    });
+    auto i_E = kmajor_image(128, Sq, [&](int fp, int s) {
+      if (fp >= 6 * P || s >= S) return 0.0;
+      const int a = fp / P, i = fp % P;
+      return ex[(((size_t)t * 3 + a / 2) * 2 + a % 2) * P * S + (size_t)i * S + s];
+    });
+    uint16_t *d_c2f, *d_W, *d_D3, *d_D3g, *d_E;
+    if ((rc = upload(h, &d_c2f, i_c2f.data(), i_c2f.size(), st)) || (rc = upload(h, &d_W, i_W.data(), i_W.size(), st)) ||
+        (rc = upload(h, &d_D3, i_D3.data(), i_D3.size(), st)) ||
+        (rc = upload(h, &d_D3g, i_D3g.data(), i_D3g.size(), st)) || (rc = upload(h, &d_E, i_E.data(), i_E.size(), st)))
+      return rc;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(h, AFR_ECUDA, "operator image upload");
+    h->mo.c2f[t] = d_c2f;
+    h->mo.W[t] = d_W;
+    h->mo.D3[t] = d_D3;
+    h->mo.D3g[t] = d_D3g;
+    h->mo.E[t] = d_E;
+  }
+  double *md, *hc;
+  if ((rc = dalloc(h, &md, N * S * 3)) || (rc = dalloc(h, &hc, N))) return rc;
+  h->mo.MD = md;
+  h->mo.hcell = hc;
+  const int FW = h->order <= 2 ? 18 : 5;
+  float *xf, *pfm, *jm;
+  const size_t ns = h->slots.n;
+  if ((rc = dalloc(h, &xf, N * FW * 6 * P)) || (rc = dalloc(h, &pfm, N * S * 20)) || (rc = dalloc(h, &jm, ns * P * 10)))
+    return rc;
+  float* rv;
+  if ((rc = dalloc(h, &rv, N * S * 10))) return rc;
+  h->mb = MxBuf{xf, pfm, jm, rv, FW};
+  float4* arow;
+  uint8_t* ofp;
+  if ((rc = dalloc(h, &arow, ns * P)) || (rc = dalloc(h, &ofp, ns * P))) return rc;
+  h->mf = MxFace{arow, ofp};
+  cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+  cudaError_t e = dispatch(h, [&](auto L) -> cudaError_t {
+    using LL = decltype(L);
+    const size_t nmd = N * S * 3;
+    switch (h->order) {
+      case 1: k_mx_md<8, 27><<<(unsigned)((nmd + 255) / 256), 256, 0, st>>>(h->g, h->ops, md);
+              k_mx_hcell<8><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(h->g, hc);
+              if (ns) k_mx_match<8, 4><<<(unsigned)((ns * 4 + 127) / 128), 128, 0, st>>>(h->g, h->ops, h->fc, h->slots, arow, ofp, 1e-6);
+              break;
+      case 2: k_mx_md<27, 64><<<(unsigned)((nmd + 255) / 256), 256, 0, st>>>(h->g, h->ops, md);
+              k_mx_hcell<27><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(h->g, hc);
+              if (ns) k_mx_match<27, 9><<<(unsigned)((ns * 9 + 127) / 128), 128, 0, st>>>(h->g, h->ops, h->fc, h->slots, arow, ofp, 1e-6);
+              break;
+      default: k_mx_md<64, 64><<<(unsigned)((nmd + 255) / 256), 256, 0, st>>>(h->g, h->ops, md);
+              k_mx_hcell<64><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(h->g, hc);
+              if (ns) k_mx_match<64, 16><<<(unsigned)((ns * 16 + 127) / 128), 128, 0, st>>>(h->g, h->ops, h->fc, h->slots, arow, ofp, 1e-6);
+              break;
+    }
+    cudaError_t r = cudaGetLastError();
+    return r != cudaSuccess ? r : LL::mx_grids(h);
+  });
+  if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
+  unsigned s = 0;
+  e = cudaMemcpyAsync(&s, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
+  cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+  h->prec = AFR_PREC_MIXED;
+  return AFR_OK;
+}
+
 int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_handle** out) {
   if (!m || !prm || !out) return AFR_EINVAL;
   *out = nullptr;
   afr_handle* h = new afr_handle();
   auto bail = [&](int rc) {
-    std::string e = h->err;
+    g_create_error = h->err;
     afr_destroy(h);
-    (void)e;
     return rc;
   };
   cudaStream_t st = (cudaStream_t)stream;
@@ -467,6 +708,8 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   h->nv = prm->n_vars;
   const int n1d = h->order + 1;
   if (h->order < 1 || h->order > 3) return bail(fail(h, AFR_EUNSUPPORTED, "order must be 1, 2 or 3"));
+  if (prm->precision != AFR_PREC_FP64 && prm->precision != AFR_PREC_MIXED)
+    return bail(fail(h, AFR_EINVAL, "precision must be AFR_PREC_FP64 or AFR_PREC_MIXED"));
   const int fine_1d = std::min(2 * h->order, 3) + 1;
   if (h->S != n1d * n1d * n1d || h->P != n1d * n1d || h->Fn != fine_1d * fine_1d * fine_1d)
     return bail(fail(h, AFR_EINVAL, "n_sps/n_fp/n_fine inconsistent with order"));
@@ -542,6 +785,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   h->g = Geom{h->N, h->n_prism, det, inv, adj, adjf, vol, mfs, wd};
 
   // ---- operators ----
+  std::vector<double> Wkeep[2];
   for (int t = 0; t < 2; ++t) {
     const bool present = t == 0 ? h->n_prism > 0 : h->N > h->n_prism;
     if (!present) continue;
@@ -571,6 +815,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload(h, &wdev, Wh.data(), Wh.size(), st))) return bail(rc);
     cudaStreamSynchronize(st);
     h->ops.W[t] = wdev;
+    Wkeep[t] = Wh;
     h->ops.D3[t] = d3;
     h->ops.D3g[t] = d3g;
     h->ops.c2f[t] = c2f;
@@ -760,6 +1005,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = dalloc(h, &h->pt, N * S * 5))) return bail(rc);
     if ((rc = dalloc(h, &h->cfp, F * P * 4))) return bail(rc);
   }
+  if (prm->precision == AFR_PREC_MIXED && (rc = mixed_setup(h, m, Wkeep, st))) return bail(rc);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "afr_create"));
   *out = h;
@@ -774,10 +1020,7 @@ int afr_inviscid_residual(afr_handle* h, const double* U, double* R, void* strea
   a.inviscid_only = 1;
   a.stage = -1;
   a.Rinv = R;
-  cudaError_t e = dispatch(h, [&](auto L) {
-    cudaError_t r = L.pre(h, U, nullptr, false, st);
-    return r != cudaSuccess ? r : L.stage(h, a, st);
-  });
+  cudaError_t e = dispatch(h, [&](auto L) { return L.eval(h, a, U, nullptr, false, st); });
   if (e != cudaSuccess) return cuda_fail(h, e, "inviscid residual");
   return check_status(h, st);
 }
@@ -791,10 +1034,7 @@ int afr_viscous_residual(afr_handle* h, const double* U, const double* nu_t, dou
   a.stage = -1;
   a.nut = nu_t;
   a.Rvisc = R;
-  cudaError_t e = dispatch(h, [&](auto L) {
-    cudaError_t r = L.pre(h, U, nu_t, true, st);
-    return r != cudaSuccess ? r : L.stage(h, a, st);
-  });
+  cudaError_t e = dispatch(h, [&](auto L) { return L.eval(h, a, U, nu_t, true, st); });
   if (e != cudaSuccess) return cuda_fail(h, e, "viscous residual");
   return check_status(h, st);
 }
@@ -840,10 +1080,6 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
     const double* cur[3] = {U, h->Ua, h->Ub};
     double* nxt[3] = {h->Ua, h->Ub, U};
     for (int stg = 0; stg < 3; ++stg) {
-      r = L.pre(h, cur[stg], sst ? nu_t : nullptr, visc, st);
-      nl += 1;
-      if (r != cudaSuccess) return r;
-      if (tm) tm->mark(st);
       StageArgs a = base_args(h);
       a.Ucur = cur[stg];
       a.U0 = U;
@@ -852,8 +1088,7 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
       a.dt = h->dt;
       a.norm_part = h->norm_part;
       a.stage = stg;
-      r = L.stage(h, a, st, tm);
-      nl += 2;
+      r = L.eval(h, a, cur[stg], sst ? nu_t : nullptr, visc, st, tm, &nl);
       if (tm) tm->mark(st);
       if (r != cudaSuccess) return r;
     }

@@ -24,7 +24,12 @@ constexpr double C_IP = 4.0;
 enum BcType : int32_t { BC_WALL = 0, BC_FARFIELD = 1, BC_INLET = 2, BC_OUTLET = 3, BC_SYMMETRY = 4 };
 
 // Status word bits written by kernels instead of trapping (host reads them).
-enum DevStatus : uint32_t { DS_OK = 0u, DS_BAD_INDEX = 1u, DS_NONFINITE = 2u };
+enum DevStatus : uint32_t {
+  DS_OK = 0u,
+  DS_BAD_INDEX = 1u,
+  DS_NONFINITE = 2u,
+  DS_TC_TIMEOUT = 4u      // a tensor-core completion wait ran out (mixed form)
+};
 
 // Per-cell-type operator set (index 0 = prism, 1 = tet), all row-major doubles.
 struct Ops {
@@ -98,81 +103,88 @@ struct Bc {
 // ---------------------------------------------------------------------------
 // pointwise physics
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void euler_flux(const double q[5], double F[3][5]) {
-  const double rho = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
-  const double rs = fmax(rho, 1e-10);
-  const double ke = 0.5 * (u * u + v * v + w * w);
-  const double e_int = p / ((GAMMA - 1.0) * rs);
-  const double rhoE = rho * (e_int + ke);
-  const double H = (rhoE + p) / rs;
-  const double mf0 = rho * u, mf1 = rho * v, mf2 = rho * w;
+// The pointwise functions are templates on the real type T: the FP64 path
+// instantiates them with double (every literal is converted with T(..), so the
+// double instantiation is the plain double expression); the mixed-precision
+// form instantiates them with float.
+template <class T>
+__device__ __forceinline__ void euler_flux(const T q[5], T F[3][5]) {
+  const T rho = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
+  const T rs = fmax(rho, T(1e-10));
+  const T ke = T(0.5) * (u * u + v * v + w * w);
+  const T e_int = p / (T(GAMMA - 1.0) * rs);
+  const T rhoE = rho * (e_int + ke);
+  const T H = (rhoE + p) / rs;
+  const T mf0 = rho * u, mf1 = rho * v, mf2 = rho * w;
   F[0][0] = mf0; F[0][1] = mf0 * u + p; F[0][2] = mf0 * v;     F[0][3] = mf0 * w;     F[0][4] = rho * H * u;
   F[1][0] = mf1; F[1][1] = mf1 * u;     F[1][2] = mf1 * v + p; F[1][3] = mf1 * w;     F[1][4] = rho * H * v;
   F[2][0] = mf2; F[2][1] = mf2 * u;     F[2][2] = mf2 * v;     F[2][3] = mf2 * w + p; F[2][4] = rho * H * w;
 }
 
-__device__ __forceinline__ double sq(double x) { return x * x; }
+template <class T>
+__device__ __forceinline__ T sq(T x) { return x * x; }
 
-__device__ __forceinline__ void ausm_up(const double qL[5], const double qR[5], const double n[3], double out[5]) {
-  const double alpha = 0.1875, beta = 0.5, Kp = 0.25, Ku = 0.75, sigma_p = 1.0, ma_ref = 0.1;
-  const double rhoL = fmax(qL[0], 1e-6), rhoR = fmax(qR[0], 1e-6);
-  const double pL = fmax(qL[4], 10.0), pR = fmax(qR[4], 10.0);
-  const double uL = qL[1], vL = qL[2], wL = qL[3];
-  const double uR = qR[1], vR = qR[2], wR = qR[3];
-  const double unL = uL * n[0] + vL * n[1] + wL * n[2];
-  const double unR = uR * n[0] + vR * n[1] + wR * n[2];
-  const double aL = sqrt(fmax(GAMMA * pL / rhoL, 1e-10));
-  const double aR = sqrt(fmax(GAMMA * pR / rhoR, 1e-10));
-  const double ML = unL / fmax(aL, 1e-10);
-  const double MR = unR / fmax(aR, 1e-10);
-  const double a_half = 0.5 * (aL + aR);
-  const double rho_half = 0.5 * (rhoL + rhoR);
-  const double Mbar2 = (sq(unL) + sq(unR)) / (2.0 * sq(a_half));
-  const double M0 = fmin(1.0, fmax(Mbar2, ma_ref * ma_ref));
-  double fa = sqrt(M0) * (2.0 - sqrt(M0));
-  fa = fmax(fa, 1e-6);
-  const double mp = (fabs(ML) >= 1.0) ? 0.5 * (ML + fabs(ML)) : 0.25 * sq(ML + 1.0) + alpha * sq(sq(ML) - 1.0);
-  const double mm = (fabs(MR) >= 1.0) ? 0.5 * (MR - fabs(MR)) : -0.25 * sq(MR - 1.0) - alpha * sq(sq(MR) - 1.0);
-  const double M_half = mp + mm;
-  const double Mp = -(Kp / fa) * fmax(1.0 - sigma_p * Mbar2, 0.0) * (pR - pL) / (rho_half * sq(a_half));
-  const double mdot = 0.5 * (rhoL * aL + rhoR * aR) * (M_half + Mp);
-  const double sgnL = (ML > 0.0) ? 1.0 : ((ML < 0.0) ? -1.0 : 0.0);
-  const double sgnR = (MR > 0.0) ? 1.0 : ((MR < 0.0) ? -1.0 : 0.0);
-  const double PpL = (fabs(ML) >= 1.0) ? 0.5 * (1.0 + sgnL)
-                                        : 0.25 * (sq(ML + 1.0) * (2.0 - ML) + beta * ML * sq(sq(ML) - 1.0));
-  const double PmR = (fabs(MR) >= 1.0) ? 0.5 * (1.0 - sgnR)
-                                        : 0.25 * (sq(MR - 1.0) * (2.0 + MR) - beta * MR * sq(sq(MR) - 1.0));
-  const double p_half = PpL * pL + PmR * pR - Ku * PpL * PmR * (rhoL + rhoR) * fa * a_half * (unR - unL);
-  const bool up = mdot >= 0.0;
+template <class T>
+__device__ __forceinline__ void ausm_up(const T qL[5], const T qR[5], const T n[3], T out[5]) {
+  const T alpha = T(0.1875), beta = T(0.5), Kp = T(0.25), Ku = T(0.75), sigma_p = T(1.0), ma_ref = T(0.1);
+  const T rhoL = fmax(qL[0], T(1e-6)), rhoR = fmax(qR[0], T(1e-6));
+  const T pL = fmax(qL[4], T(10.0)), pR = fmax(qR[4], T(10.0));
+  const T uL = qL[1], vL = qL[2], wL = qL[3];
+  const T uR = qR[1], vR = qR[2], wR = qR[3];
+  const T unL = uL * n[0] + vL * n[1] + wL * n[2];
+  const T unR = uR * n[0] + vR * n[1] + wR * n[2];
+  const T aL = sqrt(fmax(T(GAMMA) * pL / rhoL, T(1e-10)));
+  const T aR = sqrt(fmax(T(GAMMA) * pR / rhoR, T(1e-10)));
+  const T ML = unL / fmax(aL, T(1e-10));
+  const T MR = unR / fmax(aR, T(1e-10));
+  const T a_half = T(0.5) * (aL + aR);
+  const T rho_half = T(0.5) * (rhoL + rhoR);
+  const T Mbar2 = (sq(unL) + sq(unR)) / (T(2.0) * sq(a_half));
+  const T M0 = fmin(T(1.0), fmax(Mbar2, ma_ref * ma_ref));
+  T fa = sqrt(M0) * (T(2.0) - sqrt(M0));
+  fa = fmax(fa, T(1e-6));
+  const T mp = (fabs(ML) >= T(1.0)) ? T(0.5) * (ML + fabs(ML)) : T(0.25) * sq(ML + T(1.0)) + alpha * sq(sq(ML) - T(1.0));
+  const T mm = (fabs(MR) >= T(1.0)) ? T(0.5) * (MR - fabs(MR)) : -T(0.25) * sq(MR - T(1.0)) - alpha * sq(sq(MR) - T(1.0));
+  const T M_half = mp + mm;
+  const T Mp = -(Kp / fa) * fmax(T(1.0) - sigma_p * Mbar2, T(0.0)) * (pR - pL) / (rho_half * sq(a_half));
+  const T mdot = T(0.5) * (rhoL * aL + rhoR * aR) * (M_half + Mp);
+  const T sgnL = (ML > T(0.0)) ? T(1.0) : ((ML < T(0.0)) ? T(-1.0) : T(0.0));
+  const T sgnR = (MR > T(0.0)) ? T(1.0) : ((MR < T(0.0)) ? T(-1.0) : T(0.0));
+  const T PpL = (fabs(ML) >= T(1.0)) ? T(0.5) * (T(1.0) + sgnL)
+                                     : T(0.25) * (sq(ML + T(1.0)) * (T(2.0) - ML) + beta * ML * sq(sq(ML) - T(1.0)));
+  const T PmR = (fabs(MR) >= T(1.0)) ? T(0.5) * (T(1.0) - sgnR)
+                                     : T(0.25) * (sq(MR - T(1.0)) * (T(2.0) + MR) - beta * MR * sq(sq(MR) - T(1.0)));
+  const T p_half = PpL * pL + PmR * pR - Ku * PpL * PmR * (rhoL + rhoR) * fa * a_half * (unR - unL);
+  const bool up = mdot >= T(0.0);
   out[0] = mdot;
   out[1] = mdot * (up ? uL : uR) + p_half * n[0];
   out[2] = mdot * (up ? vL : vR) + p_half * n[1];
   out[3] = mdot * (up ? wL : wR) + p_half * n[2];
-  const double hL = GAMMA / (GAMMA - 1.0) * pL / rhoL + 0.5 * (sq(uL) + sq(vL) + sq(wL));
-  const double hR = GAMMA / (GAMMA - 1.0) * pR / rhoR + 0.5 * (sq(uR) + sq(vR) + sq(wR));
+  const T hL = T(GAMMA / (GAMMA - 1.0)) * pL / rhoL + T(0.5) * (sq(uL) + sq(vL) + sq(wL));
+  const T hR = T(GAMMA / (GAMMA - 1.0)) * pR / rhoR + T(0.5) * (sq(uR) + sq(vR) + sq(wR));
   out[4] = mdot * (up ? hL : hR);
 }
 
 // gv[a*3+b] = d u_a / d x_b, gT[3], viscous flux G (3,5)
-__device__ __forceinline__ void viscous_flux(const double q[5], const double gv[9], const double gT[3], double mu,
-                                             double mu_t, double G[3][5]) {
-  const double mt = mu + mu_t;
-  const double S00 = gv[0], S11 = gv[4], S22 = gv[8];
-  const double S01 = 0.5 * (gv[1] + gv[3]);
-  const double S02 = 0.5 * (gv[2] + gv[6]);
-  const double S12 = 0.5 * (gv[5] + gv[7]);
-  const double div = gv[0] + gv[4] + gv[8];
-  const double lam = -2.0 / 3.0 * mt;
-  const double t00 = 2.0 * mt * S00 + lam * div;
-  const double t11 = 2.0 * mt * S11 + lam * div;
-  const double t22 = 2.0 * mt * S22 + lam * div;
-  const double t01 = 2.0 * mt * S01, t02 = 2.0 * mt * S02, t12 = 2.0 * mt * S12;
-  const double cp = GAMMA * R_AIR / (GAMMA - 1.0);
-  const double k = mu * cp / PR + mu_t * cp / PR_T;
-  const double u = q[1], v = q[2], w = q[3];
-  G[0][0] = 0.0; G[0][1] = t00; G[0][2] = t01; G[0][3] = t02;
-  G[1][0] = 0.0; G[1][1] = t01; G[1][2] = t11; G[1][3] = t12;
-  G[2][0] = 0.0; G[2][1] = t02; G[2][2] = t12; G[2][3] = t22;
+template <class T>
+__device__ __forceinline__ void viscous_flux(const T q[5], const T gv[9], const T gT[3], T mu, T mu_t, T G[3][5]) {
+  const T mt = mu + mu_t;
+  const T S00 = gv[0], S11 = gv[4], S22 = gv[8];
+  const T S01 = T(0.5) * (gv[1] + gv[3]);
+  const T S02 = T(0.5) * (gv[2] + gv[6]);
+  const T S12 = T(0.5) * (gv[5] + gv[7]);
+  const T div = gv[0] + gv[4] + gv[8];
+  const T lam = T(-2.0 / 3.0) * mt;
+  const T t00 = T(2.0) * mt * S00 + lam * div;
+  const T t11 = T(2.0) * mt * S11 + lam * div;
+  const T t22 = T(2.0) * mt * S22 + lam * div;
+  const T t01 = T(2.0) * mt * S01, t02 = T(2.0) * mt * S02, t12 = T(2.0) * mt * S12;
+  const T cp = T(GAMMA * R_AIR / (GAMMA - 1.0));
+  const T k = mu * cp / T(PR) + mu_t * cp / T(PR_T);
+  const T u = q[1], v = q[2], w = q[3];
+  G[0][0] = T(0.0); G[0][1] = t00; G[0][2] = t01; G[0][3] = t02;
+  G[1][0] = T(0.0); G[1][1] = t01; G[1][2] = t11; G[1][3] = t12;
+  G[2][0] = T(0.0); G[2][1] = t02; G[2][2] = t12; G[2][3] = t22;
   G[0][4] = (u * t00 + v * t01 + w * t02) + (-k * gT[0]);
   G[1][4] = (u * t01 + v * t11 + w * t12) + (-k * gT[1]);
   G[2][4] = (u * t02 + v * t12 + w * t22) + (-k * gT[2]);
@@ -189,26 +201,26 @@ __device__ __forceinline__ void cons_to_prim(const double* U, double q[5]) {
 }
 
 // boundary ghost state at one flux point (boundary/fr_ghost_state.py:26-189)
-__device__ __forceinline__ void ghost_state(const Bc& bc, int code, const double qo[5], const double n[3],
-                                            double g[5]) {
+template <class T>
+__device__ __forceinline__ void ghost_state(const Bc& bc, int code, const T qo[5], const T n[3], T g[5]) {
   for (int v = 0; v < 5; ++v) g[v] = qo[v];
   const int t = bc.type[code];
-  const double vn = qo[1] * n[0] + qo[2] * n[1] + qo[3] * n[2];
+  const T vn = qo[1] * n[0] + qo[2] * n[1] + qo[3] * n[2];
   if (t == BC_WALL) {
     if (bc.noslip[code]) {
-      for (int d = 0; d < 3; ++d) g[1 + d] = 2.0 * bc.wall_vel[code * 3 + d] - qo[1 + d];
+      for (int d = 0; d < 3; ++d) g[1 + d] = T(2.0) * T(bc.wall_vel[code * 3 + d]) - qo[1 + d];
     } else {
-      for (int d = 0; d < 3; ++d) g[1 + d] = qo[1 + d] - 2.0 * vn * n[d];
+      for (int d = 0; d < 3; ++d) g[1 + d] = qo[1 + d] - T(2.0) * vn * n[d];
     }
   } else if (t == BC_FARFIELD) {
-    for (int v = 0; v < 5; ++v) g[v] = bc.Q[code * 5 + v];
+    for (int v = 0; v < 5; ++v) g[v] = T(bc.Q[code * 5 + v]);
   } else if (t == BC_INLET) {
-    if (vn < 0.0)
-      for (int v = 0; v < 5; ++v) g[v] = bc.Q[code * 5 + v];
+    if (vn < T(0.0))
+      for (int v = 0; v < 5; ++v) g[v] = T(bc.Q[code * 5 + v]);
   } else if (t == BC_OUTLET) {
-    if (vn > 0.0) g[4] = bc.p_out[code];
+    if (vn > T(0.0)) g[4] = T(bc.p_out[code]);
   } else if (t == BC_SYMMETRY) {
-    for (int d = 0; d < 3; ++d) g[1 + d] = qo[1 + d] - 2.0 * vn * n[d];
+    for (int d = 0; d < 3; ++d) g[1 + d] = qo[1 + d] - T(2.0) * vn * n[d];
   }
 }
 

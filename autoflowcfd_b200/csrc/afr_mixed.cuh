@@ -1,0 +1,955 @@
+// Mixed-precision form of the FR residual-and-update stage.
+//
+// The operator contractions run on the tensor cores (tcgen05, BF16 inputs,
+// FP32 accumulation in tensor memory) as three-term hi+lo split products,
+// D = A_hi*B_hi + A_hi*B_lo + A_lo*B_hi, which carry about 16 significant bits
+// of each factor.  Pointwise fluxes are FP32.  FP64 is kept for the state, the
+// geometry metrics, the primitive recovery from the conserved state, the
+// residual sums and RK update, the norm and the force coefficients.
+//
+// Three kernels per stage (same data flow as the reference's residual,
+// core/fr_residual/inviscid.py:139-345 and core/fr_residual/viscous_flux.py:113-302):
+//   k_mx_pre   per 8-cell tile: gradients of (u,v,w,T) (D_3d as a GEMM) and the
+//              extrapolation of all point fields to every face point of the
+//              cell (boundary_extrap of all six faces stacked as one GEMM);
+//   k_mx_face  per (slot, flux point): AUSM+up and BR1 jumps.  Where the
+//              other side's interpolation row equals one of that cell's own
+//              extrapolation rows (matched once at create: every prism face
+//              point, most tet face points) the other side is read from its
+//              face-point fields; elsewhere it is interpolated from the source
+//              cells' FP32 point fields with the reference's matrices;
+//   k_mx_vol   per C-cell tile (persistent): c2f, viscous D_3d and the folded
+//              W = f2c*D_fine divergence as GEMMs -> volume terms (FP32);
+//   k_mx_update per few cells: lifting in ascending color order, outlier
+//              zeroing, SSP-RK3 combination, positivity, filter (FP64).
+//
+// Contraction inputs are deviations from the cell mean where the operator
+// reproduces constants (c2f, extrapolation, derivatives), so the split error is
+// relative to the variation inside the cell, not to the free-stream level.  The
+// inviscid flux is split as F(q) = F(qbar) + dF: the W contraction acts on the
+// contravariant dF (formed algebraically, without cancellation), and
+// W*(adj_fine (x) F(qbar)) = MD*F(qbar) uses the FP64 metric divergence
+// MD[c,s,n] = sum_{i,m} W[s,(i,m)] adj_fine[c,i,m,n] formed at create.
+//
+// Shared-memory operand images are K-major without swizzle (afr_tc.cuh).  Row
+// orders are chosen so that lanes of a warp write eight consecutive 16-byte
+// rows (conflict-free 2-byte stores): A rows are (field, cell) with the cell
+// index fastest in groups of eight.
+#pragma once
+#include "afr_kernels.cuh"
+#include "afr_tc.cuh"
+
+namespace afr {
+
+constexpr int MX_THREADS = 256;
+constexpr int MX_PRE_CELLS = 8;
+
+__host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int pow2_cols(int x) { return x <= 32 ? 32 : (x <= 64 ? 64 : (x <= 128 ? 128 : 256)); }
+
+// Operator images (each [hi | lo], K-major canonical, BF16 bit patterns).
+struct MxOps {
+  const uint16_t* c2f[2];  // B: rows i < Fq (fine point), K = Sq (solution point)
+  const uint16_t* W[2];    // B: rows s < Sq, K = 3*Fq, k = m*Fq + i
+  const uint16_t* D3[2];   // B: rows s < Sq, K = 3*Sq, k = m*Sq + j
+  const uint16_t* D3g[2];  // B: rows m*Sq + s, K = Sq (j)
+  const uint16_t* E[2];    // A: rows fp = (ax*2+side)*NP + i (128 rows), K = Sq
+  const double* MD;        // (N, S, 3) metric divergence of the folded W
+  const double* hcell;     // (N) interior-penalty length, cube root of the mean det
+};
+
+constexpr uint8_t MX_OFP_GENERAL = 255;  // other side by interpolation from point fields
+
+struct MxFace {
+  const float4* arow;   // (n_slots*NP) own adjugate row at the flux point, and its norm
+  const uint8_t* ofp;   // (n_slots*NP) face point of the other side, (ax*2+side)*NP + j, or MX_OFP_GENERAL
+};
+
+struct MxBuf {
+  float* XF;   // (N, FW, 6*NP) point fields at every face point of the cell
+  float* PFm;  // (N, S, 20) gradients of u, v, w, T (12), mu_t, q (5), 2 unused
+  float* Jm;   // (n_slots, NP, 10) inviscid and viscous jumps
+  float* RV;   // (N, S, 10) inviscid and viscous volume terms
+  int FW;      // 18 (q 5, grads 12, mu_t) or 5 (inviscid handles)
+};
+
+namespace mxd {
+
+__device__ __forceinline__ void st_split(uint16_t* img, int img_elems, int idx, float x) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+  img[idx] = __bfloat16_as_ushort(h);
+  img[img_elems + idx] = __bfloat16_as_ushort(l);
+}
+
+// n floats, 16-byte vector accesses when both ends allow them
+__device__ __forceinline__ void copy_f32(float* dst, const float* src, int n) {
+  if (((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15u) == 0) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int t = threadIdx.x; t < n / 4; t += blockDim.x) d4[t] = s4[t];
+    for (int t = (n / 4) * 4 + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+  } else {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+  }
+}
+
+// 16-byte copy global -> shared of an operator image
+__device__ __forceinline__ void copy_img(void* dst, const void* src, int bytes) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  for (int t = threadIdx.x; t < bytes / 16; t += blockDim.x) d[t] = __ldg(s + t);
+}
+
+// D (tensor memory) = A * B^T over K with the three-term split; A has 128
+// rows, B has nb rows.  Issued by one thread.
+__device__ __forceinline__ void mma_split(uint32_t tmem, const uint16_t* A, const uint16_t* B, int nb, int K) {
+  const uint32_t a_hi = tc::smem_u32(A), a_lo = a_hi + 128u * K * 2u;
+  const uint32_t b_hi = tc::smem_u32(B), b_lo = b_hi + (uint32_t)nb * K * 2u;
+  const uint32_t idesc = tc::idesc_bf16(128, nb);
+  for (int ks = 0; ks < K / 16; ++ks) {
+    const uint32_t ao = ks * 2u * 128u * 16u, bo = ks * 2u * (uint32_t)nb * 16u;
+    const uint64_t ah = tc::make_desc(a_hi + ao, 128 * 16, 128), al = tc::make_desc(a_lo + ao, 128 * 16, 128);
+    const uint64_t bh = tc::make_desc(b_hi + bo, nb * 16, 128), bl = tc::make_desc(b_lo + bo, nb * 16, 128);
+    tc::mma_bf16(tmem, ah, bh, idesc, ks > 0 ? 1u : 0u);
+    tc::mma_bf16(tmem, ah, bl, idesc, 1u);
+    tc::mma_bf16(tmem, al, bh, idesc, 1u);
+  }
+}
+
+// (cell, point) enumeration with the cell fastest in groups of 8: lanes of a
+// warp cover 8 cells x 4 consecutive points.
+__device__ __forceinline__ void cell_point(int idx, int npts, int& c, int& p) {
+  const int rest = idx >> 3;
+  p = rest % npts;
+  c = (rest / npts) * 8 + (idx & 7);
+}
+
+// F(qbar + dq) - F(qbar) for the Euler flux, written as telescoped products so
+// that no large terms cancel (qbar, dq primitive: rho, u, v, w, p).
+__device__ __forceinline__ void euler_flux_delta(const float qb[5], const float dq[5], float dF[3][5]) {
+  const float rb = qb[0], dr = dq[0], dp = dq[4];
+  const float ub[3] = {qb[1], qb[2], qb[3]}, du[3] = {dq[1], dq[2], dq[3]};
+  const float u[3] = {ub[0] + du[0], ub[1] + du[1], ub[2] + du[2]};
+  const float g1 = float(GAMMA / (GAMMA - 1.0));
+  const float uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const float d_uu = (u[0] + ub[0]) * du[0] + (u[1] + ub[1]) * du[1] + (u[2] + ub[2]) * du[2];
+  const float p = qb[4] + dp;
+  const float r = rb + dr;
+  const float e = g1 * p + 0.5f * r * uu;                 // rho H
+  const float de = g1 * dp + 0.5f * (dr * uu + rb * d_uu);
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const float dm = dr * u[n] + rb * du[n];              // delta(rho u_n)
+    const float mb = rb * ub[n];
+    dF[n][0] = dm;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dF[n][1 + j] = dm * u[j] + mb * du[j] + (n == j ? dp : 0.f);
+    dF[n][4] = du[n] * e + ub[n] * de;
+  }
+}
+
+__device__ __forceinline__ bool wait_commit(uint64_t* bar, uint32_t& phase, unsigned* status) {
+  const bool ok = tc::mbar_wait(bar, phase);
+  phase ^= 1u;
+  if (!ok) atomicOr(status, (unsigned)DS_TC_TIMEOUT);
+  return ok;
+}
+
+}  // namespace mxd
+
+// ---------------------------------------------------------------------------
+// pre-pass: gradients and face-point extrapolation of one 8-cell tile
+// ---------------------------------------------------------------------------
+template <int S, int NP>
+struct MxPreSmem {
+  static constexpr int Sq = pad16(S), NFP = 6 * NP, NB1 = 3 * Sq, NB2MAX = 144;
+  static constexpr int oB1 = 0;                        // D3g image (hi|lo)
+  static constexpr int oA2 = oB1 + NB1 * Sq * 4;       // E image
+  static constexpr int oA1 = oA2 + 128 * Sq * 4;       // gradient inputs, rows phi*8 + c
+  static constexpr int oB2 = oA1 + 128 * Sq * 4;       // face-field inputs, rows f*8 + c
+  static constexpr int oG = oB2 + NB2MAX * Sq * 4;     // reference-space gradients [c][s][m][phi]
+  static constexpr int oQ = oG + MX_PRE_CELLS * S * 12 * 4;  // q (FP64) [c][s][5]
+  static constexpr int oM = oQ + MX_PRE_CELLS * S * 5 * 8;   // means (FP64) [c][9]
+  static constexpr int total = oM + MX_PRE_CELLS * 9 * 8;
+  static constexpr int NCOL = pow2_cols(cmax(NB1, NB2MAX));
+};
+
+template <int S, int NP>
+__global__ void __launch_bounds__(MX_THREADS, 1)
+    k_mx_pre(Geom g, MxOps mo, MxBuf mb, const double* __restrict__ U, int nv, const double* __restrict__ nut,
+             int visc, int cell_base, int cell_end, unsigned* status) {
+  using L = MxPreSmem<S, NP>;
+  constexpr int Sq = L::Sq, NFP = L::NFP, C = MX_PRE_CELLS;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int abort_flag;
+  uint16_t* sB1 = reinterpret_cast<uint16_t*>(smem + L::oB1);
+  uint16_t* sA2 = reinterpret_cast<uint16_t*>(smem + L::oA2);
+  uint16_t* sA1 = reinterpret_cast<uint16_t*>(smem + L::oA1);
+  uint16_t* sB2 = reinterpret_cast<uint16_t*>(smem + L::oB2);
+  float* sG = reinterpret_cast<float*>(smem + L::oG);
+  double* sQ = reinterpret_cast<double*>(smem + L::oQ);
+  double* sM = reinterpret_cast<double*>(smem + L::oM);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int FW = mb.FW;
+  visc = visc && FW >= 18;
+  const int nfw = visc ? 18 : 5;  // fields extrapolated by this call
+  const int NB2 = pad16(nfw * C);
+  const int ct = cell_type(g, cell_base);
+
+  if (visc) mxd::copy_img(sB1, mo.D3g[ct], L::NB1 * Sq * 4);
+  mxd::copy_img(sA2, mo.E[ct], 128 * Sq * 4);
+  // operand padding (K columns s >= S, rows never written) stays zero
+  for (int t = tid; t < 128 * Sq * 4 / 16; t += MX_THREADS) reinterpret_cast<uint4*>(sA1)[t] = make_uint4(0, 0, 0, 0);
+  for (int t = tid; t < L::NB2MAX * Sq * 4 / 16; t += MX_THREADS)
+    reinterpret_cast<uint4*>(sB2)[t] = make_uint4(0, 0, 0, 0);
+  if (warp == 0) tc::tmem_alloc(&tbase, L::NCOL);
+  if (tid == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    abort_flag = 0;
+  }
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tbase;
+  uint32_t phase = 0;
+  const int ntiles = (cell_end - cell_base + C - 1) / C;
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = cell_base + tile * C;
+    const int nc = min(C, cell_end - e0);
+    // primitives in FP64 (core/fr_residual/inviscid.py:38-47)
+    for (int t = tid; t < C * S; t += MX_THREADS) {
+      const int c = t % C, s = t / C;
+      double q[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
+      if (c < nc) cons_to_prim(U + ((size_t)(e0 + c) * S + s) * nv, q);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) sQ[(c * S + s) * 5 + v] = q[v];
+    }
+    __syncthreads();
+    // cell means of q (5) and of u, v, w, T (4)
+    for (int t = tid; t < C * 9; t += MX_THREADS) {
+      const int c = t / 9, k = t % 9;
+      double acc = 0.0;
+      for (int s = 0; s < S; ++s) {
+        const double* q = sQ + (c * S + s) * 5;
+        acc += k < 5 ? q[k] : (k < 8 ? q[k - 4] : q[4] / (fmax(q[0], 1e-10) * R_AIR));
+      }
+      sM[c * 9 + k] = acc / S;
+    }
+    __syncthreads();
+    for (int t = tid; t < C * S; t += MX_THREADS) {
+      const int c = t % C, s = t / C;
+      const double* q = sQ + (c * S + s) * 5;
+      if (c < nc) {
+        const float mutf = (visc && nut) ? float(q[0] * nut[(size_t)(e0 + c) * S + s]) : 0.f;
+        float4* o = reinterpret_cast<float4*>(mb.PFm + ((size_t)(e0 + c) * S + s) * 20);
+        o[3] = make_float4(mutf, float(q[0]), float(q[1]), float(q[2]));
+        o[4] = make_float4(float(q[3]), float(q[4]), 0.f, 0.f);
+      }
+      if (visc) {
+        const double phi[4] = {q[1], q[2], q[3], q[4] / (fmax(q[0], 1e-10) * R_AIR)};
+#pragma unroll
+        for (int f = 0; f < 4; ++f)
+          mxd::st_split(sA1, 128 * Sq, tc::kmajor_index(f * C + c, s, 128), float(phi[f] - sM[c * 9 + 5 + f]));
+        const double mut = (c < nc && nut) ? q[0] * nut[(size_t)(e0 + c) * S + s] : 0.0;
+        mxd::st_split(sB2, NB2 * Sq, tc::kmajor_index(17 * C + c, s, NB2), float(mut));
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+        mxd::st_split(sB2, NB2 * Sq, tc::kmajor_index(v * C + c, s, NB2), float(q[v] - sM[c * 9 + v]));
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (visc) {
+      if (tid == 0) {
+        tc::fence_after();
+        mxd::mma_split(tmem, sA1, sB1, L::NB1, Sq);
+        tc::commit(&bar);
+        if (!mxd::wait_commit(&bar, phase, status)) abort_flag = 1;
+      }
+      __syncthreads();
+      if (abort_flag) break;
+      tc::fence_after();
+      // rows phi*8 + c live in TMEM lanes 0..31: warps 0 and 4 split the columns
+      if ((warp & 3) == 0) {
+        const int f = lane / C, c = lane % C;
+        for (int ch = warp >> 2; ch < L::NB1 / 8; ch += 2) {
+          float v8[8];
+          tc::tmem_ld8(tmem + ch * 8, v8);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int n = ch * 8 + j, m = n / Sq, s = n % Sq;
+            if (s < S) sG[((c * S + s) * 3 + m) * 4 + f] = v8[j];
+          }
+        }
+      }
+      __syncthreads();
+      // physical gradients (core/fr_operators/gradients.py:23-64) and mu_t
+      for (int t = tid; t < C * S; t += MX_THREADS) {
+        const int c = t % C, s = t / C;
+        float gr[12];
+        if (c < nc) {
+          const double* inv = g.inv + ((size_t)(e0 + c) * S + s) * 9;
+          float iv[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) iv[k] = float(__ldg(inv + k));
+          const float* gs = sG + (c * S + s) * 12;
+#pragma unroll
+          for (int f = 0; f < 4; ++f)
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+              gr[f * 3 + n] = gs[0 * 4 + f] * iv[0 * 3 + n] + gs[1 * 4 + f] * iv[1 * 3 + n] + gs[2 * 4 + f] * iv[2 * 3 + n];
+          float4* o = reinterpret_cast<float4*>(mb.PFm + ((size_t)(e0 + c) * S + s) * 20);
+          o[0] = make_float4(gr[0], gr[1], gr[2], gr[3]);
+          o[1] = make_float4(gr[4], gr[5], gr[6], gr[7]);
+          o[2] = make_float4(gr[8], gr[9], gr[10], gr[11]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 12; ++k) gr[k] = 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 12; ++k) mxd::st_split(sB2, NB2 * Sq, tc::kmajor_index((5 + k) * C + c, s, NB2), gr[k]);
+      }
+      tc::fence_async_smem();
+      __syncthreads();
+    }
+    // extrapolation of every field to all face points: D[fp][f*8+c]
+    if (tid == 0) {
+      tc::fence_after();
+      mxd::mma_split(tmem, sA2, sB2, NB2, Sq);
+      tc::commit(&bar);
+      if (!mxd::wait_commit(&bar, phase, status)) abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    tc::fence_after();
+    {
+      const int q4 = warp & 3, fp = q4 * 32 + lane;
+      if (q4 * 32 < NFP) {
+        for (int f = warp >> 2; f < nfw; f += 2) {
+          float v8[8];
+          tc::tmem_ld8(tmem + ((uint32_t)(q4 * 32) << 16) + f * 8, v8);
+          if (fp < NFP) {
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+              if (c < nc) {
+                const float val = f < 5 ? float(sM[c * 9 + f] + (double)v8[c]) : v8[c];
+                mb.XF[((size_t)(e0 + c) * FW + f) * NFP + fp] = val;
+              }
+          }
+        }
+      }
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, L::NCOL);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face kernel: one thread per (slot, flux point), fields read at face points
+// ---------------------------------------------------------------------------
+template <int S, int NP>
+__global__ void __launch_bounds__(128) k_mx_face(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
+                                                 const double* __restrict__ hcell, float mu, int visc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= st.n * NP) return;
+  constexpr int NFP = 6 * NP;
+  const int sl = t / NP, i = t % NP;
+  const int f = st.face[sl];
+  const int e = st.cell[sl];
+  const int fl = st.flags[sl];
+  const bool is_owner = (fl & 1) == 0;
+  const bool bnd = (fl & 2) != 0;
+  const int ax = (fl >> 2) & 3;
+  const float side = (fl & 16) ? 1.f : -1.f;
+  const int FW = mb.FW;
+  const int nf = visc ? 18 : 5;
+  float ow[18], ot[18];
+  {
+    const float* xo = mb.XF + (size_t)e * FW * NFP + (ax * 2 + ((fl & 16) ? 1 : 0)) * NP + i;
+#pragma unroll
+    for (int k = 0; k < 18; ++k) ow[k] = k < nf ? __ldg(xo + k * NFP) : 0.f;
+  }
+  const double* tnp = fc.tnormal + ((size_t)f * NP + i) * 3;
+  const float tn[3] = {float(tnp[0]), float(tnp[1]), float(tnp[2])};
+  if (bnd) {
+    float gq[5];
+    ghost_state<float>(bc, fc.bc_group[f], ow, tn, gq);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) ot[v] = gq[v];
+#pragma unroll
+    for (int k = 5; k < 18; ++k) ot[k] = ow[k];
+  } else if (mf.ofp[t] != MX_OFP_GENERAL) {
+    // matched rows come from the record's other cell (either source slot may hold them)
+    const int oc = is_owner ? fc.neighbor[f] : fc.owner[f];
+    const float* xn = mb.XF + (size_t)oc * FW * NFP + mf.ofp[t];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) ot[k] = k < nf ? __ldg(xn + k * NFP) : 0.f;
+  } else {
+    // interpolation from the source cells' point fields (sum src0 then src1,
+    // zero weights skipped as in core/fr_residual/inviscid_kernel_colored.py:117-121)
+#pragma unroll
+    for (int k = 0; k < 18; ++k) ot[k] = 0.f;
+    for (int src = 0; src < 2; ++src) {
+      const int c = src == 0 ? st.c0[sl] : st.c1[sl];
+      if (c < 0) continue;
+      const double* M = src == 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S
+                                 : (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S;
+      const float* pf = mb.PFm + (size_t)c * S * 20;
+      for (int s = 0; s < S; ++s) {
+        const float w = float(__ldg(M + s));
+        if (w == 0.f) continue;
+        const float4* p4 = reinterpret_cast<const float4*>(pf + s * 20);
+        const float4 x3 = __ldg(p4 + 3), x4 = __ldg(p4 + 4);
+        ot[0] += w * x3.y; ot[1] += w * x3.z; ot[2] += w * x3.w; ot[3] += w * x4.x; ot[4] += w * x4.y;
+        if (visc) {
+          const float4 x0 = __ldg(p4), x1 = __ldg(p4 + 1), x2 = __ldg(p4 + 2);
+          ot[5] += w * x0.x;  ot[6] += w * x0.y;  ot[7] += w * x0.z;  ot[8] += w * x0.w;
+          ot[9] += w * x1.x;  ot[10] += w * x1.y; ot[11] += w * x1.z; ot[12] += w * x1.w;
+          ot[13] += w * x2.x; ot[14] += w * x2.y; ot[15] += w * x2.z; ot[16] += w * x2.w;
+          ot[17] += w * x3.x;
+        }
+      }
+    }
+  }
+  const float4 ar = mf.arow[t];
+  const float a0 = ar.x, a1 = ar.y, a2 = ar.z;
+  const float mag = fmaxf(ar.w, 1e-30f);
+  float dir[3] = {a0 / mag * side, a1 / mag * side, a2 / mag * side};
+  const float sg = is_owner ? 1.f : -1.f;
+  const float t0 = sg * tn[0], t1 = sg * tn[1], t2 = sg * tn[2];
+  if (dir[0] * t0 + dir[1] * t1 + dir[2] * t2 < 0.5f) { dir[0] = t0; dir[1] = t1; dir[2] = t2; }
+  float Fc[5], Fp[3][5];
+  ausm_up<float>(ow, ot, dir, Fc);
+  euler_flux<float>(ow, Fp);
+  float* Jo = mb.Jm + (size_t)t * 10;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) Jo[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
+  if (visc) {
+    float qa[5], ga[13];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qa[v] = 0.5f * (ow[v] + ot[v]);
+#pragma unroll
+    for (int k = 0; k < 13; ++k) ga[k] = 0.5f * (ow[5 + k] + ot[5 + k]);
+    float Gc[3][5], Go[3][5];
+    viscous_flux<float>(qa, ga, ga + 9, mu, ga[12], Gc);
+    viscous_flux<float>(ow, ow + 5, ow + 14, mu, ow[17], Go);
+    float jv[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      jv[v] = (a0 * Gc[0][v] + a1 * Gc[1][v] + a2 * Gc[2][v]) - (a0 * Go[0][v] + a1 * Go[1][v] + a2 * Go[2][v]);
+    if (bnd) {
+      // interior penalty (core/fr_operators/flux_kernels.py:140-200)
+      const float eta = float(C_IP) * (mu + ow[17]) / float(hcell[e]);
+      const float scale = eta * ar.w * side;
+#pragma unroll
+      for (int v = 1; v < 4; ++v) jv[v] += -scale * (ow[v] - ot[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Jo[5 + v] = jv[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// volume kernel: persistent over C-cell tiles, tensor-core contractions.
+// Writes the volume terms RV (N, S, 10) FP32: inviscid -(W*Ft + MD*F(qbar))/det
+// (5) and viscous D_3d*Gt/det (5).
+// ---------------------------------------------------------------------------
+constexpr int MX_VOL_THREADS = 512;
+
+template <int S, int FN, int C>
+struct MxVolSmem {
+  static constexpr int Sq = pad16(S), Fq = pad16(FN);
+  static constexpr bool VP = S <= 27;  // viscous terms built in (P1, P2)
+  static constexpr int QS = Fq * 5 + 4;  // floats per cell of the fine-point deviations
+  static constexpr int oBc = 0;
+  static constexpr int oBW = oBc + Fq * Sq * 4;
+  static constexpr int oBD = oBW + Sq * 3 * Fq * 4;
+  static constexpr int oR1 = oBD + (VP ? Sq * 3 * Sq * 4 : 0);
+  static constexpr int szAc = 128 * Sq * 4, szAD = VP ? 128 * 3 * Sq * 4 : 0, szAW = 128 * 3 * Fq * 4;
+  static constexpr int szR1 = cmax(szAc + szAD, szAW);
+  static constexpr int oR2 = oR1 + szR1;  // q (FP64) before the first product, then dq, then the RV tile
+  static constexpr int szR2 = cmax(cmax(C * QS * 4, C * S * 5 * 8), C * S * 10 * 4);
+  static constexpr int oX = oR2 + szR2;
+  static constexpr int nX = C * 5 + C * 15;  // doubles: qbar, F(qbar)
+  static constexpr int total = oX + nX * 8;
+  static constexpr int cFq = 0, cD3 = Fq, cW = Fq + Sq;  // TMEM column bases
+  static constexpr int NCOL = pow2_cols(Fq + 2 * Sq);
+};
+
+template <int S, int FN, int C>
+__global__ void __launch_bounds__(MX_VOL_THREADS, 1)
+    k_mx_vol(Geom g, MxOps mo, const double* __restrict__ Ucur, int nv, int inviscid_only, float mu,
+             const float* __restrict__ PFm, float* __restrict__ RV, int cell_base, int cell_end, unsigned* status) {
+  using L = MxVolSmem<S, FN, C>;
+  constexpr int Sq = L::Sq, Fq = L::Fq, QS = L::QS, NT = MX_VOL_THREADS;
+  static_assert(C % 8 == 0 && 5 * C <= 128, "tile rows (v, c) must fit 128 lanes in groups of 8 cells");
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tbase;
+  __shared__ int abort_flag;
+  uint16_t* sBc = reinterpret_cast<uint16_t*>(smem + L::oBc);
+  uint16_t* sBW = reinterpret_cast<uint16_t*>(smem + L::oBW);
+  uint16_t* sBD = reinterpret_cast<uint16_t*>(smem + L::oBD);
+  uint16_t* sAc = reinterpret_cast<uint16_t*>(smem + L::oR1);
+  uint16_t* sAD = reinterpret_cast<uint16_t*>(smem + L::oR1 + L::szAc);
+  uint16_t* sAW = reinterpret_cast<uint16_t*>(smem + L::oR1);
+  double* sQ = reinterpret_cast<double*>(smem + L::oR2);
+  float* sQf = reinterpret_cast<float*>(smem + L::oR2);
+  float* sR = reinterpret_cast<float*>(smem + L::oR2);
+  double* sQb = reinterpret_cast<double*>(smem + L::oX);  // [c][5]
+  double* sFb = sQb + C * 5;                              // [c][n][v] Euler flux at qbar
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool visc = L::VP && !inviscid_only;
+  const int ct = cell_type(g, cell_base);
+
+  mxd::copy_img(sBc, mo.c2f[ct], Fq * Sq * 4);
+  mxd::copy_img(sBW, mo.W[ct], Sq * 3 * Fq * 4);
+  if (visc) mxd::copy_img(sBD, mo.D3[ct], Sq * 3 * Sq * 4);
+  if (warp == 0) tc::tmem_alloc(&tbase, L::NCOL);
+  if (tid == 0) {
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    abort_flag = 0;
+  }
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tbase;
+  uint32_t phase = 0;
+  const int ntiles = (cell_end - cell_base + C - 1) / C;
+  const int q4 = warp & 3;                      // TMEM lane quarter of this warp
+  const int lrow = q4 * 32 + lane;              // TMEM lane of this thread
+  const uint32_t lane_base = (uint32_t)(q4 * 32) << 16;
+  const int wsplit = warp >> 2, nsplit = NT / 128;  // warps sharing a lane quarter split the columns
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = cell_base + tile * C;
+    const int nc = min(C, cell_end - e0);
+    // ---- primitives (FP64) and cell means ----
+    for (int t = tid; t < C * S; t += NT) {
+      const int c = t / S;
+      double q[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
+      if (c < nc) cons_to_prim(Ucur + ((size_t)e0 * S + t) * nv, q);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) sQ[t * 5 + v] = q[v];
+    }
+    __syncthreads();
+    for (int t = tid; t < C * 5; t += NT) {
+      const int c = t / 5, v = t % 5;
+      double acc = 0.0;
+      for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 5 + v];
+      sQb[t] = acc / S;
+    }
+    __syncthreads();
+    for (int c = tid; c < C; c += NT) {
+      double F[3][5];
+      euler_flux<double>(sQb + c * 5, F);
+#pragma unroll
+      for (int n = 0; n < 3; ++n)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sFb[c * 15 + n * 5 + v] = F[n][v];
+    }
+    // ---- A operands: q - qbar at the solution points; contravariant viscous flux ----
+    for (int idx = tid; idx < C * Sq; idx += NT) {
+      int c, s;
+      mxd::cell_point(idx, Sq, c, s);
+      const bool live = c < nc && s < S;
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+        mxd::st_split(sAc, 128 * Sq, tc::kmajor_index(v * C + c, s, 128),
+                      live ? float(sQ[(c * S + s) * 5 + v] - sQb[c * 5 + v]) : 0.f);
+      if (visc) {
+        float Gt[3][5];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int v = 0; v < 5; ++v) Gt[m][v] = 0.f;
+        if (live) {
+          const size_t p = (size_t)(e0 + c) * S + s;
+          const float4* pf = reinterpret_cast<const float4*>(PFm + p * 20);
+          const float4 g0 = __ldg(pf), g1 = __ldg(pf + 1), g2 = __ldg(pf + 2), g3 = __ldg(pf + 3);
+          const double* am = g.adj + p * 9;
+          double amd[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) amd[k] = __ldg(am + k);
+          float q[5];
+#pragma unroll
+          for (int v = 0; v < 5; ++v) q[v] = float(sQ[(c * S + s) * 5 + v]);
+          const float gv[9] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x};
+          const float gT[3] = {g2.y, g2.z, g2.w};
+          float G[3][5];
+          viscous_flux<float>(q, gv, gT, mu, g3.x, G);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            const float x0 = float(amd[m * 3]), x1 = float(amd[m * 3 + 1]), x2 = float(amd[m * 3 + 2]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) Gt[m][v] = x0 * G[0][v] + x1 * G[1][v] + x2 * G[2][v];
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int v = 0; v < 5; ++v)
+            mxd::st_split(sAD, 128 * 3 * Sq, tc::kmajor_index(v * C + c, m * Sq + s, 128), Gt[m][v]);
+      }
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after();
+      mxd::mma_split(tmem + L::cFq, sAc, sBc, Fq, Sq);
+      if (visc) mxd::mma_split(tmem + L::cD3, sAD, sBD, Sq, 3 * Sq);
+      tc::commit(&bar);
+      if (!mxd::wait_commit(&bar, phase, status)) abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    tc::fence_after();
+    // ---- fine-point deviations dq = c2f*(q - qbar): TMEM -> shared ----
+    if (q4 * 32 < 5 * C) {
+      for (int ch = wsplit; ch < Fq / 8; ch += nsplit) {
+        float v8[8];
+        tc::tmem_ld8(tmem + lane_base + L::cFq + ch * 8, v8);
+        if (lrow < 5 * C) {
+          const int v = lrow / C, c = lrow % C;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) sQf[c * QS + (ch * 8 + j) * 5 + v] = v8[j];
+        }
+      }
+    }
+    __syncthreads();
+    // ---- contravariant Euler flux deviations at the fine points -> A_W ----
+    for (int idx = tid; idx < C * Fq; idx += NT) {
+      int c, i;
+      mxd::cell_point(idx, Fq, c, i);
+      float Ft[3][5];
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) Ft[m][v] = 0.f;
+      if (c < nc && i < FN) {
+        const double* ad = g.adj_fine + ((size_t)(e0 + c) * FN + i) * 9;
+        double add[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) add[k] = __ldg(ad + k);
+        float qb[5], dq[5], dF[3][5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          qb[v] = float(sQb[c * 5 + v]);
+          dq[v] = sQf[c * QS + i * 5 + v];
+        }
+        mxd::euler_flux_delta(qb, dq, dF);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const float x0 = float(add[m * 3]), x1 = float(add[m * 3 + 1]), x2 = float(add[m * 3 + 2]);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) Ft[m][v] = x0 * dF[0][v] + x1 * dF[1][v] + x2 * dF[2][v];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+          mxd::st_split(sAW, 128 * 3 * Fq, tc::kmajor_index(v * C + c, m * Fq + i, 128), Ft[m][v]);
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after();
+      mxd::mma_split(tmem + L::cW, sAW, sBW, Sq, 3 * Fq);
+      tc::commit(&bar);
+    }
+    // viscous divergence while the W product runs (its columns are complete);
+    // the dq tile is consumed, so the RV tile reuses its space
+    if (q4 * 32 < 5 * C) {
+      for (int ch = wsplit; ch < Sq / 8; ch += nsplit) {
+        float v8[8];
+        if (visc) tc::tmem_ld8(tmem + lane_base + L::cD3 + ch * 8, v8);
+        if (lrow < 5 * C) {
+          const int v = lrow / C, c = lrow % C;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int s = ch * 8 + j;
+            if (s < S && c < nc)
+              sR[(c * S + s) * 10 + 5 + v] =
+                  visc ? float(double(v8[j]) / g.det[(size_t)(e0 + c) * S + s]) : 0.f;
+          }
+        }
+      }
+    }
+    if (tid == 0 && !mxd::wait_commit(&bar, phase, status)) abort_flag = 1;
+    __syncthreads();
+    if (abort_flag) break;
+    tc::fence_after();
+    // ---- inviscid volume term: -(W*dFt + MD*F(qbar)) / det ----
+    if (q4 * 32 < 5 * C) {
+      for (int ch = wsplit; ch < Sq / 8; ch += nsplit) {
+        float v8[8];
+        tc::tmem_ld8(tmem + lane_base + L::cW + ch * 8, v8);
+        if (lrow < 5 * C) {
+          const int v = lrow / C, c = lrow % C;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int s = ch * 8 + j;
+            if (s < S && c < nc) {
+              const size_t p = (size_t)(e0 + c) * S + s;
+              const double* md = mo.MD + p * 3;
+              const double mdf = md[0] * sFb[c * 15 + v] + md[1] * sFb[c * 15 + 5 + v] + md[2] * sFb[c * 15 + 10 + v];
+              sR[(c * S + s) * 10 + v] = float(-(double(v8[j]) + mdf) / g.det[p]);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // coalesced store of the tile's volume terms (cells e0 .. e0+nc are contiguous)
+    mxd::copy_f32(RV + (size_t)e0 * S * 10, sR, nc * S * 10);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, L::NCOL);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// update kernel: CPB cells per CTA.  Lifting of the face jumps in ascending
+// color order (staged in shared memory), outlier zeroing, then the SSP-RK3
+// combination, positivity and filter in FP64 (or the residual-only outputs).
+// ---------------------------------------------------------------------------
+constexpr int MX_UPD_THREADS = 256;
+constexpr int MX_UPD_MAXSLOT = 8;  // slots per cell staged in shared memory (more: read from global)
+
+template <int S, int NP, int CPB>
+struct MxUpdSmem {
+  static constexpr int oRi = 0;                        // CPB*S*5 doubles
+  static constexpr int oRv = oRi + CPB * S * 5;
+  static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*8
+  static constexpr int oW = oU + CPB * S * 8;          // outliers: CPB*40
+  static constexpr int oP = oW + CPB * 40;             // CPB*S
+  static constexpr int nD = (oP + CPB * S + 1) / 2 * 2;  // doubles (even: the jumps start 16-byte aligned)
+  static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats
+  static constexpr int total = nD * 8 + nJ * 4;
+};
+
+template <int S, int NP, int CPB>
+__global__ void __launch_bounds__(MX_UPD_THREADS)
+    k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm) {
+  using L = MxUpdSmem<S, NP, CPB>;
+  extern __shared__ double smu[];
+  double* sRi = smu + L::oRi;
+  double* sRv = smu + L::oRv;
+  double* sU = smu + L::oU;
+  double* work = smu + L::oW;
+  double* part = smu + L::oP;
+  float* sJ = reinterpret_cast<float*>(smu + L::nD);
+  const int e0 = a.cell_base + blockIdx.x * CPB;
+  const int nc = min(CPB, a.cell_end - e0);
+  const int ct = cell_type(g, e0);
+  const int nv = a.nv;
+  const bool visc = !a.inviscid_only;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
+    const size_t p = (size_t)e0 * S + t / 5;
+    sRi[t] = double(RV[p * 10 + t % 5]);
+    sRv[t] = visc ? double(RV[p * 10 + 5 + t % 5]) : 0.0;
+  }
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
+  const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
+  const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
+  if (staged) mxd::copy_f32(sJ, Jm + (size_t)k_beg * NP * 10, (k_end - k_beg) * NP * 10);
+  __syncthreads();
+  // lift the jumps of each cell's slots, ascending color order
+  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
+    const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    const int e = e0 + b;
+    const double dj = g.det[(size_t)e * S + s];
+    double ci = 0.0, cv = 0.0;
+    for (int k = fc.slot_ptr[e]; k < fc.slot_ptr[e + 1]; ++k) {
+      const int fl = a.slot_flags[k];
+      const int ax = (fl >> 2) & 3;
+      const int fp = ops.dist_fp[ax * S + s];
+      const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
+      const float* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10;
+      ci += -(gw * double(Jk[v])) / dj;
+      if (visc) cv += (gw * double(Jk[5 + v])) / dj;
+    }
+    sRi[t] = sRi[t] + ci;
+    if (visc) sRv[t] = sRv[t] + cv;
+  }
+  __syncthreads();
+  suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
+
+  if (a.stage < 0) {
+    for (int t = tid; t < nc * S * nv; t += blockDim.x) {
+      const int p = t / nv, v = t % nv;
+      if (a.Rinv) a.Rinv[(size_t)e0 * S * nv + t] = v < 5 ? sRi[p * 5 + v] : 0.0;
+      if (a.Rvisc) a.Rvisc[(size_t)e0 * S * nv + t] = (v < 5 && visc) ? sRv[p * 5 + v] : 0.0;
+    }
+    return;
+  }
+  // RK stage combination + positivity, in place over the state tile
+  for (int p = tid; p < nc * S; p += blockDim.x) {
+    double Lr[8], un[8];
+    double sq_sum = 0.0;
+    for (int v = 0; v < nv; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
+    for (int v = 0; v < nv; ++v) sq_sum += Lr[v] * Lr[v];
+    const size_t gp = (size_t)e0 * S + p;
+    const double dts = a.dt[gp];
+    const double* u0 = a.U0 + gp * nv;
+    double* uc = sU + p * 8;
+    if (a.stage == 0) {
+      for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
+    } else if (a.stage == 1) {
+      for (int v = 0; v < nv; ++v) un[v] = (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v];
+    } else {
+      for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v];
+    }
+    const double rho = fmax(un[0], 1e-6);
+    un[0] = rho;
+    double vel[3] = {un[1] / rho, un[2] / rho, un[3] / rho};
+    const double vm = sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    if (vm > 1e4) {
+      const double cf = 1e4 / vm;
+      for (int d = 0; d < 3; ++d) { vel[d] *= cf; un[1 + d] = rho * vel[d]; }
+    }
+    const double ke = 0.5 * rho * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    const double pr = (GAMMA - 1.0) * (un[4] - ke);
+    if (pr < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
+    if (nv > 5) un[5] = fmax(un[5], 0.0);
+    if (nv > 6) un[6] = fmax(un[6], 1e-8);
+    for (int v = 0; v < nv; ++v) uc[v] = un[v];
+    part[p] = sq_sum;
+  }
+  __syncthreads();
+  const double* Fm = ops.filt[ct];
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) {
+    const int p = t / nv, v = t % nv;
+    const int b = p / S, s = p % S;
+    double val;
+    if (v < 5) {
+      double acc = 0.0;
+      for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * sU[(b * S + j) * 8 + v];
+      val = acc;
+    } else {
+      val = sU[p * 8 + v];
+    }
+    a.Unext[(size_t)e0 * S * nv + t] = val;
+  }
+  if (a.stage == 0 && tid < nc) {
+    double acc = 0.0;
+    for (int s = 0; s < S; ++s) acc += part[tid * S + s];
+    a.norm_part[e0 + tid] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// set-up kernels of the mixed form
+// ---------------------------------------------------------------------------
+// own adjugate row at each slot flux point (E * adj, FP64 then rounded) and the
+// face point of the other side whose extrapolation row equals the slot's
+// interpolation row to tol relative (MX_OFP_GENERAL where none does)
+template <int S, int NP>
+__global__ void k_mx_match(Geom g, Ops ops, Faces fc, SlotTable st, float4* arow, uint8_t* ofp, double tol) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= st.n * NP) return;
+  const int sl = t / NP, i = t % NP;
+  const int f = st.face[sl], e = st.cell[sl], fl = st.flags[sl];
+  const bool is_owner = (fl & 1) == 0, bnd = (fl & 2) != 0;
+  const int ax = (fl >> 2) & 3, sb = (fl & 16) ? 1 : 0;
+  const int ct = cell_type(g, e);
+  const double* Er = ops.extrap + (((size_t)ct * 3 + ax) * 2 + sb) * NP * S + (size_t)i * S;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int s = 0; s < S; ++s) {
+    const double w = Er[s];
+    const double* ad = g.adj + ((size_t)e * S + s) * 9 + ax * 3;
+    a0 += w * ad[0];
+    a1 += w * ad[1];
+    a2 += w * ad[2];
+  }
+  arow[t] = make_float4(float(a0), float(a1), float(a2), float(sqrt(a0 * a0 + a1 * a1 + a2 * a2)));
+  if (bnd) {
+    ofp[t] = 0;
+    return;
+  }
+  // the other side's interpolation row; the reference may split one cell's
+  // row over its two source slots, so same-cell rows are added first
+  const int c0 = st.c0[sl], c1 = st.c1[sl];
+  const int expect = is_owner ? fc.neighbor[f] : fc.owner[f];
+  const bool one_cell = (c0 == expect || c0 < 0) && (c1 == expect || c1 < 0) && (c0 >= 0 || c1 >= 0);
+  if (!one_cell) {
+    ofp[t] = MX_OFP_GENERAL;
+    return;
+  }
+  const double* M0 = c0 >= 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S : nullptr;
+  const double* M1 = c1 >= 0 ? (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S : nullptr;
+  const int oax = is_owner ? fc.n_axis[f] : fc.o_axis[f];
+  const int osb = (is_owner ? fc.n_side[f] : fc.o_side[f]) > 0.0 ? 1 : 0;
+  const int oct = cell_type(g, expect);
+  double mmax = 0.0;
+  for (int s = 0; s < S; ++s) mmax = fmax(mmax, fabs((M0 ? M0[s] : 0.0) + (M1 ? M1[s] : 0.0)));
+  int best = -1;
+  double best_err = INFINITY;
+  for (int j = 0; j < NP; ++j) {
+    const double* Eo = ops.extrap + (((size_t)oct * 3 + oax) * 2 + osb) * NP * S + (size_t)j * S;
+    double err = 0.0;
+    for (int s = 0; s < S && err <= best_err; ++s)
+      err = fmax(err, fabs((M0 ? M0[s] : 0.0) + (M1 ? M1[s] : 0.0) - Eo[s]));
+    if (err < best_err) {
+      best_err = err;
+      best = j;
+    }
+  }
+  ofp[t] = (best >= 0 && best_err <= tol * fmax(mmax, 1e-300)) ? (uint8_t)((oax * 2 + osb) * NP + best)
+                                                                 : MX_OFP_GENERAL;
+}
+
+// MD[c,s,n] = sum_{i,m} W[s, i*3+m] adj_fine[c,i,m,n]  (W's columns follow D_fine: i*3+m)
+template <int S, int FN>
+__global__ void k_mx_md(Geom g, Ops ops, double* MD) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)g.N * S * 3) return;
+  const int n = (int)(t % 3);
+  const int s = (int)((t / 3) % S);
+  const size_t c = t / (3 * S);
+  const int ct = cell_type(g, (int)c);
+  const double* w = ops.W[ct] + (size_t)s * FN * 3;
+  const double* ad = g.adj_fine + c * FN * 9;
+  double acc = 0.0;
+  for (int i = 0; i < FN; ++i)
+    for (int m = 0; m < 3; ++m) acc += w[i * 3 + m] * ad[i * 9 + m * 3 + n];
+  MD[t] = acc;
+}
+
+template <int S>
+__global__ void k_mx_hcell(Geom g, double* hcell) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.N) return;
+  double vol = 0.0;
+  for (int s = 0; s < S; ++s) vol += g.det[(size_t)e * S + s];
+  vol /= S;
+  double h = pow(vol, 1.0 / 3.0);
+  if (h < 1e-300) h = 1e-300;
+  hcell[e] = h;
+}
+
+}  // namespace afr

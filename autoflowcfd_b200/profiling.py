@@ -20,12 +20,17 @@ def step_breakdown(solver):
     vals = [v for v in ms if v >= 0]
     sst = solver.k is not None
     names = ["local_dt"] + (["sst_point", "sst_face", "sst_update"] if sst else [])
+    # per stage: pre-pass, face kernel, cell kernel (plain form) or volume
+    # kernel (mixed form), update kernel (mixed form; empty in the plain form)
     for stg in range(3):
-        names += [f"pre{stg}", f"face{stg}", f"cell{stg}"]
+        names += [f"pre{stg}", f"face{stg}", f"cell{stg}", f"upd{stg}"]
     names += ["norm"]
     per = dict(zip(names, vals))
-    face = [per[f"face{i}"] for i in range(3) if f"face{i}" in per]
-    cell = [per[f"cell{i}"] for i in range(3) if f"cell{i}" in per]
-    return {"per_kernel_ms": per, "launches_per_step": int(nl.value),
-            "k_face_ms_per_launch": sum(face) / len(face) if face else None,
-            "k_cell_ms_per_launch": sum(cell) / len(cell) if cell else None}
+
+    def avg(key):
+        xs = [per[f"{key}{i}"] for i in range(3) if f"{key}{i}" in per]
+        return sum(xs) / len(xs) if xs else None
+
+    return {"per_kernel_ms": per, "launches_per_step": int(nl.value), "k_pre_ms_per_launch": avg("pre"),
+            "k_face_ms_per_launch": avg("face"), "k_cell_ms_per_launch": avg("cell"),
+            "k_update_ms_per_launch": avg("upd")}

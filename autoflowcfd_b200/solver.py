@@ -58,12 +58,16 @@ class B200FRSolver:
         inviscid_only: Euler runs (the viscous residual is zero).
         global_dt_factor: > 0 selects time-accurate global stepping
             dt = factor * min(dt_local).
+        precision: "fp64" (plain form, FP64 throughout) or "mixed" (operator
+            contractions as BF16 hi+lo split tensor-core products with FP32
+            accumulation, FP32 fluxes; FP64 state, metrics, norms and Cd/Cl).
         device: CUDA device.
     """
 
     def __init__(self, case: Dict[str, np.ndarray], turb_model_name: str = "NONE", mu_molecular: float = 1.8e-5,
                  rho_inf: float = 1.225, vel_inf: float = 33.33, p_inf: float = 101325.0,
-                 inviscid_only: bool = False, global_dt_factor: float = 0.0, device="cuda:0"):
+                 inviscid_only: bool = False, global_dt_factor: float = 0.0, precision: str = "fp64",
+                 device="cuda:0"):
         name = turb_model_name.upper()
         if name not in ("SST", "NONE"):
             raise ValueError(f"Unknown turbulence model: {turb_model_name}")
@@ -82,6 +86,10 @@ class B200FRSolver:
         prm.inviscid_only = 1 if inviscid_only else 0
         prm.mu, prm.rho_inf, prm.vel_inf, prm.p_inf = self.mu_molecular, rho_inf, vel_inf, p_inf
         prm.global_dt_factor = float(global_dt_factor)
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.precision = precision
+        prm.precision = _lib.AFR_PREC_MIXED if precision == "mixed" else _lib.AFR_PREC_FP64
         self._prm = prm
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):

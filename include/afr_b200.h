@@ -53,6 +53,20 @@ enum {
 };
 
 enum { AFR_TURB_NONE = 0, AFR_TURB_SST = 1 };
+
+/* Arithmetic form of the residual-and-update stage.  AFR_PREC_FP64 is FP64
+ * throughout.  AFR_PREC_MIXED runs the operator contractions (c2f, the
+ * folded f2c*D_fine divergence, the viscous D_3d divergence, the gradients
+ * and the extrapolation to faces) on the tensor cores as BF16 hi+lo split
+ * products with FP32 accumulation and the pointwise fluxes in FP32, keeping
+ * FP64 for the state, geometry metrics, primitive recovery, residual sums,
+ * RK update, norm and Cd/Cl.  Viscous terms are built up to P2 in the mixed
+ * form (P3 mixed handles must be inviscid).  A contraction accumulated in FP32
+ * carries about 2^-24 * (operator row l1 norm) * |x|, so afr_create refuses
+ * the mixed form (AFR_EUNSUPPORTED) when a present cell type's operators have
+ * row l1 norms above 1e6: the reference's collapsed-tet operators at P2 and P3
+ * (row l1 norms ~2e11 and ~2e8); prisms at every order and tets at P1 pass. */
+enum { AFR_PREC_FP64 = 0, AFR_PREC_MIXED = 1 };
 enum { AFR_BC_WALL = 0, AFR_BC_FARFIELD = 1, AFR_BC_INLET = 2, AFR_BC_OUTLET = 3, AFR_BC_SYMMETRY = 4 };
 
 typedef struct afr_handle afr_handle;
@@ -123,7 +137,7 @@ typedef struct afr_params {
   int32_t n_vars;           /* 5, or 7 with SST (columns 5:7 carried, zero residual) */
   int32_t turb;             /* AFR_TURB_* */
   int32_t inviscid_only;    /* 1: viscous residual is zero (Euler) */
-  int32_t reserved;
+  int32_t precision;        /* AFR_PREC_FP64 (plain form) or AFR_PREC_MIXED */
   double mu;                /* molecular viscosity of the mean flow (FRSolver mu_molecular) */
   double rho_inf, vel_inf, p_inf;
   double global_dt_factor;  /* >0: dt = factor * min(dt_local) everywhere (time-accurate runs) */
@@ -131,6 +145,8 @@ typedef struct afr_params {
 
 int afr_create(const afr_mesh_desc* mesh, const afr_params* params, void* stream, afr_handle** out);
 int afr_destroy(afr_handle* h);
+/* Message of the last failure on h; with h == NULL, of the last failed
+ * afr_create on the calling thread. */
 const char* afr_last_error(const afr_handle* h);
 const char* afr_status_string(int status);
 int afr_version(void);
