@@ -42,6 +42,7 @@ struct afr_handle {
   double* red = nullptr;      // reduction results
   double* pt = nullptr;
   double* cfp = nullptr;
+  double* sp8 = nullptr;
   uint8_t* wall_face = nullptr;
   uint8_t* cd_wall = nullptr;
   double* area_w = nullptr;
@@ -332,12 +333,21 @@ struct Launch {
     return r;
   }
   static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
-    k_sst_point<S><<<h->N, 128, 0, st>>>(h->g, h->ops, a);
+    constexpr int CPB = SstTile<S>::CPB, TH = SstTile<S>::THREADS;
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n > 0) k_sst_point<S><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, a, ranges[r], ranges[r + 1]);
+    }
     if (tm) tm->mark(st);
     const int nt = h->F * NP;
     k_sst_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, a);
     if (tm) tm->mark(st);
-    k_sst_update<S, NP><<<h->N, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n > 0)
+        k_sst_update<S, NP><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, h->fc, a, ranges[r], ranges[r + 1]);
+    }
     if (tm) tm->mark(st);
     return cudaGetLastError();
   }
@@ -1004,6 +1014,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   if (prm->turb == AFR_TURB_SST) {
     if ((rc = dalloc(h, &h->pt, N * S * 5))) return bail(rc);
     if ((rc = dalloc(h, &h->cfp, F * P * 4))) return bail(rc);
+    if ((rc = dalloc(h, &h->sp8, N * S * 8))) return bail(rc);
   }
   if (prm->precision == AFR_PREC_MIXED && (rc = mixed_setup(h, m, Wkeep, st))) return bail(rc);
   cudaError_t e = cudaStreamSynchronize(st);
@@ -1051,7 +1062,7 @@ int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, doubl
   if (!h || !U || !dt_local || !k || !omega || !nu_t) return AFR_EINVAL;
   if (h->prm.turb != AFR_TURB_SST) return fail(h, AFR_EINVAL, "handle was created without SST");
   cudaStream_t st = (cudaStream_t)stream;
-  SstArgs s{U, dt_local, k, omega, nu_t, h->pt, h->cfp, h->wall_face, diag, h->nv, h->prm.mu};
+  SstArgs s{U, dt_local, k, omega, nu_t, h->pt, h->sp8, h->cfp, h->wall_face, diag, h->nv, h->prm.mu};
   cudaError_t e = dispatch(h, [&](auto L) { return L.sst(h, s, st); });
   if (e != cudaSuccess) return cuda_fail(h, e, "sst update");
   return check_status(h, st);
@@ -1072,7 +1083,7 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
   cudaError_t e = dispatch(h, [&](auto L) {
     cudaError_t r = cudaSuccess;
     if (sst) {
-      SstArgs s{U, h->dt, k, omega, nu_t, h->pt, h->cfp, h->wall_face, nullptr, h->nv, h->prm.mu};
+      SstArgs s{U, h->dt, k, omega, nu_t, h->pt, h->sp8, h->cfp, h->wall_face, nullptr, h->nv, h->prm.mu};
       r = L.sst(h, s, st, tm);
       nl += 3;
       if (r != cudaSuccess) return r;

@@ -41,7 +41,7 @@
 
 namespace afr {
 
-constexpr int MX_THREADS = 256;
+constexpr int MX_THREADS = 512;  // pre-pass CTA
 constexpr int MX_PRE_CELLS = 8;
 
 __host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
@@ -92,6 +92,22 @@ __device__ __forceinline__ void copy_f32(float* dst, const float* src, int n) {
     for (int t = (n / 4) * 4 + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
   } else {
     for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+  }
+}
+
+// L2 prefetch of bytes [off, off + bytes) of an array of total bytes (bulk
+// copy engine, no data returned to the SM); the range is clipped to 16-byte
+// boundaries inside the array.  A hint: issued by one thread.
+__device__ __forceinline__ void prefetch_l2(const void* base, size_t total, size_t off, size_t bytes) {
+  const size_t lo = off & ~size_t(15);
+  size_t hi = off + bytes;
+  hi = (hi + 15) & ~size_t(15);
+  const size_t cap = total & ~size_t(15);
+  if (hi > cap) hi = cap;
+  const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+  for (size_t p = lo; p < hi; p += 32768) {
+    const uint32_t n = (uint32_t)((hi - p) < 32768 ? (hi - p) : 32768);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b + p), "r"(n) : "memory");
   }
 }
 
@@ -223,6 +239,14 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = cell_base + tile * C;
     const int nc = min(C, cell_end - e0);
+    if (tid == 0 && tile + (int)gridDim.x < ntiles) {
+      // the next tile's inputs (contiguous cell ranges) into L2 while this one runs
+      const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
+      const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
+      mxd::prefetch_l2(U, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
+      if (visc) mxd::prefetch_l2(g.inv, NS * 72, en * S * 72, nn * S * 72);
+      if (nut) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
+    }
     // primitives in FP64 (core/fr_residual/inviscid.py:38-47)
     for (int t = tid; t < C * S; t += MX_THREADS) {
       const int c = t % C, s = t / C;
@@ -279,7 +303,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       // rows phi*8 + c live in TMEM lanes 0..31: warps 0 and 4 split the columns
       if ((warp & 3) == 0) {
         const int f = lane / C, c = lane % C;
-        for (int ch = warp >> 2; ch < L::NB1 / 8; ch += 2) {
+        for (int ch = warp >> 2; ch < L::NB1 / 8; ch += MX_THREADS / 128) {
           float v8[8];
           tc::tmem_ld8(tmem + ch * 8, v8);
 #pragma unroll
@@ -332,7 +356,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     {
       const int q4 = warp & 3, fp = q4 * 32 + lane;
       if (q4 * 32 < NFP) {
-        for (int f = warp >> 2; f < nfw; f += 2) {
+        for (int f = warp >> 2; f < nfw; f += MX_THREADS / 128) {
           float v8[8];
           tc::tmem_ld8(tmem + ((uint32_t)(q4 * 32) << 16) + f * 8, v8);
           if (fp < NFP) {
@@ -540,6 +564,19 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = cell_base + tile * C;
     const int nc = min(C, cell_end - e0);
+    if (tid == 0 && tile + (int)gridDim.x < ntiles) {
+      // the next tile's inputs (contiguous cell ranges) into L2 while this one runs
+      const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
+      const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
+      mxd::prefetch_l2(Ucur, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
+      mxd::prefetch_l2(g.adj_fine, (size_t)g.N * FN * 72, en * FN * 72, nn * FN * 72);
+      mxd::prefetch_l2(g.det, NS * 8, en * S * 8, nn * S * 8);
+      mxd::prefetch_l2(mo.MD, NS * 24, en * S * 24, nn * S * 24);
+      if (visc) {
+        mxd::prefetch_l2(PFm, NS * 80, en * S * 80, nn * S * 80);
+        mxd::prefetch_l2(g.adj, NS * 72, en * S * 72, nn * S * 72);
+      }
+    }
     // ---- primitives (FP64) and cell means ----
     for (int t = tid; t < C * S; t += NT) {
       const int c = t / S;
@@ -773,7 +810,8 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
     sRi[t] = double(RV[p * 10 + t % 5]);
     sRv[t] = visc ? double(RV[p * 10 + 5 + t % 5]) : 0.0;
   }
-  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
+  for (int p = tid; p < nc * S; p += blockDim.x)
+    for (int v = 0; v < nv; ++v) sU[p * 8 + v] = a.Ucur[((size_t)e0 * S + p) * nv + v];
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
   const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
   if (staged) mxd::copy_f32(sJ, Jm + (size_t)k_beg * NP * 10, (k_end - k_beg) * NP * 10);
@@ -782,7 +820,7 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
     const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     const int e = e0 + b;
-    const double dj = g.det[(size_t)e * S + s];
+    const double rdj = 1.0 / g.det[(size_t)e * S + s];  // one division per point (no bitwise target here)
     double ci = 0.0, cv = 0.0;
     for (int k = fc.slot_ptr[e]; k < fc.slot_ptr[e + 1]; ++k) {
       const int fl = a.slot_flags[k];
@@ -790,9 +828,11 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
       const int fp = ops.dist_fp[ax * S + s];
       const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
       const float* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10;
-      ci += -(gw * double(Jk[v])) / dj;
-      if (visc) cv += (gw * double(Jk[5 + v])) / dj;
+      ci -= gw * double(Jk[v]);
+      if (visc) cv += gw * double(Jk[5 + v]);
     }
+    ci *= rdj;
+    cv *= rdj;
     sRi[t] = sRi[t] + ci;
     if (visc) sRv[t] = sRv[t] + cv;
   }
@@ -800,11 +840,12 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
   suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
 
   if (a.stage < 0) {
-    for (int t = tid; t < nc * S * nv; t += blockDim.x) {
-      const int p = t / nv, v = t % nv;
-      if (a.Rinv) a.Rinv[(size_t)e0 * S * nv + t] = v < 5 ? sRi[p * 5 + v] : 0.0;
-      if (a.Rvisc) a.Rvisc[(size_t)e0 * S * nv + t] = (v < 5 && visc) ? sRv[p * 5 + v] : 0.0;
-    }
+    for (int p = tid; p < nc * S; p += blockDim.x)
+      for (int v = 0; v < nv; ++v) {
+        const size_t o = ((size_t)e0 * S + p) * nv + v;
+        if (a.Rinv) a.Rinv[o] = v < 5 ? sRi[p * 5 + v] : 0.0;
+        if (a.Rvisc) a.Rvisc[o] = (v < 5 && visc) ? sRv[p * 5 + v] : 0.0;
+      }
     return;
   }
   // RK stage combination + positivity, in place over the state tile
@@ -842,19 +883,15 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
   }
   __syncthreads();
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < nc * S * nv; t += blockDim.x) {
-    const int p = t / nv, v = t % nv;
+  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
+    const int p = t / 5, v = t % 5;
     const int b = p / S, s = p % S;
-    double val;
-    if (v < 5) {
-      double acc = 0.0;
-      for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * sU[(b * S + j) * 8 + v];
-      val = acc;
-    } else {
-      val = sU[p * 8 + v];
-    }
-    a.Unext[(size_t)e0 * S * nv + t] = val;
+    double acc = 0.0;
+    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * sU[(b * S + j) * 8 + v];
+    a.Unext[((size_t)e0 * S + p) * nv + v] = acc;
   }
+  for (int p = tid; p < nc * S; p += blockDim.x)
+    for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = sU[p * 8 + v];
   if (a.stage == 0 && tid < nc) {
     double acc = 0.0;
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];

@@ -18,6 +18,7 @@ struct SstArgs {
   double* w;            // (N,S) in/out
   double* nut;          // (N,S) in/out (kinematic eddy viscosity)
   double* pt;           // (N,S,5) scratch: Sk, Sw, beta_blend, gamma_k, gamma_w
+  double* sp8;          // (N,S,8) scratch: rho, u, v, w, k, omega, gamma_k, gamma_w (face gathers)
   double* cfp;          // (F,P,4) scratch: conv_k, diff_k, conv_w, diff_w face corrections
   const uint8_t* wall_face;  // (F) WALL boundary faces (k Dirichlet-zero ghost)
   double* dbg;          // optional (N,S,4): Sk, Sw, transport_k, transport_w
@@ -57,32 +58,60 @@ __device__ __forceinline__ double sst_F2(double k, double w, double d, double nu
   return tanh(a * a);
 }
 
-// per cell: gradients of (rho u, rho v, rho w, k, omega), pointwise SST terms
+// SST cells per CTA (the three per-cell SST kernels)
 template <int S>
-__global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a) {
-  __shared__ double f[S * 5];
-  __shared__ double gc[S * 3 * 5];
-  const int e = blockIdx.x;
-  const int ct = cell_type(g, e);
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const double* u = a.U + ((size_t)e * S + s) * a.nv;
-    f[s * 5 + 0] = u[1];
-    f[s * 5 + 1] = u[2];
-    f[s * 5 + 2] = u[3];
-    f[s * 5 + 3] = a.k[(size_t)e * S + s];
-    f[s * 5 + 4] = a.w[(size_t)e * S + s];
+struct SstTile {
+  static constexpr int CPB = S <= 8 ? 16 : (S <= 27 ? 4 : 2);
+  static constexpr int THREADS = 128;
+};
+
+// per cell: gradients of (rho u, rho v, rho w, k, omega), pointwise SST terms.
+// CPB cells per CTA; cells [cell_base, cell_end) share one cell type.
+template <int S>
+__global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, int cell_base, int cell_end) {
+  constexpr int CPB = SstTile<S>::CPB;
+  __shared__ double f[CPB * S * 5];
+  __shared__ double gc[CPB * S * 3 * 5];
+  const int e0 = cell_base + blockIdx.x * CPB;
+  const int nc = min(CPB, cell_end - e0);
+  const int ct = cell_type(g, e0);
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const size_t p = (size_t)e0 * S + t;
+    const double* u = a.U + p * a.nv;
+    f[t * 5 + 0] = u[1];
+    f[t * 5 + 1] = u[2];
+    f[t * 5 + 2] = u[3];
+    f[t * 5 + 3] = a.k[p];
+    f[t * 5 + 4] = a.w[p];
   }
   __syncthreads();
-  block_gemm<S * 3, 5, S>(gc, 5, ops.D3g[ct], S, f, 5);
+  // reference-space gradients, rows s*3+m of D3g, summed in ascending j
+  for (int t = threadIdx.x; t < S * 3 * 5; t += blockDim.x) {
+    const int r = t / 5, q = t % 5;
+    const double* Dr = ops.D3g[ct] + (size_t)r * S;
+    double acc[CPB];
+#pragma unroll
+    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+    for (int j = 0; j < S; ++j) {
+      const double w = __ldg(Dr + j);
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) acc[b] += w * f[(b * S + j) * 5 + q];
+    }
+#pragma unroll
+    for (int b = 0; b < CPB; ++b)
+      if (b < nc) gc[(b * S * 3 + r) * 5 + q] = acc[b];
+  }
   __syncthreads();
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const size_t p = (size_t)e * S + s;
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const int s = t % S;
+    const size_t p = (size_t)e0 * S + t;
     const double* inv = g.inv + p * 9;
+    const double* gcs = gc + (size_t)(t - s) * 3 * 5;  // this cell's rows
     double gp[5][3];
     for (int q = 0; q < 5; ++q)
       for (int n = 0; n < 3; ++n) {
         double acc = 0.0;
-        for (int m = 0; m < 3; ++m) acc += gc[(s * 3 + m) * 5 + q] * inv[m * 3 + n];
+        for (int m = 0; m < 3; ++m) acc += gcs[(s * 3 + m) * 5 + q] * inv[m * 3 + n];
         gp[q][n] = acc;
       }
     // |grad| <= 1e6 clip of grad k, grad omega
@@ -143,6 +172,15 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a) {
     o[2] = beta;
     o[3] = a.mu + sk * rnut;
     o[4] = a.mu + sw * rnut;
+    double* o8 = a.sp8 + p * 8;
+    o8[0] = rho;
+    o8[1] = u[1] / rho;
+    o8[2] = u[2] / rho;
+    o8[3] = u[3] / rho;
+    o8[4] = kf;
+    o8[5] = wf;
+    o8[6] = o[3];
+    o8[7] = o[4];
   }
 }
 
@@ -156,21 +194,17 @@ __global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
   const int ct = cell_type(g, oc);
   const int ax = fc.o_axis[f];
   const double* E = ops.extrap + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * NP * S + i * S;
-  // owner side: rho, rho u (3), k, w, gamma_k, gamma_w
+  // owner side: rho, u (3), k, w, gamma_k, gamma_w (point values packed by k_sst_point)
   double po[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int s = 0; s < S; ++s) {
-    const size_t p = (size_t)oc * S + s;
-    const double* u = a.U + p * a.nv;
-    const double rho = fmax(u[0], 1e-10);
+    const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)oc * S + s) * 8);
     const double we = __ldg(E + s);
-    po[0] += we * rho;
-    po[1] += we * (u[1] / rho);
-    po[2] += we * (u[2] / rho);
-    po[3] += we * (u[3] / rho);
-    po[4] += we * a.k[p];
-    po[5] += we * a.w[p];
-    po[6] += we * a.pt[p * 5 + 3];
-    po[7] += we * a.pt[p * 5 + 4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const double2 v = __ldg(x + h);
+      po[2 * h] += we * v.x;
+      po[2 * h + 1] += we * v.y;
+    }
   }
   // neighbour side: k, w, gamma_k, gamma_w
   double pn[4];
@@ -183,30 +217,22 @@ __global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
     pn[3] = po[7];
   } else {
     for (int q = 0; q < 4; ++q) pn[q] = 0.0;
-    if (c0 >= 0) {
-      const double* M = fc.nb_m0 + ((size_t)f * NP + i) * S;
-      for (int q = 0; q < 4; ++q) {
-        double acc = 0.0;
-        for (int s = 0; s < S; ++s) {
-          const size_t p = (size_t)c0 * S + s;
-          const double x = q == 0 ? a.k[p] : q == 1 ? a.w[p] : a.pt[p * 5 + 1 + q];
-          acc += __ldg(M + s) * x;
-        }
-        pn[q] = acc;
+    // k, w, gamma_k, gamma_w of the source cells, each summed over s in order
+    for (int src = 0; src < 2; ++src) {
+      const int c = src == 0 ? c0 : (i1 >= 0 ? fc.nb_c1[i1] : -1);
+      if (c < 0) continue;
+      const double* M = src == 0 ? fc.nb_m0 + ((size_t)f * NP + i) * S : fc.nb_m1 + ((size_t)i1 * NP + i) * S;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int s = 0; s < S; ++s) {
+        const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)c * S + s) * 8 + 4);
+        const double w = __ldg(M + s);
+        const double2 v0 = __ldg(x), v1 = __ldg(x + 1);
+        acc[0] += w * v0.x;
+        acc[1] += w * v0.y;
+        acc[2] += w * v1.x;
+        acc[3] += w * v1.y;
       }
-    }
-    if (i1 >= 0) {
-      const int c1 = fc.nb_c1[i1];
-      const double* M = fc.nb_m1 + ((size_t)i1 * NP + i) * S;
-      for (int q = 0; q < 4; ++q) {
-        double acc = 0.0;
-        for (int s = 0; s < S; ++s) {
-          const size_t p = (size_t)c1 * S + s;
-          const double x = q == 0 ? a.k[p] : q == 1 ? a.w[p] : a.pt[p * 5 + 1 + q];
-          acc += __ldg(M + s) * x;
-        }
-        pn[q] += acc;
-      }
+      for (int q = 0; q < 4; ++q) pn[q] = src == 0 ? acc[q] : pn[q] + acc[q];
     }
   }
   const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
@@ -221,40 +247,49 @@ __global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
 }
 
 // per cell: volume transport terms, gather of the face corrections, outlier
-// suppression and the point-implicit k / omega update
+// suppression and the point-implicit k / omega update.  CPB cells per CTA.
 template <int S, int NP>
-__global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a) {
-  __shared__ double fl[S * 4];       // k, w, gamma_k, gamma_w
-  __shared__ double gc[S * 3 * 2];   // reference-space grads of k, w
-  __shared__ double Ft[S * 3 * 4];   // contravariant fluxes: conv k, diff k, conv w, diff w
-  __shared__ double R[S * 4];        // volume residuals
-  __shared__ double C[S * 4];        // interface corrections
-  __shared__ double T[S * 5];        // transport k, w (+ padding for the outlier helper)
-  __shared__ double Ref[S * 5];
+__global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a, int cell_base,
+                                                    int cell_end) {
+  constexpr int CPB = SstTile<S>::CPB;
+  __shared__ double fl[CPB * S * 4];      // k, w, gamma_k, gamma_w
+  __shared__ double gc[CPB * S * 3 * 2];  // reference-space grads of k, w
+  __shared__ double Ft[CPB * S * 3 * 4];  // contravariant fluxes: conv k, diff k, conv w, diff w
+  __shared__ double R[CPB * S * 4];       // volume residuals, then with the interface corrections
+  __shared__ double T[CPB * S * 5];       // transport k, w (+ padding for the outlier helper)
+  __shared__ double Ref[CPB * S * 5];
   __shared__ double work[24];
-  const int e = blockIdx.x;
-  const int ct = cell_type(g, e);
-  const double* det = g.det + (size_t)e * S;
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const size_t p = (size_t)e * S + s;
-    fl[s * 4 + 0] = a.k[p];
-    fl[s * 4 + 1] = a.w[p];
-    fl[s * 4 + 2] = a.pt[p * 5 + 3];
-    fl[s * 4 + 3] = a.pt[p * 5 + 4];
-    for (int q = 0; q < 4; ++q) C[s * 4 + q] = 0.0;
+  const int e0 = cell_base + blockIdx.x * CPB;
+  const int nc = min(CPB, cell_end - e0);
+  const int ct = cell_type(g, e0);
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)e0 * S + t) * 8 + 4);
+    const double2 v0 = x[0], v1 = x[1];
+    fl[t * 4 + 0] = v0.x;
+    fl[t * 4 + 1] = v0.y;
+    fl[t * 4 + 2] = v1.x;
+    fl[t * 4 + 3] = v1.y;
   }
   __syncthreads();
-  // grad k, grad w in reference space (D3g rows s*3+m)
+  // grad k, grad w in reference space (D3g rows s*3+m, ascending j)
   for (int t = threadIdx.x; t < S * 3 * 2; t += blockDim.x) {
     const int r = t / 2, q = t % 2;
     const double* Dr = ops.D3g[ct] + (size_t)r * S;
-    double acc = 0.0;
-    for (int j = 0; j < S; ++j) acc += __ldg(Dr + j) * fl[j * 4 + q];
-    gc[r * 2 + q] = acc;
+    double acc[CPB];
+#pragma unroll
+    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+    for (int j = 0; j < S; ++j) {
+      const double w = __ldg(Dr + j);
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) acc[b] += w * fl[(b * S + j) * 4 + q];
+    }
+#pragma unroll
+    for (int b = 0; b < CPB; ++b)
+      if (b < nc) gc[(b * S * 3 + r) * 2 + q] = acc[b];
   }
   __syncthreads();
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const size_t p = (size_t)e * S + s;
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const size_t p = (size_t)e0 * S + t;
     const double* inv = g.inv + p * 9;
     const double* adj = g.adj + p * 9;
     const double* u = a.U + p * a.nv;
@@ -264,77 +299,94 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
       double gphys[3];
       for (int n = 0; n < 3; ++n) {
         double acc = 0.0;
-        for (int m = 0; m < 3; ++m) acc += gc[(s * 3 + m) * 2 + q] * inv[m * 3 + n];
+        for (int m = 0; m < 3; ++m) acc += gc[(t * 3 + m) * 2 + q] * inv[m * 3 + n];
         gphys[n] = acc;
       }
-      const double phi = fl[s * 4 + q];
-      const double gam = fl[s * 4 + 2 + q];
+      const double phi = fl[t * 4 + q];
+      const double gam = fl[t * 4 + 2 + q];
       double Fc[3], Fd[3];
       for (int d = 0; d < 3; ++d) {
         Fc[d] = (rho * vel[d]) * phi;
         Fd[d] = gam * gphys[d];
       }
       for (int m = 0; m < 3; ++m) {
-        Ft[(s * 3 + m) * 4 + 2 * q] = adj[m * 3 + 0] * Fc[0] + adj[m * 3 + 1] * Fc[1] + adj[m * 3 + 2] * Fc[2];
-        Ft[(s * 3 + m) * 4 + 2 * q + 1] = adj[m * 3 + 0] * Fd[0] + adj[m * 3 + 1] * Fd[1] + adj[m * 3 + 2] * Fd[2];
+        Ft[(t * 3 + m) * 4 + 2 * q] = adj[m * 3 + 0] * Fc[0] + adj[m * 3 + 1] * Fc[1] + adj[m * 3 + 2] * Fc[2];
+        Ft[(t * 3 + m) * 4 + 2 * q + 1] = adj[m * 3 + 0] * Fd[0] + adj[m * 3 + 1] * Fd[1] + adj[m * 3 + 2] * Fd[2];
       }
     }
   }
   __syncthreads();
-  // divergence: sum over m of (sum_j Ft[j,m] D[s,j,m])
+  // divergence: sum over m of (sum_j Ft[j,m] D[s,j,m]); then the face
+  // corrections of every face side in ascending color order
   for (int t = threadIdx.x; t < S * 4; t += blockDim.x) {
     const int s = t / 4, q = t % 4;
     const double* Dr = ops.D3[ct] + (size_t)s * S * 3;
-    double div = 0.0;
+    double div[CPB];
+#pragma unroll
+    for (int b = 0; b < CPB; ++b) div[b] = 0.0;
     for (int m = 0; m < 3; ++m) {
-      double acc = 0.0;
-      for (int j = 0; j < S; ++j) acc += Ft[(j * 3 + m) * 4 + q] * __ldg(Dr + j * 3 + m);
-      div += acc;
+      double acc[CPB];
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+      for (int j = 0; j < S; ++j) {
+        const double d = __ldg(Dr + j * 3 + m);
+#pragma unroll
+        for (int b = 0; b < CPB; ++b) acc[b] += Ft[((b * S + j) * 3 + m) * 4 + q] * d;
+      }
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) div[b] += acc[b];
     }
-    R[t] = -div / det[s];
+#pragma unroll
+    for (int b = 0; b < CPB; ++b)
+      if (b < nc) R[(b * S + s) * 4 + q] = -div[b] / g.det[(size_t)(e0 + b) * S + s];
   }
-  __syncthreads();
-  // face corrections in ascending color order (every face side)
-  const int b = fc.tslot_ptr[e], en = fc.tslot_ptr[e + 1];
-  for (int si = b; si < en; ++si) {
-    const int code = fc.tslot[si];
-    const int f = code >> 1;
-    const bool is_owner = (code & 1) == 0;
-    const int ax = is_owner ? fc.o_axis[f] : fc.n_axis[f];
-    const double side = is_owner ? fc.o_side[f] : fc.n_side[f];
-    const double* gp = side > 0.0 ? ops.g_right : ops.g_left;
-    for (int t = threadIdx.x; t < S * 4; t += blockDim.x) {
-      const int s = t / 4, q = t % 4;
+  for (int t = threadIdx.x; t < nc * S * 4; t += blockDim.x) {
+    const int p = t / 4, q = t % 4, s = p % S;
+    const int e = e0 + p / S;
+    const double dj = g.det[(size_t)e * S + s];
+    double C = 0.0;
+    for (int si = fc.tslot_ptr[e]; si < fc.tslot_ptr[e + 1]; ++si) {
+      const int code = fc.tslot[si];
+      const int f = code >> 1;
+      const bool is_owner = (code & 1) == 0;
+      const int ax = is_owner ? fc.o_axis[f] : fc.n_axis[f];
+      const double side = is_owner ? fc.o_side[f] : fc.n_side[f];
+      const double* gp = side > 0.0 ? ops.g_right : ops.g_left;
       const int fp = ops.dist_fp[ax * S + s];
       const double contrib = gp[ops.dist_co[ax * S + s]] * a.cfp[((size_t)f * NP + fp) * 4 + q];
-      if (is_owner) C[t] -= contrib / det[s];
-      else C[t] += contrib / det[s];
+      if (is_owner) C -= contrib / dj;
+      else C += contrib / dj;
     }
-    __syncthreads();
-  }
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const double rho = fmax(a.U[((size_t)e * S + s) * a.nv], 1e-10);
-    const double conv_k = R[s * 4 + 0] + C[s * 4 + 0];
-    const double diff_k = R[s * 4 + 1] - C[s * 4 + 1];
-    const double conv_w = R[s * 4 + 2] + C[s * 4 + 2];
-    const double diff_w = R[s * 4 + 3] - C[s * 4 + 3];
-    T[s * 5 + 0] = (conv_k + diff_k) / fmax(rho, 1e-10);
-    T[s * 5 + 1] = (conv_w + diff_w) / fmax(rho, 1e-10);
-    T[s * 5 + 2] = 0.0; T[s * 5 + 3] = 0.0; T[s * 5 + 4] = 0.0;
-    Ref[s * 5 + 0] = fl[s * 4 + 0];
-    Ref[s * 5 + 1] = fl[s * 4 + 1];
-    Ref[s * 5 + 2] = 0.0; Ref[s * 5 + 3] = 0.0; Ref[s * 5 + 4] = 0.0;
+    Ref[t] = C;  // staged: R is complete only after the barrier below
   }
   __syncthreads();
-  suppress_outliers<S>(T, Ref, 5, work);
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    const size_t p = (size_t)e * S + s;
+  for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
+    const double rho = fmax(a.U[((size_t)e0 * S + p) * a.nv], 1e-10);
+    const double* Cp = Ref + p * 4;
+    const double conv_k = R[p * 4 + 0] + Cp[0];
+    const double diff_k = R[p * 4 + 1] - Cp[1];
+    const double conv_w = R[p * 4 + 2] + Cp[2];
+    const double diff_w = R[p * 4 + 3] - Cp[3];
+    T[p * 5 + 0] = (conv_k + diff_k) / fmax(rho, 1e-10);
+    T[p * 5 + 1] = (conv_w + diff_w) / fmax(rho, 1e-10);
+    T[p * 5 + 2] = 0.0; T[p * 5 + 3] = 0.0; T[p * 5 + 4] = 0.0;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
+    Ref[p * 5 + 0] = fl[p * 4 + 0];
+    Ref[p * 5 + 1] = fl[p * 4 + 1];
+    Ref[p * 5 + 2] = 0.0; Ref[p * 5 + 3] = 0.0; Ref[p * 5 + 4] = 0.0;
+  }
+  __syncthreads();
+  for (int b = 0; b < nc; ++b) suppress_outliers<S>(T + b * S * 5, Ref + b * S * 5, 5, work);
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const size_t p = (size_t)e0 * S + t;
     const double rho = fmax(a.U[p * a.nv], 1e-10);
-    const double tk = dfinite(T[s * 5 + 0]);
-    const double tw = dfinite(T[s * 5 + 1]);
+    const double tk = dfinite(T[t * 5 + 0]);
+    const double tw = dfinite(T[t * 5 + 1]);
     const double* pt = a.pt + p * 5;
     const double dts = a.dt[p];
-    const double kf = fl[s * 4 + 0], wf = fl[s * 4 + 1];
+    const double kf = fl[t * 4 + 0], wf = fl[t * 4 + 1];
     const double wo = fmax(wf, 1e-10);
     const double dkd = dfinite((pt[0] / fmax(rho, 1e-10)) / (1.0 + dts * (SST_BSTAR * wo)));
     const double dwd = dfinite((pt[1] / fmax(rho, 1e-10)) / (1.0 + dts * (pt[2] * wo)));
