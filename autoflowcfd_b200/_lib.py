@@ -10,7 +10,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libafr_b200.so")
+# AFR_B200_LIB selects another build of the same C-ABI (for example an instrumented one)
+LIB_PATH = os.environ.get("AFR_B200_LIB") or os.path.join(HERE, "libafr_b200.so")
 
 AFR_OK, AFR_EINVAL, AFR_ENOMEM, AFR_ECUDA, AFR_ENONFINITE, AFR_EUNSUPPORTED, AFR_EINDEX = range(7)
 AFR_TURB_NONE, AFR_TURB_SST = 0, 1

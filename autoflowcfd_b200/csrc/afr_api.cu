@@ -56,6 +56,7 @@ struct afr_handle {
   MxFace mf{};
   MxBuf mb{};
   int mx_pre_blocks = 0, mx_cell_blocks = 0;  // resident CTAs of the persistent kernels
+  int mx_pre_per_sm = 0;
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   std::string err;
@@ -266,6 +267,15 @@ struct Launch {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_mx_update<S, NP, MXU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)mx_upd_smem());
+    // the largest shared-memory carveout for the two persistent kernels, whose
+    // shared memory sets how many CTAs fit on an SM
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_pre<S, NP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_vol<S, FN, MXC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+
     if (e == cudaSuccess)
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_mx_pre<S, NP>, MX_THREADS, mx_pre_smem());
     if (e == cudaSuccess)
@@ -276,6 +286,7 @@ struct Launch {
     if (bp < 1 || bc < 1) return cudaErrorInvalidConfiguration;
     h->mx_pre_blocks = bp * sms;
     h->mx_cell_blocks = bc * sms;
+    h->mx_pre_per_sm = bp;
     return cudaSuccess;
   }
   static int n_ranges(const afr_handle* h) { return (h->n_prism > 0 ? 1 : 0) + (h->N > h->n_prism ? 1 : 0); }
@@ -313,7 +324,7 @@ struct Launch {
       a.cell_end = ranges[r + 1];
       const int n = a.cell_end - a.cell_base;
       if (n <= 0) continue;
-      k_mx_update<S, NP, MXU><<<(n + MXU - 1) / MXU, MX_UPD_THREADS, mx_upd_smem(), st>>>(h->g, h->ops, h->fc, a,
+      k_mx_update<S, NP, MXU><<<(n + MXU - 1) / MXU, MxUpdSmem<S, NP, MXU>::THREADS, mx_upd_smem(), st>>>(h->g, h->ops, h->fc, a,
                                                                                         h->mb.RV, h->mb.Jm);
     }
     return cudaGetLastError();
@@ -385,6 +396,20 @@ std::vector<uint16_t> kmajor_image(int R, int K, Get get) {
       const size_t idx = ((size_t)(k >> 3) * R + r) * 8 + (k & 7);
       img[idx] = hi;
       img[(size_t)R * K + idx] = lo;
+    }
+  return img;
+}
+
+// N x K matrix -> one stacked image of 2N rows: the hi parts over the lo parts
+template <class Get>
+std::vector<uint16_t> kmajor_image_cat(int N, int K, Get get) {
+  auto split = kmajor_image(N, K, get);  // [hi | lo], each N x K
+  std::vector<uint16_t> img(2 * (size_t)N * K, 0);
+  for (int r = 0; r < N; ++r)
+    for (int k = 0; k < K; ++k) {
+      const size_t src = ((size_t)(k >> 3) * N + r) * 8 + (k & 7);
+      img[((size_t)(k >> 3) * 2 * N + r) * 8 + (k & 7)] = split[src];
+      img[((size_t)(k >> 3) * 2 * N + N + r) * 8 + (k & 7)] = split[(size_t)N * K + src];
     }
   return img;
 }
@@ -620,12 +645,12 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
     const double* D3 = m->D_3d[t];
     const double* Wt = Wkeep[t].data();
     const double* ex = m->boundary_extrap;
-    auto i_c2f = kmajor_image(Fq, Sq, [&](int i, int s) { return (i < Fn && s < S) ? c2f[i * S + s] : 0.0; });
-    auto i_W = kmajor_image(Sq, 3 * Fq, [&](int s, int k) {
+    auto i_c2f = kmajor_image_cat(Fq, Sq, [&](int i, int s) { return (i < Fn && s < S) ? c2f[i * S + s] : 0.0; });
+    auto i_W = kmajor_image_cat(Sq, 3 * Fq, [&](int s, int k) {
       const int mm = k / Fq, i = k % Fq;
       return (s < S && i < Fn) ? Wt[(size_t)s * 3 * Fn + i * 3 + mm] : 0.0;
     });
-    auto i_D3 = kmajor_image(Sq, 3 * Sq, [&](int s, int k) {
+    auto i_D3 = kmajor_image_cat(Sq, 3 * Sq, [&](int s, int k) {
       const int mm = k / Sq, j = k % Sq;
       return (s < S && j < S) ? D3[(size_t)s * 3 * S + j * 3 + mm] : 0.0;
     });

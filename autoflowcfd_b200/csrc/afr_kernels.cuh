@@ -532,21 +532,18 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     part[p] = sq_sum;
   }
   __syncthreads();
-  // modal filter on the first five variables
+  // modal filter on the first five variables; lanes of a warp share the
+  // filter row s (broadcast loads), each output summed over j in order
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < nc * S * nv; t += blockDim.x) {
-    const int p = t / nv, v = t % nv;
-    const int b = p / S, s = p % S;
-    double val;
-    if (v < 5) {
-      double acc = 0.0;
-      for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * 8 + v];
-      val = acc;
-    } else {
-      val = Up[p * 8 + v];
-    }
-    a.Unext[(size_t)e0 * S * nv + t] = val;
+  for (int t = tid; t < S * CPB * 5; t += blockDim.x) {
+    const int s = t / (CPB * 5), r = t % (CPB * 5), b = r / 5, v = r % 5;
+    if (b >= nc) continue;
+    double acc = 0.0;
+    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * 8 + v];
+    a.Unext[((size_t)(e0 + b) * S + s) * nv + v] = acc;
   }
+  for (int p = tid; p < nc * S; p += blockDim.x)
+    for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = Up[p * 8 + v];
   if (a.stage == 0 && tid < nc) {
     double acc = 0.0;  // fixed order per cell: points ascending
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];

@@ -48,11 +48,12 @@ __host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int pow2_cols(int x) { return x <= 32 ? 32 : (x <= 64 ? 64 : (x <= 128 ? 128 : 256)); }
 
-// Operator images (each [hi | lo], K-major canonical, BF16 bit patterns).
+// Operator images, K-major canonical, BF16 bit patterns.  "cat" images stack
+// the hi rows over the lo rows (2N rows, one image); the others are [hi | lo].
 struct MxOps {
-  const uint16_t* c2f[2];  // B: rows i < Fq (fine point), K = Sq (solution point)
-  const uint16_t* W[2];    // B: rows s < Sq, K = 3*Fq, k = m*Fq + i
-  const uint16_t* D3[2];   // B: rows s < Sq, K = 3*Sq, k = m*Sq + j
+  const uint16_t* c2f[2];  // B cat: rows i < Fq (fine point), K = Sq (solution point)
+  const uint16_t* W[2];    // B cat: rows s < Sq, K = 3*Fq, k = m*Fq + i
+  const uint16_t* D3[2];   // B cat: rows s < Sq, K = 3*Sq, k = m*Sq + j
   const uint16_t* D3g[2];  // B: rows m*Sq + s, K = Sq (j)
   const uint16_t* E[2];    // A: rows fp = (ax*2+side)*NP + i (128 rows), K = Sq
   const double* MD;        // (N, S, 3) metric divergence of the folded W
@@ -111,6 +112,24 @@ __device__ __forceinline__ void prefetch_l2(const void* base, size_t total, size
   }
 }
 
+// two consecutive K positions (idx even) of one row: hi and lo parts as
+// packed bf16x2 words, one conversion per part
+__device__ __forceinline__ void st_split2(uint16_t* img, int img_elems, int idx, float x0, float x1) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+  *reinterpret_cast<__nv_bfloat162*>(img + idx) = h;
+  *reinterpret_cast<__nv_bfloat162*>(img + img_elems + idx) = l;
+}
+
+// (cell, point pair) enumeration with the cell fastest in groups of 8: lanes
+// of a warp cover 8 cells x 4 consecutive pairs (8 points, one 16-byte row each)
+__device__ __forceinline__ void cell_pair(int idx, int npts, int& c, int& p0) {
+  const int rest = idx >> 3;
+  p0 = 2 * (rest % (npts / 2));
+  c = (rest / (npts / 2)) * 8 + (idx & 7);
+}
+
 // 16-byte copy global -> shared of an operator image
 __device__ __forceinline__ void copy_img(void* dst, const void* src, int bytes) {
   const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -131,6 +150,23 @@ __device__ __forceinline__ void mma_split(uint32_t tmem, const uint16_t* A, cons
     tc::mma_bf16(tmem, ah, bh, idesc, ks > 0 ? 1u : 0u);
     tc::mma_bf16(tmem, ah, bl, idesc, 1u);
     tc::mma_bf16(tmem, al, bh, idesc, 1u);
+  }
+}
+
+// D (tensor memory, 2n columns) with the three-term split against a stacked
+// operator image Bcat = [B_hi; B_lo] (2n rows): columns [0, n) collect
+// A_hi*B_hi + A_lo*B_hi and columns [n, 2n) collect A_hi*B_lo; the sum of the
+// two blocks is the product.  Two MMAs per K step, A_hi read once.
+__device__ __forceinline__ void mma_cat(uint32_t tmem, const uint16_t* A, const uint16_t* Bcat, int n, int K) {
+  const uint32_t a_hi = tc::smem_u32(A), a_lo = a_hi + 128u * K * 2u;
+  const uint32_t b = tc::smem_u32(Bcat);
+  const uint32_t id2 = tc::idesc_bf16(128, 2 * n), id1 = tc::idesc_bf16(128, n);
+  for (int ks = 0; ks < K / 16; ++ks) {
+    const uint32_t ao = ks * 2u * 128u * 16u, bo = ks * 2u * 2u * (uint32_t)n * 16u;
+    const uint64_t ah = tc::make_desc(a_hi + ao, 128 * 16, 128), al = tc::make_desc(a_lo + ao, 128 * 16, 128);
+    const uint64_t bc = tc::make_desc(b + bo, 2 * n * 16, 128);  // all 2n rows; the first n are B_hi
+    tc::mma_bf16(tmem, ah, bc, id2, ks > 0 ? 1u : 0u);
+    tc::mma_bf16(tmem, al, bc, id1, 1u);
   }
 }
 
@@ -166,6 +202,17 @@ __device__ __forceinline__ void euler_flux_delta(const float qb[5], const float 
   }
 }
 
+// primitives (rho, u, v, w, p) without pressure floor (core/fr_residual/inviscid.py:38-47)
+// and T = p / (rho R), with one reciprocal of rho (the mixed form has no bitwise target)
+__device__ __forceinline__ void prim_T(const double* U, double q[6]) {
+  const double rho = fmax(U[0], 1e-10);
+  const double r = 1.0 / rho;
+  const double u = U[1] * r, v = U[2] * r, w = U[3] * r;
+  const double p = (GAMMA - 1.0) * rho * (U[4] * r - 0.5 * (u * u + v * v + w * w));
+  q[0] = rho; q[1] = u; q[2] = v; q[3] = w; q[4] = p;
+  q[5] = p * r * (1.0 / R_AIR);
+}
+
 __device__ __forceinline__ bool wait_commit(uint64_t* bar, uint32_t& phase, unsigned* status) {
   const bool ok = tc::mbar_wait(bar, phase);
   phase ^= 1u;
@@ -186,8 +233,8 @@ struct MxPreSmem {
   static constexpr int oA1 = oA2 + 128 * Sq * 4;       // gradient inputs, rows phi*8 + c
   static constexpr int oB2 = oA1 + 128 * Sq * 4;       // face-field inputs, rows f*8 + c
   static constexpr int oG = oB2 + NB2MAX * Sq * 4;     // reference-space gradients [c][s][m][phi]
-  static constexpr int oQ = oG + MX_PRE_CELLS * S * 12 * 4;  // q (FP64) [c][s][5]
-  static constexpr int oM = oQ + MX_PRE_CELLS * S * 5 * 8;   // means (FP64) [c][9]
+  static constexpr int oQ = oG + MX_PRE_CELLS * S * 12 * 4;  // q and T (FP64) [c][s][6]
+  static constexpr int oM = oQ + MX_PRE_CELLS * S * 6 * 8;   // means (FP64) [c][9]
   static constexpr int total = oM + MX_PRE_CELLS * 9 * 8;
   static constexpr int NCOL = pow2_cols(cmax(NB1, NB2MAX));
 };
@@ -247,29 +294,27 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       if (visc) mxd::prefetch_l2(g.inv, NS * 72, en * S * 72, nn * S * 72);
       if (nut) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
     }
-    // primitives in FP64 (core/fr_residual/inviscid.py:38-47)
+    // primitives and temperature in FP64
     for (int t = tid; t < C * S; t += MX_THREADS) {
       const int c = t % C, s = t / C;
-      double q[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
-      if (c < nc) cons_to_prim(U + ((size_t)(e0 + c) * S + s) * nv, q);
+      double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
+      if (c < nc) mxd::prim_T(U + ((size_t)(e0 + c) * S + s) * nv, q);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) sQ[(c * S + s) * 5 + v] = q[v];
+      for (int v = 0; v < 6; ++v) sQ[(c * S + s) * 6 + v] = q[v];
     }
     __syncthreads();
     // cell means of q (5) and of u, v, w, T (4)
     for (int t = tid; t < C * 9; t += MX_THREADS) {
       const int c = t / 9, k = t % 9;
+      const int col = k < 5 ? k : (k < 8 ? k - 4 : 5);
       double acc = 0.0;
-      for (int s = 0; s < S; ++s) {
-        const double* q = sQ + (c * S + s) * 5;
-        acc += k < 5 ? q[k] : (k < 8 ? q[k - 4] : q[4] / (fmax(q[0], 1e-10) * R_AIR));
-      }
+      for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 6 + col];
       sM[c * 9 + k] = acc / S;
     }
     __syncthreads();
     for (int t = tid; t < C * S; t += MX_THREADS) {
       const int c = t % C, s = t / C;
-      const double* q = sQ + (c * S + s) * 5;
+      const double* q = sQ + (c * S + s) * 6;
       if (c < nc) {
         const float mutf = (visc && nut) ? float(q[0] * nut[(size_t)(e0 + c) * S + s]) : 0.f;
         float4* o = reinterpret_cast<float4*>(mb.PFm + ((size_t)(e0 + c) * S + s) * 20);
@@ -277,7 +322,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         o[4] = make_float4(float(q[3]), float(q[4]), 0.f, 0.f);
       }
       if (visc) {
-        const double phi[4] = {q[1], q[2], q[3], q[4] / (fmax(q[0], 1e-10) * R_AIR)};
+        const double phi[4] = {q[1], q[2], q[3], q[5]};
 #pragma unroll
         for (int f = 0; f < 4; ++f)
           mxd::st_split(sA1, 128 * Sq, tc::kmajor_index(f * C + c, s, 128), float(phi[f] - sM[c * 9 + 5 + f]));
@@ -508,10 +553,13 @@ struct MxVolSmem {
   static constexpr int oR2 = oR1 + szR1;  // q (FP64) before the first product, then dq, then the RV tile
   static constexpr int szR2 = cmax(cmax(C * QS * 4, C * S * 5 * 8), C * S * 10 * 4);
   static constexpr int oX = oR2 + szR2;
-  static constexpr int nX = C * 5 + C * 15;  // doubles: qbar, F(qbar)
+  // doubles: qbar, F(qbar); with VP also det and the metric divergence of the tile
+  static constexpr int nX = C * 5 + C * 15 + (VP ? C * S * 4 : 0);
   static constexpr int total = oX + nX * 8;
-  static constexpr int cFq = 0, cD3 = Fq, cW = Fq + Sq;  // TMEM column bases
-  static constexpr int NCOL = pow2_cols(Fq + 2 * Sq);
+  // TMEM columns: each product holds two column blocks (stacked hi / lo operand)
+  static constexpr int cFq = 0, cD3 = 2 * Fq, cW = 2 * Fq + (VP ? 2 * Sq : 0);
+  static constexpr int NCOL = pow2_cols(cW + 2 * Sq);
+  static_assert(cW + 2 * Sq <= NCOL, "tensor memory columns");
 };
 
 template <int S, int FN, int C>
@@ -521,6 +569,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
   using L = MxVolSmem<S, FN, C>;
   constexpr int Sq = L::Sq, Fq = L::Fq, QS = L::QS, NT = MX_VOL_THREADS;
   static_assert(C % 8 == 0 && 5 * C <= 128, "tile rows (v, c) must fit 128 lanes in groups of 8 cells");
+  static_assert(L::NCOL <= 256 && L::total <= 227 * 1024, "tensor memory / shared memory budget");
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tbase;
@@ -536,6 +585,8 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
   float* sR = reinterpret_cast<float*>(smem + L::oR2);
   double* sQb = reinterpret_cast<double*>(smem + L::oX);  // [c][5]
   double* sFb = sQb + C * 5;                              // [c][n][v] Euler flux at qbar
+  double* sDet = sFb + C * 15;                            // [c][s] 1/det (VP)
+  double* sMD = sDet + C * S;                             // [c][s][3] (VP)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool visc = L::VP && !inviscid_only;
   const int ct = cell_type(g, cell_base);
@@ -577,11 +628,20 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         mxd::prefetch_l2(g.adj, NS * 72, en * S * 72, nn * S * 72);
       }
     }
-    // ---- primitives (FP64) and cell means ----
+    // ---- primitives (FP64), det and metric divergence of the tile ----
     for (int t = tid; t < C * S; t += NT) {
       const int c = t / S;
-      double q[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
-      if (c < nc) cons_to_prim(Ucur + ((size_t)e0 * S + t) * nv, q);
+      double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
+      if (c < nc) {
+        const size_t p = (size_t)e0 * S + t;
+        mxd::prim_T(Ucur + p * nv, q);
+        if (L::VP) {
+          sDet[t] = 1.0 / g.det[p];  // reciprocal: the readouts multiply
+          sMD[t * 3 + 0] = mo.MD[p * 3 + 0];
+          sMD[t * 3 + 1] = mo.MD[p * 3 + 1];
+          sMD[t * 3 + 2] = mo.MD[p * 3 + 2];
+        }
+      }
 #pragma unroll
       for (int v = 0; v < 5; ++v) sQ[t * 5 + v] = q[v];
     }
@@ -621,9 +681,6 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
           const float4* pf = reinterpret_cast<const float4*>(PFm + p * 20);
           const float4 g0 = __ldg(pf), g1 = __ldg(pf + 1), g2 = __ldg(pf + 2), g3 = __ldg(pf + 3);
           const double* am = g.adj + p * 9;
-          double amd[9];
-#pragma unroll
-          for (int k = 0; k < 9; ++k) amd[k] = __ldg(am + k);
           float q[5];
 #pragma unroll
           for (int v = 0; v < 5; ++v) q[v] = float(sQ[(c * S + s) * 5 + v]);
@@ -633,7 +690,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
           viscous_flux<float>(q, gv, gT, mu, g3.x, G);
 #pragma unroll
           for (int m = 0; m < 3; ++m) {
-            const float x0 = float(amd[m * 3]), x1 = float(amd[m * 3 + 1]), x2 = float(amd[m * 3 + 2]);
+            const float x0 = float(__ldg(am + m * 3)), x1 = float(__ldg(am + m * 3 + 1)), x2 = float(__ldg(am + m * 3 + 2));
 #pragma unroll
             for (int v = 0; v < 5; ++v) Gt[m][v] = x0 * G[0][v] + x1 * G[1][v] + x2 * G[2][v];
           }
@@ -649,8 +706,8 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     __syncthreads();
     if (tid == 0) {
       tc::fence_after();
-      mxd::mma_split(tmem + L::cFq, sAc, sBc, Fq, Sq);
-      if (visc) mxd::mma_split(tmem + L::cD3, sAD, sBD, Sq, 3 * Sq);
+      mxd::mma_cat(tmem + L::cFq, sAc, sBc, Fq, Sq);
+      if (visc) mxd::mma_cat(tmem + L::cD3, sAD, sBD, Sq, 3 * Sq);
       tc::commit(&bar);
       if (!mxd::wait_commit(&bar, phase, status)) abort_flag = 1;
     }
@@ -660,12 +717,13 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     // ---- fine-point deviations dq = c2f*(q - qbar): TMEM -> shared ----
     if (q4 * 32 < 5 * C) {
       for (int ch = wsplit; ch < Fq / 8; ch += nsplit) {
-        float v8[8];
+        float v8[8], w8[8];
         tc::tmem_ld8(tmem + lane_base + L::cFq + ch * 8, v8);
+        tc::tmem_ld8(tmem + lane_base + L::cFq + Fq + ch * 8, w8);
         if (lrow < 5 * C) {
           const int v = lrow / C, c = lrow % C;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) sQf[c * QS + (ch * 8 + j) * 5 + v] = v8[j];
+          for (int j = 0; j < 8; ++j) sQf[c * QS + (ch * 8 + j) * 5 + v] = v8[j] + w8[j];
         }
       }
     }
@@ -681,9 +739,6 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         for (int v = 0; v < 5; ++v) Ft[m][v] = 0.f;
       if (c < nc && i < FN) {
         const double* ad = g.adj_fine + ((size_t)(e0 + c) * FN + i) * 9;
-        double add[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) add[k] = __ldg(ad + k);
         float qb[5], dq[5], dF[3][5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -693,7 +748,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         mxd::euler_flux_delta(qb, dq, dF);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          const float x0 = float(add[m * 3]), x1 = float(add[m * 3 + 1]), x2 = float(add[m * 3 + 2]);
+          const float x0 = float(__ldg(ad + m * 3)), x1 = float(__ldg(ad + m * 3 + 1)), x2 = float(__ldg(ad + m * 3 + 2));
 #pragma unroll
           for (int v = 0; v < 5; ++v) Ft[m][v] = x0 * dF[0][v] + x1 * dF[1][v] + x2 * dF[2][v];
         }
@@ -708,23 +763,25 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     __syncthreads();
     if (tid == 0) {
       tc::fence_after();
-      mxd::mma_split(tmem + L::cW, sAW, sBW, Sq, 3 * Fq);
+      mxd::mma_cat(tmem + L::cW, sAW, sBW, Sq, 3 * Fq);
       tc::commit(&bar);
     }
     // viscous divergence while the W product runs (its columns are complete);
     // the dq tile is consumed, so the RV tile reuses its space
     if (q4 * 32 < 5 * C) {
       for (int ch = wsplit; ch < Sq / 8; ch += nsplit) {
-        float v8[8];
-        if (visc) tc::tmem_ld8(tmem + lane_base + L::cD3 + ch * 8, v8);
+        float v8[8], w8[8];
+        if (visc) {
+          tc::tmem_ld8(tmem + lane_base + L::cD3 + ch * 8, v8);
+          tc::tmem_ld8(tmem + lane_base + L::cD3 + Sq + ch * 8, w8);
+        }
         if (lrow < 5 * C) {
           const int v = lrow / C, c = lrow % C;
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int s = ch * 8 + j;
             if (s < S && c < nc)
-              sR[(c * S + s) * 10 + 5 + v] =
-                  visc ? float(double(v8[j]) / g.det[(size_t)(e0 + c) * S + s]) : 0.f;
+              sR[(c * S + s) * 10 + 5 + v] = visc ? float(double(v8[j] + w8[j]) * sDet[c * S + s]) : 0.f;
           }
         }
       }
@@ -736,8 +793,9 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     // ---- inviscid volume term: -(W*dFt + MD*F(qbar)) / det ----
     if (q4 * 32 < 5 * C) {
       for (int ch = wsplit; ch < Sq / 8; ch += nsplit) {
-        float v8[8];
+        float v8[8], w8[8];
         tc::tmem_ld8(tmem + lane_base + L::cW + ch * 8, v8);
+        tc::tmem_ld8(tmem + lane_base + L::cW + Sq + ch * 8, w8);
         if (lrow < 5 * C) {
           const int v = lrow / C, c = lrow % C;
 #pragma unroll
@@ -745,9 +803,10 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
             const int s = ch * 8 + j;
             if (s < S && c < nc) {
               const size_t p = (size_t)(e0 + c) * S + s;
-              const double* md = mo.MD + p * 3;
+              const double* md = L::VP ? sMD + (c * S + s) * 3 : mo.MD + p * 3;
+              const double rdj = L::VP ? sDet[c * S + s] : 1.0 / g.det[p];
               const double mdf = md[0] * sFb[c * 15 + v] + md[1] * sFb[c * 15 + 5 + v] + md[2] * sFb[c * 15 + 10 + v];
-              sR[(c * S + s) * 10 + v] = float(-(double(v8[j]) + mdf) / g.det[p]);
+              sR[(c * S + s) * 10 + v] = float(-(double(v8[j] + w8[j]) + mdf) * rdj);
             }
           }
         }
@@ -773,23 +832,26 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
 // color order (staged in shared memory), outlier zeroing, then the SSP-RK3
 // combination, positivity and filter in FP64 (or the residual-only outputs).
 // ---------------------------------------------------------------------------
-constexpr int MX_UPD_THREADS = 256;
 constexpr int MX_UPD_MAXSLOT = 8;  // slots per cell staged in shared memory (more: read from global)
 
 template <int S, int NP, int CPB>
 struct MxUpdSmem {
+  static constexpr int THREADS = 256;
   static constexpr int oRi = 0;                        // CPB*S*5 doubles
   static constexpr int oRv = oRi + CPB * S * 5;
   static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*8
   static constexpr int oW = oU + CPB * S * 8;          // outliers: CPB*40
   static constexpr int oP = oW + CPB * 40;             // CPB*S
-  static constexpr int nD = (oP + CPB * S + 1) / 2 * 2;  // doubles (even: the jumps start 16-byte aligned)
+  static constexpr int oG = oP + CPB * S;            // g_left, g_right (2*4)
+  static constexpr int nD = (oG + 8 + 1) / 2 * 2;     // doubles (even: the jumps start 16-byte aligned)
   static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats
-  static constexpr int total = nD * 8 + nJ * 4;
+  // ints: slot flags of the staged slots, per-cell slot pointers, distribution maps
+  static constexpr int nI = CPB * MX_UPD_MAXSLOT + CPB + 1 + 6 * S;
+  static constexpr int total = nD * 8 + nJ * 4 + nI * 4;
 };
 
 template <int S, int NP, int CPB>
-__global__ void __launch_bounds__(MX_UPD_THREADS)
+__global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm) {
   using L = MxUpdSmem<S, NP, CPB>;
   extern __shared__ double smu[];
@@ -798,13 +860,28 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
   double* sU = smu + L::oU;
   double* work = smu + L::oW;
   double* part = smu + L::oP;
+  double* sGw = smu + L::oG;  // [0..3] g_left, [4..7] g_right
   float* sJ = reinterpret_cast<float*>(smu + L::nD);
+  int* sFl = reinterpret_cast<int*>(sJ + L::nJ);
+  int* sPtr = sFl + CPB * MX_UPD_MAXSLOT;
+  int* sDfp = sPtr + CPB + 1;
+  int* sDco = sDfp + 3 * S;
   const int e0 = a.cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, a.cell_end - e0);
   const int ct = cell_type(g, e0);
   const int nv = a.nv;
   const bool visc = !a.inviscid_only;
   const int tid = threadIdx.x;
+  constexpr int N1D = S == 8 ? 2 : (S == 27 ? 3 : 4);
+  for (int t = tid; t < 3 * S; t += blockDim.x) {
+    sDfp[t] = ops.dist_fp[t];
+    sDco[t] = ops.dist_co[t];
+  }
+  if (tid < N1D) {
+    sGw[tid] = ops.g_left[tid];
+    sGw[4 + tid] = ops.g_right[tid];
+  }
+  if (tid <= nc) sPtr[tid] = fc.slot_ptr[e0 + tid];
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
     const size_t p = (size_t)e0 * S + t / 5;
     sRi[t] = double(RV[p * 10 + t % 5]);
@@ -814,7 +891,10 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
     for (int v = 0; v < nv; ++v) sU[p * 8 + v] = a.Ucur[((size_t)e0 * S + p) * nv + v];
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
   const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
-  if (staged) mxd::copy_f32(sJ, Jm + (size_t)k_beg * NP * 10, (k_end - k_beg) * NP * 10);
+  if (staged) {
+    mxd::copy_f32(sJ, Jm + (size_t)k_beg * NP * 10, (k_end - k_beg) * NP * 10);
+    for (int t = tid; t < k_end - k_beg; t += blockDim.x) sFl[t] = a.slot_flags[k_beg + t];
+  }
   __syncthreads();
   // lift the jumps of each cell's slots, ascending color order
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
@@ -822,11 +902,11 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
     const int e = e0 + b;
     const double rdj = 1.0 / g.det[(size_t)e * S + s];  // one division per point (no bitwise target here)
     double ci = 0.0, cv = 0.0;
-    for (int k = fc.slot_ptr[e]; k < fc.slot_ptr[e + 1]; ++k) {
-      const int fl = a.slot_flags[k];
+    for (int k = sPtr[b]; k < sPtr[b + 1]; ++k) {
+      const int fl = staged ? sFl[k - k_beg] : a.slot_flags[k];
       const int ax = (fl >> 2) & 3;
-      const int fp = ops.dist_fp[ax * S + s];
-      const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
+      const int fp = sDfp[ax * S + s];
+      const double gw = sGw[((fl & 16) ? 4 : 0) + sDco[ax * S + s]];
       const float* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10;
       ci -= gw * double(Jk[v]);
       if (visc) cv += gw * double(Jk[5 + v]);
@@ -865,9 +945,11 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
     } else {
       for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v];
     }
+    // positivity (core/time_integration/positivity.py:13-45), one reciprocal of rho
     const double rho = fmax(un[0], 1e-6);
     un[0] = rho;
-    double vel[3] = {un[1] / rho, un[2] / rho, un[3] / rho};
+    const double rr = 1.0 / rho;
+    double vel[3] = {un[1] * rr, un[2] * rr, un[3] * rr};
     const double vm = sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
     if (vm > 1e4) {
       const double cf = 1e4 / vm;
@@ -882,13 +964,14 @@ __global__ void __launch_bounds__(MX_UPD_THREADS)
     part[p] = sq_sum;
   }
   __syncthreads();
+  // modal filter; lanes of a warp share the filter row s (broadcast loads)
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
-    const int p = t / 5, v = t % 5;
-    const int b = p / S, s = p % S;
+  for (int t = tid; t < S * CPB * 5; t += blockDim.x) {
+    const int s = t / (CPB * 5), r = t % (CPB * 5), b = r / 5, v = r % 5;
+    if (b >= nc) continue;
     double acc = 0.0;
     for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * sU[(b * S + j) * 8 + v];
-    a.Unext[((size_t)e0 * S + p) * nv + v] = acc;
+    a.Unext[((size_t)(e0 + b) * S + s) * nv + v] = acc;
   }
   for (int p = tid; p < nc * S; p += blockDim.x)
     for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = sU[p * 8 + v];
