@@ -56,7 +56,10 @@ struct afr_handle {
   MxFace mf{};
   MxBuf mb{};
   int mx_pre_blocks = 0, mx_cell_blocks = 0;  // resident CTAs of the persistent kernels
-  int mx_pre_per_sm = 0;
+  int mx_pre_per_sm = 0, mx_pre_max_per_sm = 0, n_sms = 0;
+  // launch shapes chosen by afr_autotune (defaults until then)
+  int mx_face_block = 128;  // threads per face-kernel CTA: 64, 128 or 256
+  int mx_upd_var = 1;       // update-kernel cells per CTA: 0 = half, 1 = base, 2 = double
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   std::string err;
@@ -254,6 +257,7 @@ struct Launch {
   static constexpr int MXU = S <= 8 ? 16 : (S <= 27 ? 4 : 2);  // cells per update-kernel CTA
   static size_t mx_pre_smem() { return MxPreSmem<S, NP>::total; }
   static size_t mx_vol_smem() { return MxVolSmem<S, FN, MXC>::total; }
+  static constexpr int MXU0 = MXU / 2 > 0 ? MXU / 2 : 1, MXU2 = MXU * 2;  // autotuner candidates
   static size_t mx_upd_smem() { return MxUpdSmem<S, NP, MXU>::total; }
   // resident CTAs per SM of the persistent kernels, capped by tensor memory (512 columns per SM)
   static cudaError_t mx_grids(afr_handle* h) {
@@ -267,6 +271,12 @@ struct Launch {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_mx_update<S, NP, MXU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)mx_upd_smem());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_update<S, NP, MXU0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)MxUpdSmem<S, NP, MXU0>::total);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_mx_update<S, NP, MXU2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)MxUpdSmem<S, NP, MXU2>::total);
     // the largest shared-memory carveout for the two persistent kernels, whose
     // shared memory sets how many CTAs fit on an SM
     if (e == cudaSuccess)
@@ -286,8 +296,14 @@ struct Launch {
     if (bp < 1 || bc < 1) return cudaErrorInvalidConfiguration;
     h->mx_pre_blocks = bp * sms;
     h->mx_cell_blocks = bc * sms;
-    h->mx_pre_per_sm = bp;
+    h->mx_pre_per_sm = h->mx_pre_max_per_sm = bp;
+    h->n_sms = sms;
     return cudaSuccess;
+  }
+  template <int CPB>
+  static void mx_update_launch(afr_handle* h, const StageArgs& a, int n, cudaStream_t st) {
+    k_mx_update<S, NP, CPB><<<(n + CPB - 1) / CPB, MxUpdSmem<S, NP, CPB>::THREADS, MxUpdSmem<S, NP, CPB>::total, st>>>(
+        h->g, h->ops, h->fc, a, h->mb.RV, h->mb.Jm);
   }
   static int n_ranges(const afr_handle* h) { return (h->n_prism > 0 ? 1 : 0) + (h->N > h->n_prism ? 1 : 0); }
   static cudaError_t mx_pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
@@ -304,8 +320,8 @@ struct Launch {
   static cudaError_t mx_stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm) {
     const int nt = h->slots.n * NP;
     if (nt > 0)
-      k_mx_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell,
-                                                         (float)h->prm.mu, a.inviscid_only ? 0 : 1);
+      k_mx_face<S, NP><<<(nt + h->mx_face_block - 1) / h->mx_face_block, h->mx_face_block, 0, st>>>(
+          h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell, (float)h->prm.mu, a.inviscid_only ? 0 : 1);
     if (tm) tm->mark(st);
     const int ranges[3] = {0, h->n_prism, h->N};
     for (int r = 0; r < 2; ++r) {
@@ -324,8 +340,9 @@ struct Launch {
       a.cell_end = ranges[r + 1];
       const int n = a.cell_end - a.cell_base;
       if (n <= 0) continue;
-      k_mx_update<S, NP, MXU><<<(n + MXU - 1) / MXU, MxUpdSmem<S, NP, MXU>::THREADS, mx_upd_smem(), st>>>(h->g, h->ops, h->fc, a,
-                                                                                        h->mb.RV, h->mb.Jm);
+      if (h->mx_upd_var == 0) mx_update_launch<MXU0>(h, a, n, st);
+      else if (h->mx_upd_var == 2) mx_update_launch<MXU2>(h, a, n, st);
+      else mx_update_launch<MXU>(h, a, n, st);
     }
     return cudaGetLastError();
   }
@@ -719,6 +736,28 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
   cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
   h->prec = AFR_PREC_MIXED;
+  // The dense per-record interpolation matrices are read afterwards only by
+  // the general (unmatched) face points and by the SST face kernel: release
+  // them when neither exists.
+  if (ns && h->prm.turb != AFR_TURB_SST) {
+    std::vector<uint8_t> o(ns * P);
+    e = cudaMemcpy(o.data(), ofp, o.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
+    bool all_matched = true;
+    for (uint8_t v : o) all_matched = all_matched && v != MX_OFP_GENERAL;
+    if (all_matched) {
+      const double* mats[4] = {h->fc.nb_m0, h->fc.nb_m1, h->fc.ow_m0, h->fc.ow_m1};
+      const size_t rows[4] = {(size_t)h->F, (size_t)m->n_nb_src1, (size_t)h->F, (size_t)m->n_ow_src1};
+      for (int i = 0; i < 4; ++i) {
+        auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)mats[i]);
+        if (it == h->allocs.end()) continue;
+        h->allocs.erase(it);
+        cudaFree((void*)mats[i]);
+        h->bytes -= std::max<size_t>(rows[i] * P * S, 1) * sizeof(double);
+      }
+      h->fc.nb_m0 = h->fc.nb_m1 = h->fc.ow_m0 = h->fc.ow_m1 = nullptr;
+    }
+  }
   return AFR_OK;
 }
 
@@ -1001,7 +1040,8 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
       return bail(rc);
     cudaStreamSynchronize(st);
     h->slots = SlotTable{(int32_t)ns, d_f, d_c, d_fl, d_0, d_1, d_i1};
-    if ((rc = dalloc(h, &h->J, ns * P * 10))) return bail(rc);
+    // FP64 jumps: the plain stage only
+    if (prm->precision != AFR_PREC_MIXED && (rc = dalloc(h, &h->J, ns * P * 10))) return bail(rc);
   }
   // ---- boundary condition table ----
   {
@@ -1148,6 +1188,137 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
 
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
   return step_impl(h, U, k, omega, nu_t, norm_out, (cudaStream_t)stream, nullptr, nullptr);
+}
+
+// ---- launch-shape autotuner (mixed form) ----
+namespace {
+// device time of one residual evaluation (both residuals) with the current launch shapes, best of reps
+float time_eval(afr_handle* h, const double* U, const double* nut, double* Rinv, double* Rvisc, cudaStream_t st,
+                int reps) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int r = 0; r < reps + 1; ++r) {
+    StageArgs a = base_args(h);
+    a.Ucur = U;
+    a.stage = -1;
+    a.nut = nut;
+    a.Rinv = Rinv;
+    a.Rvisc = Rvisc;
+    cudaEventRecord(e0, st);
+    dispatch(h, [&](auto L) { return L.eval(h, a, U, nut, !h->prm.inviscid_only, st); });
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0) best = std::min(best, ms);  // the first run warms caches and code
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+__global__ void k_segment_sums(const double* __restrict__ part, const int64_t* __restrict__ ptr, double* out) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int64_t i = ptr[blockIdx.x] + threadIdx.x; i < ptr[blockIdx.x + 1]; i += blockDim.x) acc += part[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+}  // namespace
+
+int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* choice_out, void* stream) {
+  if (!h || !U) return AFR_EINVAL;
+  if (h->prec != AFR_PREC_MIXED) {
+    if (choice_out) choice_out[0] = choice_out[1] = choice_out[2] = -1;
+    return AFR_OK;  // the plain form keeps its fixed shapes
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)h->N * h->S * h->nv;
+  double *Ri = nullptr, *Rv = nullptr;
+  if (cudaMalloc((void**)&Ri, n * sizeof(double)) != cudaSuccess || cudaMalloc((void**)&Rv, n * sizeof(double)) != cudaSuccess) {
+    cudaFree(Ri);
+    return fail(h, AFR_ENOMEM, "autotune scratch");
+  }
+  const double* nut = h->prm.turb == AFR_TURB_SST ? nu_t : nullptr;
+  // coordinate search: pre-pass CTAs per SM, face-kernel block, update-kernel cells per CTA
+  {
+    int best = h->mx_pre_per_sm;
+    float tb = 1e30f;
+    for (int c = 1; c <= h->mx_pre_max_per_sm; ++c) {
+      h->mx_pre_per_sm = c;
+      h->mx_pre_blocks = c * h->n_sms;
+      const float t = time_eval(h, U, nut, Ri, Rv, st, 3);
+      if (t < tb) { tb = t; best = c; }
+    }
+    h->mx_pre_per_sm = best;
+    h->mx_pre_blocks = best * h->n_sms;
+  }
+  {
+    const int cand[3] = {64, 128, 256};
+    int best = h->mx_face_block;
+    float tb = 1e30f;
+    for (int c : cand) {
+      h->mx_face_block = c;
+      const float t = time_eval(h, U, nut, Ri, Rv, st, 3);
+      if (t < tb) { tb = t; best = c; }
+    }
+    h->mx_face_block = best;
+  }
+  {
+    int best = h->mx_upd_var;
+    float tb = 1e30f;
+    for (int c = 0; c < 3; ++c) {
+      h->mx_upd_var = c;
+      const float t = time_eval(h, U, nut, Ri, Rv, st, 3);
+      if (t < tb) { tb = t; best = c; }
+    }
+    h->mx_upd_var = best;
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(Ri);
+  cudaFree(Rv);
+  if (e != cudaSuccess) return cuda_fail(h, e, "autotune");
+  if (choice_out) {
+    choice_out[0] = h->mx_pre_per_sm;
+    choice_out[1] = h->mx_face_block;
+    choice_out[2] = h->mx_upd_var;
+  }
+  return check_status(h, st);
+}
+
+int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, double* out, void* stream) {
+  if (!h || nseg <= 0 || !cell_ptr || !out) return AFR_EINVAL;
+  if (cell_ptr[0] < 0 || cell_ptr[nseg] > h->N) return fail(h, AFR_EINVAL, "segment bounds outside the mesh");
+  for (int i = 0; i < nseg; ++i)
+    if (cell_ptr[i + 1] < cell_ptr[i]) return fail(h, AFR_EINVAL, "segment pointers must not decrease");
+  cudaStream_t st = (cudaStream_t)stream;
+  int64_t* dptr = nullptr;
+  double* dsum = nullptr;
+  if (cudaMalloc((void**)&dptr, (nseg + 1) * sizeof(int64_t)) != cudaSuccess ||
+      cudaMalloc((void**)&dsum, nseg * sizeof(double)) != cudaSuccess) {
+    cudaFree(dptr);
+    return fail(h, AFR_ENOMEM, "segment scratch");
+  }
+  std::vector<double> sums(nseg);
+  cudaMemcpyAsync(dptr, cell_ptr, (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+  k_segment_sums<<<nseg, 256, 0, st>>>(h->norm_part, dptr, dsum);
+  cudaMemcpyAsync(sums.data(), dsum, nseg * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(dptr);
+  cudaFree(dsum);
+  if (e != cudaSuccess) return cuda_fail(h, e, "segment norms");
+  for (int i = 0; i < nseg; ++i) {
+    const double cnt = (double)(cell_ptr[i + 1] - cell_ptr[i]) * h->S * h->nv;
+    out[i] = cnt > 0 ? std::sqrt(sums[i]) / std::sqrt(cnt) : 0.0;
+  }
+  return AFR_OK;
 }
 
 int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* ms_out, int n_ms,

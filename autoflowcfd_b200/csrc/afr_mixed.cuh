@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
 // face kernel: one thread per (slot, flux point), fields read at face points
 // ---------------------------------------------------------------------------
 template <int S, int NP>
-__global__ void __launch_bounds__(128) k_mx_face(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
+__global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
                                                  const double* __restrict__ hcell, float mu, int visc) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= st.n * NP) return;

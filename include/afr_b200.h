@@ -205,6 +205,22 @@ int afr_greedy_face_coloring(int64_t n_faces, int64_t n_cells, const int64_t* ow
  * The sum order is fixed for a given n, so results are bitwise repeatable. */
 int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream);
 
+/* Launch-shape autotuner of the mixed form: times one residual evaluation of
+ * the state U (nu_t for SST handles) for each candidate pre-pass CTAs per SM,
+ * face-kernel block size (64/128/256) and update-kernel cells per CTA (half /
+ * base / double), one parameter at a time, and keeps the fastest in the
+ * handle.  U is not modified.  choice_out (3 ints, may be NULL) receives the
+ * choices; plain-form handles keep their fixed shapes (choices -1).  No
+ * counterpart in the reference (launch shapes have none there). */
+int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* choice_out, void* stream);
+
+/* Per-segment RMS residual norms of the last afr_step: segment i is cells
+ * [cell_ptr[i], cell_ptr[i+1]) (host array of nseg+1), the norm is
+ * sqrt(sum(dU/dt^2) / (cells * n_sps * n_vars)) over the segment, summed in a
+ * fixed order.  For several independent cases concatenated into one handle
+ * (state.py:99-108 per case).  Synchronises the stream. */
+int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, double* out, void* stream);
+
 /* Tensor-core self-check: D[128 x n] = A[128 x k] * B[n x k]^T on the
  * calling device with tcgen05.mma, A and B row-major BF16 bit patterns and D
  * row-major FP32, all device memory; 16 <= n, k <= 256, both multiples of 16.
