@@ -39,6 +39,7 @@ struct afr_handle {
   double* Ub = nullptr;
   double* dt = nullptr;
   double* norm_part = nullptr;
+  double* norm_rho_part = nullptr;
   double* red = nullptr;      // reduction results
   double* pt = nullptr;
   double* cfp = nullptr;
@@ -1075,6 +1076,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   if ((rc = dalloc(h, &h->Ub, N * S * h->nv))) return bail(rc);
   if ((rc = dalloc(h, &h->dt, N * S))) return bail(rc);
   if ((rc = dalloc(h, &h->norm_part, N))) return bail(rc);
+  if ((rc = dalloc(h, &h->norm_rho_part, N))) return bail(rc);
   if ((rc = dalloc(h, &h->red, 4))) return bail(rc);
   if (prm->turb == AFR_TURB_SST) {
     if ((rc = dalloc(h, &h->pt, N * S * 5))) return bail(rc);
@@ -1163,6 +1165,7 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
       a.nut = sst ? nu_t : nullptr;
       a.dt = h->dt;
       a.norm_part = h->norm_part;
+      a.norm_rho_part = h->norm_rho_part;
       a.stage = stg;
       r = L.eval(h, a, cur[stg], sst ? nu_t : nullptr, visc, st, tm, &nl);
       if (tm) tm->mark(st);
@@ -1293,8 +1296,9 @@ int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* ch
   return check_status(h, st);
 }
 
-int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, double* out, void* stream) {
-  if (!h || nseg <= 0 || !cell_ptr || !out) return AFR_EINVAL;
+int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t which, double* out,
+                      void* stream) {
+  if (!h || nseg <= 0 || !cell_ptr || !out || (which != 0 && which != 1)) return AFR_EINVAL;
   if (cell_ptr[0] < 0 || cell_ptr[nseg] > h->N) return fail(h, AFR_EINVAL, "segment bounds outside the mesh");
   for (int i = 0; i < nseg; ++i)
     if (cell_ptr[i + 1] < cell_ptr[i]) return fail(h, AFR_EINVAL, "segment pointers must not decrease");
@@ -1308,14 +1312,14 @@ int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, doub
   }
   std::vector<double> sums(nseg);
   cudaMemcpyAsync(dptr, cell_ptr, (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
-  k_segment_sums<<<nseg, 256, 0, st>>>(h->norm_part, dptr, dsum);
+  k_segment_sums<<<nseg, 256, 0, st>>>(which ? h->norm_rho_part : h->norm_part, dptr, dsum);
   cudaMemcpyAsync(sums.data(), dsum, nseg * sizeof(double), cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   cudaFree(dptr);
   cudaFree(dsum);
   if (e != cudaSuccess) return cuda_fail(h, e, "segment norms");
   for (int i = 0; i < nseg; ++i) {
-    const double cnt = (double)(cell_ptr[i + 1] - cell_ptr[i]) * h->S * h->nv;
+    const double cnt = (double)(cell_ptr[i + 1] - cell_ptr[i]) * h->S * (which ? 1 : h->nv);
     out[i] = cnt > 0 ? std::sqrt(sums[i]) / std::sqrt(cnt) : 0.0;
   }
   return AFR_OK;

@@ -25,6 +25,7 @@ struct StageArgs {
   double* Rinv;         // residual-only mode outputs (N,S,nv), may be null
   double* Rvisc;
   double* norm_part;    // (N) per-cell sum of squares of dU/dt (stage 0)
+  double* norm_rho_part;  // (N) per-cell sum of squares of the density column of dU/dt (stage 0)
   int nv;
   int stage;            // 0,1,2 RK stage, -1 residual only
   int inviscid_only;
@@ -530,6 +531,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
     for (int v = 0; v < nv; ++v) Up[p * 8 + v] = un[v];
     part[p] = sq_sum;
+    part[CPB * S + p] = Lr[0] * Lr[0];
   }
   __syncthreads();
   // modal filter on the first five variables; lanes of a warp share the
@@ -548,6 +550,9 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     double acc = 0.0;  // fixed order per cell: points ascending
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];
     a.norm_part[e0 + tid] = acc;
+    double acc_rho = 0.0;
+    for (int s = 0; s < S; ++s) acc_rho += part[CPB * S + tid * S + s];
+    a.norm_rho_part[e0 + tid] = acc_rho;
   }
 }
 

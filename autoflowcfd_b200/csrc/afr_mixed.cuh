@@ -841,8 +841,8 @@ struct MxUpdSmem {
   static constexpr int oRv = oRi + CPB * S * 5;
   static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*8
   static constexpr int oW = oU + CPB * S * 8;          // outliers: CPB*40
-  static constexpr int oP = oW + CPB * 40;             // CPB*S
-  static constexpr int oG = oP + CPB * S;            // g_left, g_right (2*4)
+  static constexpr int oP = oW + CPB * 40;             // 2*CPB*S: squared dU/dt, squared density column
+  static constexpr int oG = oP + 2 * CPB * S;        // g_left, g_right (2*4)
   static constexpr int nD = (oG + 8 + 1) / 2 * 2;     // doubles (even: the jumps start 16-byte aligned)
   static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats
   // ints: slot flags of the staged slots, per-cell slot pointers, distribution maps
@@ -962,6 +962,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
     for (int v = 0; v < nv; ++v) uc[v] = un[v];
     part[p] = sq_sum;
+    part[CPB * S + p] = Lr[0] * Lr[0];
   }
   __syncthreads();
   // modal filter; lanes of a warp share the filter row s (broadcast loads)
@@ -979,6 +980,9 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     double acc = 0.0;
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];
     a.norm_part[e0 + tid] = acc;
+    double acc_rho = 0.0;
+    for (int s = 0; s < S; ++s) acc_rho += part[CPB * S + tid * S + s];
+    a.norm_rho_part[e0 + tid] = acc_rho;
   }
 }
 

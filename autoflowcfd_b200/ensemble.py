@@ -7,7 +7,7 @@ every case of that order, and the steps of all order groups are replayed as
 one CUDA graph.  Per-cell arithmetic does not depend on which other cells
 share a launch (no cross-cell reductions, gathers stay inside a case), so each
 case gets exactly the result it gets alone; per-case FP64 residual norms come
-from ``afr_segment_norms`` and per-case Cd from the case's own wall faces.
+from ``afr_segment_norms``.
 
 All cases share one molecular viscosity: the Reynolds number of a case is set
 through its box length, L = Re * mu / (rho u), so a single ``mu`` serves
@@ -15,7 +15,7 @@ every Mach number of the draw.
 """
 
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -53,6 +53,7 @@ class EnsembleCase:
     seed: int
     lengths: tuple          # box size (m)
     jitter: float = 0.1
+    bump_x: float = 0.5     # streamwise bump position as a fraction of Lx
 
     @property
     def velocity(self) -> float:
@@ -89,14 +90,14 @@ def plane_config(spec: EnsembleCase) -> Dict[str, dict]:
     return cfg
 
 
-def build_case(spec: EnsembleCase) -> Dict[str, np.ndarray]:
+def build_case(spec: EnsembleCase, wall_distance: bool = False) -> Dict[str, np.ndarray]:
     """Tables of one case (reference layout) from the box generator."""
     from . import boxgeom, boxmesh
 
     Lx, Ly, Lz = spec.lengths
-    bump = (spec.bump * Lz, 0.5 * Lx, 0.5 * Ly, 0.25 * Lz) if spec.bump > 0 else None
+    bump = (spec.bump * Lz, spec.bump_x * Lx, 0.5 * Ly, 0.25 * Lz) if spec.bump > 0 else None
     box = boxmesh.prism_box(*spec.shape, spec.lengths, jitter=spec.jitter, seed=spec.seed, bump=bump)
-    return boxgeom.build_case(box, spec.order, plane_config(spec), wall_distance=False)
+    return boxgeom.build_case(box, spec.order, plane_config(spec), wall_distance=wall_distance)
 
 
 def uniform_state(spec: EnsembleCase, n_cells: int, n_sps: int) -> np.ndarray:
@@ -172,7 +173,6 @@ class _Group:
     members: List[int]                 # case indices in the draw
     cell_ptr: np.ndarray               # (len(members)+1,) cell ranges inside the group
     solver: object = None
-    face_ranges: List[tuple] = field(default_factory=list)
 
 
 class B200Ensemble:
@@ -247,15 +247,16 @@ class B200Ensemble:
         return out
 
     # --------------------------------------------------------------- results
-    def norms(self) -> np.ndarray:
-        """Per-case FP64 RMS residual norms of the last step, in draw order."""
+    def norms(self, density: bool = False) -> np.ndarray:
+        """Per-case FP64 RMS residual norms of the last step (all variables, or
+        the density column), in draw order."""
         from .solver import _stream
 
         res = np.zeros(len(self.specs))
         for g in self.groups:
             out = np.zeros(len(g.members))
             check(LIB.afr_segment_norms(g.solver._h, len(g.members), g.cell_ptr.ctypes.data_as(_lib._P_I64),
-                                        out.ctypes.data_as(_lib._P_D), _stream()), g.solver._h)
+                                        1 if density else 0, out.ctypes.data_as(_lib._P_D), _stream()), g.solver._h)
             res[g.members] = out
         return res
 

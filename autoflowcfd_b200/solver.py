@@ -186,6 +186,15 @@ class B200FRSolver:
             return norm.value
         return float("nan")
 
+    def density_residual(self) -> float:
+        """RMS of the density column of dU/dt at the last step (FP64), the
+        quantity a steady solve's stopping rule watches."""
+        ptr = np.array([0, self.n_cells], dtype=np.int64)
+        out = np.zeros(1)
+        check(LIB.afr_segment_norms(self._h, 1, ptr.ctypes.data_as(_lib._P_I64), 1, out.ctypes.data_as(_lib._P_D),
+                                    _stream()), self._h)
+        return float(out[0])
+
     def solve(self, max_iter: int = 1000, dt: float = 1e-3, tol: float = 1e-6, output_interval: int = 0) -> dict:
         """GPUFRSolver.solve (core/gpu/gpu_solver.py:403-453): stops on tol or a
         non-finite norm."""

@@ -365,6 +365,49 @@ def run_ensemble(args):
     ens.cleanup()
 
 
+def run_serve(args):
+    """C5: serving loop (Poisson arrivals, HBM-gated admission, continuous batching)."""
+    import torch
+
+    from autoflowcfd_b200 import serving as SV
+    from autoflowcfd_b200.solver import B200FRSolver
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    reqs = SV.poisson_requests(args.requests, rate_per_s=4.0, seed=args.seed)
+    lp = SV.ServingLoop(precision="mixed" if args.form == "both" else args.form, turb=args.turb,
+                        max_active=args.max_active, steps_per_slice=10, drop=1e-6, max_iter=args.max_iter)
+    t0 = time.perf_counter()
+    results = lp.run(reqs)
+    wall = time.perf_counter() - t0
+    summary = SV.latency_summary(results, wall)
+    # FP64 re-solve of 5 % of the requests (at least two), same number of steps, alone
+    rng = np.random.default_rng(args.seed + 1)
+    pick = sorted(rng.choice(len(results), size=max(2, len(results) // 20), replace=False).tolist())
+    byid = {r.rid: r for r in results}
+    cd_err = []
+    for i in pick:
+        r = byid[reqs[i].rid]
+        ref = SV.ServingLoop(precision="fp64", turb=args.turb, max_active=1, steps_per_slice=10, drop=1e-6,
+                             max_iter=r.iterations - 1).run([SV.SolveRequest(r.rid, 0.0, reqs[i].spec)])[0]
+        cd_err.append(abs(r.cd - ref.cd) / max(abs(ref.cd), 1e-300))
+    cells = [r.n_cells for r in results]
+    line = {
+        "metric": "serving: solves/hour, p50/p99 latency (s)", "value": summary["solves_per_hour"],
+        "unit": "solves/hour", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x2 split tensor-core contractions (f32 accumulate), f32 fluxes, f64 state",
+        "data": "synthetic (seeded Poisson request stream)",
+        "config": {"workload": "C5 serving: Poisson 4 req/s, prism boxes 8k-200k hex, P1/P2, Mach 0.05-0.25, "
+                               "parametric wall bump", "requests": len(reqs), "physics": args.turb,
+                   "stop": "density residual drop 1e-6 or max_iter", "max_iter": args.max_iter,
+                   "max_active": args.max_active, "admission": "free device memory (cudaMemGetInfo) minus reserve",
+                   "cells_range": [int(min(cells)), int(max(cells))]},
+        "latency": summary, "wall_s": wall, "peak_active": lp.peak_active,
+        "cd_vs_fp64_resolve": {"requests": [int(reqs[i].rid) for i in pick], "max_rel_err": float(max(cd_err)),
+                               "mean_rel_err": float(np.mean(cd_err))},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,7 +418,11 @@ def main():
     ap.add_argument("--small", action="store_true", help="24x20x18 hex instead of 96x80x72 (profiling)")
     ap.add_argument("--shape", default=None, help="nx,ny,nz hex cells of a profiling-size box")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "ensemble"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "ensemble", "serve"])
+    ap.add_argument("--requests", type=int, default=32, help="serve: number of requests")
+    ap.add_argument("--max-iter", type=int, default=200, help="serve: step cap per request")
+    ap.add_argument("--max-active", type=int, default=16, help="serve: admitted requests at most")
+    ap.add_argument("--turb", default="NONE", choices=["NONE", "SST"], help="serve: physics of the requests")
     ap.add_argument("--cases", type=int, default=256, help="ensemble: number of cases")
     ap.add_argument("--seed", type=int, default=2024, help="ensemble: draw seed")
     args = ap.parse_args()
@@ -386,6 +433,9 @@ def main():
         return
     if args.workload == "ensemble":
         run_ensemble(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
         return
 
     import torch

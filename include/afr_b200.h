@@ -215,11 +215,15 @@ int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream);
 int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* choice_out, void* stream);
 
 /* Per-segment RMS residual norms of the last afr_step: segment i is cells
- * [cell_ptr[i], cell_ptr[i+1]) (host array of nseg+1), the norm is
- * sqrt(sum(dU/dt^2) / (cells * n_sps * n_vars)) over the segment, summed in a
- * fixed order.  For several independent cases concatenated into one handle
- * (state.py:99-108 per case).  Synchronises the stream. */
-int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, double* out, void* stream);
+ * [cell_ptr[i], cell_ptr[i+1]) (host array of nseg+1).  which = 0: the norm
+ * over all variables, sqrt(sum(dU/dt^2) / (cells * n_sps * n_vars)), as
+ * FRState.get_residual_norm (state.py:99-108); which = 1: the density column
+ * only, sqrt(sum((drho/dt)^2) / (cells * n_sps)).  Summed in a fixed order.
+ * For several independent cases concatenated into one handle, and for the
+ * density-residual stopping rule of a steady solve (nseg = 1).  Synchronises
+ * the stream. */
+int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t which, double* out,
+                      void* stream);
 
 /* Tensor-core self-check: D[128 x n] = A[128 x k] * B[n x k]^T on the
  * calling device with tcgen05.mma, A and B row-major BF16 bit patterns and D

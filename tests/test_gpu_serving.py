@@ -1,0 +1,51 @@
+"""Serving loop on the GPU: requests admitted while others run (continuous
+batching on separate streams) finish with bitwise the state they reach alone."""
+import numpy as np
+import pytest
+
+from autoflowcfd_b200 import ensemble as E
+from autoflowcfd_b200 import serving as SV
+
+pytestmark = pytest.mark.gpu
+
+
+def requests():
+    specs = [E.EnsembleCase((6, 3, 3), 2, 0.1, 0.05, 31, (0.15, 0.075, 0.075), bump_x=0.4),
+             E.EnsembleCase((4, 2, 2), 1, 0.2, 0.0, 32, (0.07, 0.035, 0.035)),
+             E.EnsembleCase((8, 4, 4), 2, 0.08, 0.07, 33, (0.2, 0.1, 0.1), bump_x=0.6)]
+    return [SV.SolveRequest(i, 0.0, s) for i, s in enumerate(specs)]
+
+
+TABLES = {}
+
+
+def tables():
+    if not TABLES:
+        TABLES.update({r.rid: E.build_case(r.spec) for r in requests()})
+    return TABLES
+
+
+def loop(**kw):
+    # drop 0: every request runs to max_iter, so alone and mixed runs take the same steps
+    return SV.ServingLoop(precision="mixed", max_active=2, steps_per_slice=5, drop=0.0, max_iter=20,
+                          keep_state=True, **kw)
+
+
+def test_results_same_alone_and_in_the_mix():
+    lp = loop()
+    mixed = {r.rid: r for r in lp.run(requests(), tables=tables())}
+    assert len(mixed) == 3 and lp.peak_active == 2  # two ran together, the third waited for a slot
+    for req in requests():
+        alone = loop().run([req], tables=tables())[0]
+        got = mixed[req.rid]
+        assert got.iterations == alone.iterations == 21  # iteration 1 plus four slices of five
+        assert got.status == alone.status == "max_iter"
+        assert np.array_equal(got.state, alone.state), req.rid
+        assert got.cd == alone.cd
+        assert got.latency_s >= 0
+
+
+def test_latency_summary():
+    res = loop().run(requests(), tables=tables())
+    s = SV.latency_summary(res, wall_s=10.0)
+    assert s["completed"] == 3 and s["p99_s"] >= s["p50_s"] > 0
