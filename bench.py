@@ -237,6 +237,22 @@ def run_reference(args, rank, world):
 SEGMENT = 8
 
 
+def max_over_ranks(times_ms, dist=None, device="cpu"):
+    """Per-rank device times -> the maximum over ranks (every rank gets it).
+    Replicas run independent cases, so the job's time is the slowest rank's."""
+    import torch
+
+    ts = torch.tensor(list(times_ms), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(ts, op=dist.ReduceOp.MAX)
+    return [float(v) for v in ts]
+
+
+def replica_throughput(world, units_per_rank_step, ms_per_step):
+    """Whole-job throughput of N replicas: all ranks' units over the max-over-ranks time."""
+    return world * units_per_rank_step / (ms_per_step * 1e-3)
+
+
 def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
     """Time one solver's steps (device-resident, restarted from the seeded
     state every SEGMENT steps), one breakdown step, and optionally the e2e
@@ -488,12 +504,10 @@ def main():
     del case
     dofs_per_step = N * S * 5 * 3
     head = res[forms[0]]
-    ts = torch.tensor([head["ms"], head.get("e2e_ms", 0.0)] + [res[f]["ms"] for f in forms], dtype=torch.float64,
-                      device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(ts, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = float(ts[0]), float(ts[1])
-    value = world * dofs_per_step / (ms * 1e-3)
+    ts = max_over_ranks([head["ms"], head.get("e2e_ms", 0.0)] + [res[f]["ms"] for f in forms], dist,
+                        device=f"cuda:{local}")
+    ms, ms_e2e = ts[0], ts[1]
+    value = replica_throughput(world, dofs_per_step, ms)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
@@ -527,7 +541,7 @@ def main():
                    "restart_every_steps": SEGMENT,
                    "l2": "inputs larger than L2 (state %.2f GB)" % (N * S * 7 * 8 / 1e9),
                    "mesh_gen_s": round(t_gen, 1)},
-        "e2e": {"value": world * dofs_per_step / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
+        "e2e": {"value": replica_throughput(world, dofs_per_step, ms_e2e), "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"], "ms_per_step": ms_e2e},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
@@ -540,7 +554,7 @@ def main():
     }
     if "fp64" in res and mixed_head:
         f64 = res["fp64"]
-        line["plain_fp64"] = {"value": world * dofs_per_step / (float(ts[3]) * 1e-3), "unit": UNIT,
+        line["plain_fp64"] = {"value": replica_throughput(world, dofs_per_step, ts[3]), "unit": UNIT,
                               "ms_per_step": float(ts[3]),
                               "breakdown_ms_per_step": f64["breakdown"].get("per_kernel_ms"),
                               "speedup_of_mixed": float(ts[3]) / ms}
