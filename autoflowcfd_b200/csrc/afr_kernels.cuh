@@ -38,6 +38,10 @@ struct StageArgs {
 
 __device__ __forceinline__ int cell_type(const Geom& g, int e) { return e < g.n_prism ? 0 : 1; }
 
+// Doubles per point of a state tile staged in shared memory (n_vars <= 7 used).
+// Odd, so that threads reading consecutive points' rows hit different banks.
+constexpr int US = 9;
+
 // out[r][c] (+)= sum_k A[r*lda + k] * B[k*ldb + c] for r<R, c<C; A global, B/out shared.
 template <int R, int C, int K>
 __device__ __forceinline__ void block_gemm(double* out, int ldo, const double* __restrict__ A, int lda,
@@ -122,9 +126,9 @@ __device__ void suppress_outliers_cells(double* sRi, double* sRv, const double* 
     const int bb = t / 5, v = t % 5;
     double* w = work + bb * 20;
     if (!(S & 1)) w[v] = 0.5 * (w[10 + v] + w[15 + v]);
-    const double* Ur = sU + (bb % nc) * S * 8;
+    const double* Ur = sU + (bb % nc) * S * US;
     double acc = 0.0;
-    for (int s = 0; s < S; ++s) acc += fabs(Ur[s * 8 + v]);
+    for (int s = 0; s < S; ++s) acc += fabs(Ur[s * US + v]);
     w[5 + v] = acc / S;
   }
   __syncthreads();
@@ -336,8 +340,8 @@ template <int S, int FN, int CPB, int NPMAX>
 struct CellSmem {
   static constexpr int oPF = 0;                    // CPB*S*18
   static constexpr int oAdj = oPF + CPB * S * PFW; // CPB*S*9
-  static constexpr int oU = oAdj + CPB * S * 9;    // CPB*S*8
-  static constexpr int oDet = oU + CPB * S * 8;    // CPB*S
+  static constexpr int oU = oAdj + CPB * S * 9;    // CPB*S*US
+  static constexpr int oDet = oU + CPB * S * US;    // CPB*S
   static constexpr int oRi = oDet + CPB * S;       // CPB*S*5
   static constexpr int oRv = oRi + CPB * S * 5;    // CPB*S*5
   static constexpr int oQf = oRv + CPB * S * 5;    // CPB*FN*5
@@ -374,7 +378,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   // ---- load ----
   for (int t = tid; t < nc * S * PFW; t += blockDim.x) sPF[t] = a.PF[(size_t)e0 * S * PFW + t];
   for (int t = tid; t < nc * S * 9; t += blockDim.x) sAdj[t] = g.adj[(size_t)e0 * S * 9 + t];
-  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * 8 + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * US + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
   for (int t = tid; t < nc * S; t += blockDim.x) sDet[t] = g.det[(size_t)e0 * S + t];
   // the jumps of this CTA's slots are contiguous (slots are stored cell-major)
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
@@ -495,7 +499,8 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   }
 
   // ---- RK stage combination + positivity (per point) ----
-  double* Up = sQf;  // (CPB*S, 8) reuses the fine-point scratch
+  double* Up = sQf;  // (CPB*S, US) reuses the fine-point scratch (and the flux scratch after it)
+  static_assert(CPB * S * US <= CPB * FN * 20, "RK tile must fit the fine-point and flux scratch");
   double* part = sGt;  // (CPB*S) squared dU/dt per point (stage 0)
   for (int p = tid; p < nc * S; p += blockDim.x) {
     double Lr[8], un[8];
@@ -505,7 +510,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     const size_t gp = (size_t)e0 * S + p;
     const double dts = a.dt[gp];
     const double* u0 = a.U0 + gp * nv;
-    const double* uc = sU + p * 8;
+    const double* uc = sU + p * US;
     if (a.stage == 0) {
       for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
     } else if (a.stage == 1) {
@@ -529,7 +534,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     if (pr < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
     if (nv > 5) un[5] = fmax(un[5], 0.0);
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
-    for (int v = 0; v < nv; ++v) Up[p * 8 + v] = un[v];
+    for (int v = 0; v < nv; ++v) Up[p * US + v] = un[v];
     part[p] = sq_sum;
     part[CPB * S + p] = Lr[0] * Lr[0];
   }
@@ -541,11 +546,11 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     const int s = t / (CPB * 5), r = t % (CPB * 5), b = r / 5, v = r % 5;
     if (b >= nc) continue;
     double acc = 0.0;
-    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * 8 + v];
+    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * US + v];
     a.Unext[((size_t)(e0 + b) * S + s) * nv + v] = acc;
   }
   for (int p = tid; p < nc * S; p += blockDim.x)
-    for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = Up[p * 8 + v];
+    for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = Up[p * US + v];
   if (a.stage == 0 && tid < nc) {
     double acc = 0.0;  // fixed order per cell: points ascending
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];

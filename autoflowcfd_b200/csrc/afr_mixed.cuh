@@ -839,8 +839,9 @@ struct MxUpdSmem {
   static constexpr int THREADS = 256;
   static constexpr int oRi = 0;                        // CPB*S*5 doubles
   static constexpr int oRv = oRi + CPB * S * 5;
-  static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*8
-  static constexpr int oW = oU + CPB * S * 8;          // outliers: CPB*40
+  static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*US
+  static constexpr int oU0 = oU + CPB * S * US;        // CPB*S*US step-start state
+  static constexpr int oW = oU0 + CPB * S * US;        // outliers: CPB*40
   static constexpr int oP = oW + CPB * 40;             // 2*CPB*S: squared dU/dt, squared density column
   static constexpr int oG = oP + 2 * CPB * S;        // g_left, g_right (2*4)
   static constexpr int nD = (oG + 8 + 1) / 2 * 2;     // doubles (even: the jumps start 16-byte aligned)
@@ -859,6 +860,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
   double* sRv = smu + L::oRv;
   double* sU = smu + L::oU;
   double* work = smu + L::oW;
+  double* sU0 = smu + L::oU0;
   double* part = smu + L::oP;
   double* sGw = smu + L::oG;  // [0..3] g_left, [4..7] g_right
   float* sJ = reinterpret_cast<float*>(smu + L::nD);
@@ -887,8 +889,18 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     sRi[t] = double(RV[p * 10 + t % 5]);
     sRv[t] = visc ? double(RV[p * 10 + 5 + t % 5]) : 0.0;
   }
-  for (int p = tid; p < nc * S; p += blockDim.x)
-    for (int v = 0; v < nv; ++v) sU[p * 8 + v] = a.Ucur[((size_t)e0 * S + p) * nv + v];
+  // the tile's current and step-start states are contiguous blocks: coalesced
+  // loads (t -> point t/nv, variable t%nv through an exact float reciprocal)
+  {
+    const float rnv = 1.0f / float(nv);
+    const double* uc = a.Ucur + (size_t)e0 * S * nv;
+    const double* u0 = a.U0 + (size_t)e0 * S * nv;
+    for (int t = tid; t < nc * S * nv; t += blockDim.x) {
+      const int p = __float2int_rz((float(t) + 0.5f) * rnv), v = t - p * nv;
+      sU[p * US + v] = uc[t];
+      if (a.stage >= 0) sU0[p * US + v] = u0[t];
+    }
+  }
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
   const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
   if (staged) {
@@ -936,8 +948,8 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     for (int v = 0; v < nv; ++v) sq_sum += Lr[v] * Lr[v];
     const size_t gp = (size_t)e0 * S + p;
     const double dts = a.dt[gp];
-    const double* u0 = a.U0 + gp * nv;
-    double* uc = sU + p * 8;
+    const double* u0 = sU0 + p * US;
+    double* uc = sU + p * US;
     if (a.stage == 0) {
       for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
     } else if (a.stage == 1) {
@@ -965,17 +977,30 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     part[CPB * S + p] = Lr[0] * Lr[0];
   }
   __syncthreads();
-  // modal filter; lanes of a warp share the filter row s (broadcast loads)
+  // modal filter, each output summed over j in order; one thread per (s, v)
+  // for all cells of the tile (the filter row is loaded once per j); the
+  // outputs are assembled in the residual buffers (no longer needed) and
+  // stored as one contiguous block
+  double* sOut = sRi;  // (nc*S, nv) row-major, fits in sRi + sRv
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < S * CPB * 5; t += blockDim.x) {
-    const int s = t / (CPB * 5), r = t % (CPB * 5), b = r / 5, v = r % 5;
-    if (b >= nc) continue;
-    double acc = 0.0;
-    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * sU[(b * S + j) * 8 + v];
-    a.Unext[((size_t)(e0 + b) * S + s) * nv + v] = acc;
+  for (int t = tid; t < S * 5; t += blockDim.x) {
+    const int s = t / 5, v = t % 5;
+    double acc[CPB];
+#pragma unroll
+    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
+    for (int j = 0; j < S; ++j) {
+      const double f = __ldg(Fm + s * S + j);
+#pragma unroll
+      for (int b = 0; b < CPB; ++b) acc[b] += f * sU[(b * S + j) * US + v];
+    }
+#pragma unroll
+    for (int b = 0; b < CPB; ++b)
+      if (b < nc) sOut[(b * S + s) * nv + v] = acc[b];
   }
   for (int p = tid; p < nc * S; p += blockDim.x)
-    for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = sU[p * 8 + v];
+    for (int v = 5; v < nv; ++v) sOut[p * nv + v] = sU[p * US + v];
+  __syncthreads();
+  for (int t = tid; t < nc * S * nv; t += blockDim.x) a.Unext[(size_t)e0 * S * nv + t] = sOut[t];
   if (a.stage == 0 && tid < nc) {
     double acc = 0.0;
     for (int s = 0; s < S; ++s) acc += part[tid * S + s];

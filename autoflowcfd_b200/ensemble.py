@@ -183,28 +183,44 @@ class B200Ensemble:
         precision: "mixed" (default) or "fp64".
         inviscid_only: Euler instead of laminar Navier-Stokes.
         cases: prebuilt tables per spec (built from the specs when omitted).
+        max_group_cells: cases of one order are split into groups of at most
+            this many cells (one handle each), which bounds the transient device
+            memory of a handle's set-up.
     """
 
     def __init__(self, specs: Sequence[EnsembleCase], precision: str = "mixed", inviscid_only: bool = False,
-                 cases: Optional[Sequence[Dict[str, np.ndarray]]] = None, device="cuda:0"):
+                 cases: Optional[Sequence[Dict[str, np.ndarray]]] = None, device="cuda:0",
+                 max_group_cells: int = 2_000_000):
         from .solver import B200FRSolver
 
         self.specs = list(specs)
         self.device = torch.device(device)
         tables = list(cases) if cases is not None else [build_case(s) for s in self.specs]
         self.groups: List[_Group] = []
+        chunks = []
         for order in sorted({s.order for s in self.specs}):
-            members = [i for i, s in enumerate(self.specs) if s.order == order]
+            cur, cells = [], 0
+            for i in (i for i, s in enumerate(self.specs) if s.order == order):
+                n = int(tables[i]["n_cells"])
+                if cur and cells + n > max_group_cells:
+                    chunks.append((order, cur))
+                    cur, cells = [], 0
+                cur.append(i)
+                cells += n
+            if cur:
+                chunks.append((order, cur))
+        for order, members in chunks:
             part = [tables[i] for i in members]
             cell_ptr = np.concatenate([[0], np.cumsum([int(c["n_cells"]) for c in part])]).astype(np.int64)
             merged = concatenate(part)
-            # the handle's free stream only scales Cd/Cl; per-case Cd uses the case's own velocity
+            # the handle's free stream only scales Cd/Cl
             solver = B200FRSolver(merged, turb_model_name="NONE", mu_molecular=MU, rho_inf=RHO_INF,
                                   vel_inf=self.specs[members[0]].velocity, p_inf=P_INF, inviscid_only=inviscid_only,
                                   precision=precision, device=device)
             U = np.concatenate([uniform_state(self.specs[i], int(tables[i]["n_cells"]), int(tables[i]["n_sps"]))
                                 for i in members])
             solver.set_state_from_cpu(U)
+            del merged, U
             self.groups.append(_Group(order, members, cell_ptr, solver))
         self.graph = None
         self.steps_done = 0

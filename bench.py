@@ -96,6 +96,12 @@ def initial_state(case, spec):
     return U, k, om, nut, mu
 
 
+# DRAM bytes per cell and launch of the mixed stage kernels, measured with ncu
+# on the 76,800-prism P2 SST case (profiles/mixed_stage_kernels_p2_sst_prism_76800.md);
+# a full-size launch moves these times the number of cells.
+MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 9108.0, "k_mx_face": 7073.0, "k_mx_vol": 17130.0, "k_mx_update": 6171.0}
+
+
 def mixed_algorithmic_bytes(case, nv=7):
     """Minimum bytes each per-stage kernel of the mixed form must move (every
     array it reads or writes once, in the layout the form stores).
@@ -253,6 +259,59 @@ def replica_throughput(world, units_per_rank_step, ms_per_step):
     return world * units_per_rank_step / (ms_per_step * 1e-3)
 
 
+def e2e_pipelined(s, starts, steps, stream, barrier):
+    """End to end through the C-ABI: every step copies its inputs (U, k,
+    omega, nu_t) from pinned host memory and its result state back to pinned
+    host memory.  Two device state sets alternate: while step i computes on one,
+    a copy stream writes back step i-1's result and loads step i+1's inputs
+    into the other, so transfers overlap compute.  Each step starts from the
+    same host start state (the C2 state diverges under long runs)."""
+    import torch
+
+    n = max(2, steps // 2)
+    host_in = [t.cpu().pin_memory() for t in starts]
+    host_out = [[torch.empty_like(t).pin_memory() for t in host_in] for _ in range(2)]
+    dev = [[torch.empty_like(t) for t in starts] for _ in range(2)]
+    copy = torch.cuda.Stream(device=starts[0].device)
+    loaded = [torch.cuda.Event() for _ in range(2)]
+    computed = [torch.cuda.Event() for _ in range(2)]
+    saved = [torch.cuda.Event() for _ in range(2)]
+    orig = (s.U, s.k, s.omega, s.nu_t)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    copy.wait_event(e0)
+    with torch.cuda.stream(copy):
+        for d, h in zip(dev[0], host_in):
+            d.copy_(h, non_blocking=True)
+        loaded[0].record(copy)
+    for i in range(n):
+        b = i % 2
+        if i + 1 < n:  # next inputs into the other set once its previous result is saved
+            with torch.cuda.stream(copy):
+                if i >= 1:
+                    copy.wait_event(saved[1 - b])
+                for d, h in zip(dev[1 - b], host_in):
+                    d.copy_(h, non_blocking=True)
+                loaded[1 - b].record(copy)
+        stream.wait_event(loaded[b])
+        s.U, s.k, s.omega, s.nu_t = dev[b]
+        s.step(want_norm=False)
+        computed[b].record(stream)
+        with torch.cuda.stream(copy):
+            copy.wait_event(computed[b])
+            for o, d in zip(host_out[b], dev[b]):
+                o.copy_(d, non_blocking=True)
+            saved[b].record(copy)
+    stream.wait_event(saved[(n - 1) % 2])
+    stream.wait_event(saved[n % 2])
+    e1.record(stream)
+    barrier()
+    s.U, s.k, s.omega, s.nu_t = orig
+    h2d = sum(t.numel() * 8 for t in host_in)
+    return {"e2e_ms": e0.elapsed_time(e1) / n, "h2d": h2d, "d2h": h2d}
+
+
 def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
     """Time one solver's steps (device-resident, restarted from the seeded
     state every SEGMENT steps), one breakdown step, and optionally the e2e
@@ -301,25 +360,7 @@ def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
     restart()
     out["breakdown"] = profiling.step_breakdown(s)
     if want_e2e:
-        # state in pinned host memory, copied in and out every step; the
-        # residual norm is read back every step
-        hst = [t.cpu().pin_memory() for t in starts]
-        outs = [torch.empty_like(t).pin_memory() for t in hst]
-        h2d = sum(t.numel() * 8 for t in hst)
-        barrier()
-        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n = max(1, steps // 2)
-        e2.record(stream)
-        for _ in range(n):
-            for d, h in zip((s.U, s.k, s.omega, s.nu_t), hst):
-                d.copy_(h, non_blocking=True)
-            s.step(want_norm=True)
-            for o, d in zip(outs, (s.U, s.k, s.omega, s.nu_t)):
-                o.copy_(d, non_blocking=True)
-        e3.record(stream)
-        barrier()
-        out["e2e_ms"] = e2.elapsed_time(e3) / n
-        out["h2d"], out["d2h"] = h2d, h2d + 8
+        out.update(e2e_pipelined(s, starts, steps, stream, barrier))
     return out
 
 
@@ -544,7 +585,9 @@ def main():
         "e2e": {"value": replica_throughput(world, dofs_per_step, ms_e2e), "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"], "ms_per_step": ms_e2e},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / hbm_peak) if achieved else None,
+                     "traffic": (MEASURED_TRAFFIC_PER_CELL[dom] * N) if dom in MEASURED_TRAFFIC_PER_CELL else None,
+                     "traffic_source": "ncu DRAM bytes per cell on 76,800 prisms, scaled to this launch",
                      "kernel": dom, "algorithmic_bytes_per_launch": alg[dom], "per_kernel": per_kernel,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "gpu_launches": bd.get("launches_per_step", 0) * args.steps,
