@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
     const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     const int e = e0 + b;
-    const double dj = sDet[b * S + s];
+    const double rdj = 1.0 / sDet[b * S + s];  // each term within an ulp of g' J / det
     double ci = 0.0, cv = 0.0;
     for (int k = fc.slot_ptr[e]; k < fc.slot_ptr[e + 1]; ++k) {
       const int fl = a.slot_flags[k];
@@ -480,8 +480,8 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
       const int fp = ops.dist_fp[ax * S + s];
       const double gw = ((fl & 16) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
       const double* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : J + ((size_t)k * NP + fp) * 10;
-      ci += -(gw * Jk[v]) / dj;
-      if (visc) cv += (gw * Jk[5 + v]) / dj;
+      ci += -(gw * Jk[v]) * rdj;
+      if (visc) cv += (gw * Jk[5 + v]) * rdj;
     }
     sRi[t] = sRi[t] + ci;
     if (visc) sRv[t] = sRv[t] + cv;

@@ -44,7 +44,8 @@ __device__ __forceinline__ double sst_F1(double k, double w, double d, double nu
   double a = fmin(fmax(t1, t2), t3);
   if (!isfinite(a)) a = 1e75;
   a = fmin(a, 1e75);
-  return tanh(pow(a, 4.0));
+  const double a2 = a * a;
+  return tanh(a2 * a2);  // arg1**4 (sst.py:92-141); within an ulp of pow(a, 4)
 }
 
 __device__ __forceinline__ double sst_F2(double k, double w, double d, double nu) {
@@ -343,7 +344,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   for (int t = threadIdx.x; t < nc * S * 4; t += blockDim.x) {
     const int p = t / 4, q = t % 4, s = p % S;
     const int e = e0 + p / S;
-    const double dj = g.det[(size_t)e * S + s];
+    // one reciprocal per point: each term differs from contrib / det by at most an ulp
+    const double rdj = 1.0 / g.det[(size_t)e * S + s];
     double C = 0.0;
     for (int si = fc.tslot_ptr[e]; si < fc.tslot_ptr[e + 1]; ++si) {
       const int code = fc.tslot[si];
@@ -354,8 +356,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
       const double* gp = side > 0.0 ? ops.g_right : ops.g_left;
       const int fp = ops.dist_fp[ax * S + s];
       const double contrib = gp[ops.dist_co[ax * S + s]] * a.cfp[((size_t)f * NP + fp) * 4 + q];
-      if (is_owner) C -= contrib / dj;
-      else C += contrib / dj;
+      if (is_owner) C -= contrib * rdj;
+      else C += contrib * rdj;
     }
     Ref[t] = C;  // staged: R is complete only after the barrier below
   }
