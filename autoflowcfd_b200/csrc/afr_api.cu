@@ -984,14 +984,21 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     std::vector<int32_t> order(F);
     for (size_t f = 0; f < F; ++f) order[f] = (int32_t)f;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return m->colors[a] < m->colors[b]; });
+    // transport slot code: face << 4 | axis << 2 | (neighbor side) << 1 | (side > 0)
+    if (F >= ((size_t)1 << 27)) return bail(fail(h, AFR_EUNSUPPORTED, "more than 2^27 faces"));
+    auto tcode = [&](int32_t f, bool nb) -> int32_t {
+      const int ax = (int)(nb ? m->neighbor_axis[f] : m->owner_axis[f]);
+      const double side = nb ? m->neighbor_side[f] : m->owner_side[f];
+      return (f << 4) | (ax << 2) | (nb ? 2 : 0) | (side > 0.0 ? 1 : 0);
+    };
     auto build = [&](bool transport, int32_t** dptr, int32_t** dslot) -> int {
       std::vector<int32_t> cnt(N + 1, 0);
       auto visit = [&](auto&& emit) {
         for (int32_t f : order) {
           const bool bnd = m->is_boundary[f] != 0;
           if (transport) {
-            emit((int32_t)m->owner_cell[f], f * 2);
-            if (m->neighbor_cell[f] >= 0) emit((int32_t)m->neighbor_cell[f], f * 2 + 1);
+            emit((int32_t)m->owner_cell[f], tcode(f, false));
+            if (m->neighbor_cell[f] >= 0) emit((int32_t)m->neighbor_cell[f], tcode(f, true));
           } else {
             if (m->owner_is_primary[f]) emit((int32_t)m->owner_cell[f], f * 2);
             if (!bnd && m->neighbor_is_primary[f]) emit((int32_t)m->neighbor_cell[f], f * 2 + 1);

@@ -88,7 +88,7 @@ struct Faces {
   const int32_t* slot;        // face*2 + (0 owner, 1 neighbor)
   // transport slots: every face side (owner always, neighbor if interior)
   const int32_t* tslot_ptr;   // (N+1)
-  const int32_t* tslot;
+  const int32_t* tslot;       // face << 4 | axis << 2 | (neighbor side) << 1 | (side > 0)
 };
 
 struct Bc {

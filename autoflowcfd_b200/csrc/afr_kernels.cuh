@@ -502,24 +502,32 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   double* Up = sQf;  // (CPB*S, US) reuses the fine-point scratch (and the flux scratch after it)
   static_assert(CPB * S * US <= CPB * FN * 20, "RK tile must fit the fine-point and flux scratch");
   double* part = sGt;  // (CPB*S) squared dU/dt per point (stage 0)
+  // loops over the 8 possible variables, unrolled, so the arrays stay in registers
   for (int p = tid; p < nc * S; p += blockDim.x) {
     double Lr[8], un[8];
     double sq_sum = 0.0;
-    for (int v = 0; v < nv; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
-    for (int v = 0; v < nv; ++v) sq_sum += Lr[v] * Lr[v];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (v < nv) sq_sum += Lr[v] * Lr[v];
     const size_t gp = (size_t)e0 * S + p;
     const double dts = a.dt[gp];
     const double* u0 = a.U0 + gp * nv;
     const double* uc = sU + p * US;
     if (a.stage == 0) {
-      for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) un[v] = v < nv ? u0[v] + dts * Lr[v] : 0.0;
     } else if (a.stage == 1) {
-      for (int v = 0; v < nv; ++v) un[v] = (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) un[v] = v < nv ? (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v] : 0.0;
     } else {
       // 1/3 U0 + 0 U1 + 2/3 U2 + 2/3 dt L; the 0*U1 term is dropped: it can only
       // turn a finite value into NaN where U1 is non-finite, and U2 (filtered
       // from U1) is then non-finite at the same cell already.
-      for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        un[v] = v < nv ? (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v] : 0.0;
     }
     const double rho = fmax(un[0], 1e-6);
     un[0] = rho;
@@ -534,7 +542,9 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     if (pr < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
     if (nv > 5) un[5] = fmax(un[5], 0.0);
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
-    for (int v = 0; v < nv; ++v) Up[p * US + v] = un[v];
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (v < nv) Up[p * US + v] = un[v];
     part[p] = sq_sum;
     part[CPB * S + p] = Lr[0] * Lr[0];
   }

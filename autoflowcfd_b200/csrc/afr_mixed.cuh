@@ -263,8 +263,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
   const int NB2 = pad16(nfw * C);
   const int ct = cell_type(g, cell_base);
 
-  if (visc) mxd::copy_img(sB1, mo.D3g[ct], L::NB1 * Sq * 4);
-  mxd::copy_img(sA2, mo.E[ct], 128 * Sq * 4);
+  if (visc) mxd::copy_img(sB1, (ct ? mo.D3g[1] : mo.D3g[0]), L::NB1 * Sq * 4);
+  mxd::copy_img(sA2, (ct ? mo.E[1] : mo.E[0]), 128 * Sq * 4);
   // operand padding (K columns s >= S, rows never written) stays zero
   for (int t = tid; t < 128 * Sq * 4 / 16; t += MX_THREADS) reinterpret_cast<uint4*>(sA1)[t] = make_uint4(0, 0, 0, 0);
   for (int t = tid; t < L::NB2MAX * Sq * 4 / 16; t += MX_THREADS)
@@ -591,9 +591,9 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
   const bool visc = L::VP && !inviscid_only;
   const int ct = cell_type(g, cell_base);
 
-  mxd::copy_img(sBc, mo.c2f[ct], Fq * Sq * 4);
-  mxd::copy_img(sBW, mo.W[ct], Sq * 3 * Fq * 4);
-  if (visc) mxd::copy_img(sBD, mo.D3[ct], Sq * 3 * Sq * 4);
+  mxd::copy_img(sBc, (ct ? mo.c2f[1] : mo.c2f[0]), Fq * Sq * 4);
+  mxd::copy_img(sBW, (ct ? mo.W[1] : mo.W[0]), Sq * 3 * Fq * 4);
+  if (visc) mxd::copy_img(sBD, (ct ? mo.D3[1] : mo.D3[0]), Sq * 3 * Sq * 4);
   if (warp == 0) tc::tmem_alloc(&tbase, L::NCOL);
   if (tid == 0) {
     tc::mbar_init(&bar, 1);
@@ -940,22 +940,30 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
       }
     return;
   }
-  // RK stage combination + positivity, in place over the state tile
+  // RK stage combination + positivity, in place over the state tile (loops
+  // over the 8 possible variables, unrolled, so the arrays stay in registers)
   for (int p = tid; p < nc * S; p += blockDim.x) {
     double Lr[8], un[8];
     double sq_sum = 0.0;
-    for (int v = 0; v < nv; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
-    for (int v = 0; v < nv; ++v) sq_sum += Lr[v] * Lr[v];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) Lr[v] = v < 5 ? sRi[p * 5 + v] + (visc ? sRv[p * 5 + v] : 0.0) : 0.0;
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (v < nv) sq_sum += Lr[v] * Lr[v];
     const size_t gp = (size_t)e0 * S + p;
     const double dts = a.dt[gp];
     const double* u0 = sU0 + p * US;
     double* uc = sU + p * US;
     if (a.stage == 0) {
-      for (int v = 0; v < nv; ++v) un[v] = u0[v] + dts * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) un[v] = v < nv ? u0[v] + dts * Lr[v] : 0.0;
     } else if (a.stage == 1) {
-      for (int v = 0; v < nv; ++v) un[v] = (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) un[v] = v < nv ? (0.75 * u0[v] + 0.25 * uc[v]) + (0.25 * dts) * Lr[v] : 0.0;
     } else {
-      for (int v = 0; v < nv; ++v) un[v] = (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v];
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        un[v] = v < nv ? (1.0 / 3.0 * u0[v] + 2.0 / 3.0 * uc[v]) + (2.0 / 3.0 * dts) * Lr[v] : 0.0;
     }
     // positivity (core/time_integration/positivity.py:13-45), one reciprocal of rho
     const double rho = fmax(un[0], 1e-6);
@@ -972,7 +980,9 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     if (pr < 1.0) un[4] = 1.0 / (GAMMA - 1.0) + ke;
     if (nv > 5) un[5] = fmax(un[5], 0.0);
     if (nv > 6) un[6] = fmax(un[6], 1e-8);
-    for (int v = 0; v < nv; ++v) uc[v] = un[v];
+#pragma unroll
+    for (int v = 0; v < 8; ++v)
+      if (v < nv) uc[v] = un[v];
     part[p] = sq_sum;
     part[CPB * S + p] = Lr[0] * Lr[0];
   }

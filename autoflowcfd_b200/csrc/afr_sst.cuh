@@ -341,25 +341,45 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     for (int b = 0; b < CPB; ++b)
       if (b < nc) R[(b * S + s) * 4 + q] = -div[b] / g.det[(size_t)(e0 + b) * S + s];
   }
-  for (int t = threadIdx.x; t < nc * S * 4; t += blockDim.x) {
-    const int p = t / 4, q = t % 4, s = p % S;
+  // one thread per point, all four fields; the slots are fetched four at a time
+  // (independent loads) and summed in slot order
+  for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
+    const int s = p % S;
     const int e = e0 + p / S;
     // one reciprocal per point: each term differs from contrib / det by at most an ulp
     const double rdj = 1.0 / g.det[(size_t)e * S + s];
-    double C = 0.0;
-    for (int si = fc.tslot_ptr[e]; si < fc.tslot_ptr[e + 1]; ++si) {
-      const int code = fc.tslot[si];
-      const int f = code >> 1;
-      const bool is_owner = (code & 1) == 0;
-      const int ax = is_owner ? fc.o_axis[f] : fc.n_axis[f];
-      const double side = is_owner ? fc.o_side[f] : fc.n_side[f];
-      const double* gp = side > 0.0 ? ops.g_right : ops.g_left;
-      const int fp = ops.dist_fp[ax * S + s];
-      const double contrib = gp[ops.dist_co[ax * S + s]] * a.cfp[((size_t)f * NP + fp) * 4 + q];
-      if (is_owner) C -= contrib * rdj;
-      else C += contrib * rdj;
+    double C[4] = {0.0, 0.0, 0.0, 0.0};
+    const int sb = fc.tslot_ptr[e], se = fc.tslot_ptr[e + 1];
+    for (int s0 = sb; s0 < se; s0 += 4) {
+      int code[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) code[u] = s0 + u < se ? __ldg(fc.tslot + s0 + u) : -1;
+      double gw[4];
+      double2 c01[4], c23[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (code[u] < 0) continue;
+        const int ax = (code[u] >> 2) & 3;
+        gw[u] = ((code[u] & 1) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
+        const double2* cr =
+            reinterpret_cast<const double2*>(a.cfp + ((size_t)(code[u] >> 4) * NP + ops.dist_fp[ax * S + s]) * 4);
+        c01[u] = cr[0];
+        c23[u] = cr[1];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (code[u] < 0) continue;
+        const double cv[4] = {c01[u].x, c01[u].y, c23[u].x, c23[u].y};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double contrib = gw[u] * cv[q];
+          if (code[u] & 2) C[q] += contrib * rdj;
+          else C[q] -= contrib * rdj;
+        }
+      }
     }
-    Ref[t] = C;  // staged: R is complete only after the barrier below
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Ref[p * 4 + q] = C[q];  // staged: R is complete only after the barrier below
   }
   __syncthreads();
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
