@@ -79,6 +79,7 @@ SIGNATURES = {
                                                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     "afr_rms_norm_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
     "afr_autotune": (ctypes.c_int, [ctypes.c_void_p] * 3 + [_P_I32, ctypes.c_void_p]),
+    "afr_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _P_I32]),
     "afr_segment_norms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P_I64, ctypes.c_int32, _P_D,
                                          ctypes.c_void_p]),
     "afr_tc_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -58,6 +58,7 @@ struct afr_handle {
   MxBuf mb{};
   int mx_pre_blocks = 0, mx_cell_blocks = 0;  // resident CTAs of the persistent kernels
   int mx_pre_per_sm = 0, mx_pre_max_per_sm = 0, n_sms = 0;
+  int mx_pre_occ = 0, mx_vol_occ = 0;          // occupancy-API CTAs per SM, before the tensor-memory cap
   // launch shapes chosen by afr_autotune (defaults until then)
   int mx_face_block = 128;  // threads per face-kernel CTA: 64, 128 or 256
   int mx_upd_var = 1;       // update-kernel cells per CTA: 0 = half, 1 = base, 2 = double
@@ -221,6 +222,30 @@ struct StepTimer {
   }
 };
 
+// CTAs of a kernel that fit on one SM by registers (allocated per warp in
+// units of 256), shared memory (static + dynamic + the per-CTA reservation),
+// threads and the CTA limit
+static cudaError_t resident_ctas(const void* fn, int threads, size_t dyn_smem, int dev, int* out) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  int smem_sm = 0, regs_sm = 0, thr_sm = 0, blk_sm = 0, resv = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  if (e != cudaSuccess) return e;
+  const long warps = (threads + 31) / 32;
+  const long regs_cta = warps * (((long)fa.numRegs * 32 + 255) / 256 * 256);
+  const size_t smem_cta = fa.sharedSizeBytes + dyn_smem + (size_t)resv;
+  long n = blk_sm;
+  if (regs_cta > 0) n = std::min(n, (long)regs_sm / regs_cta);
+  n = std::min(n, (long)(smem_sm / smem_cta));
+  n = std::min(n, (long)thr_sm / (warps * 32));
+  *out = (int)n;
+  return cudaSuccess;
+}
+
 template <int S, int FN, int NP, int N1D>
 struct Launch {
   static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 2 : 1);
@@ -287,11 +312,20 @@ struct Launch {
       e = cudaFuncSetAttribute(k_mx_vol<S, FN, MXC>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
 
+    // The runtime's occupancy query answers one CTA per SM for every kernel
+    // that uses tensor memory (it cannot know the allocation size), while the
+    // SM co-schedules more where registers, shared memory and threads allow:
+    // the residency is computed from those here and capped by the columns.
+    int api_p = 0, api_c = 0;
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bp, k_mx_pre<S, NP>, MX_THREADS, mx_pre_smem());
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api_p, k_mx_pre<S, NP>, MX_THREADS, mx_pre_smem());
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, k_mx_vol<S, FN, MXC>, MX_VOL_THREADS, mx_vol_smem());
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api_c, k_mx_vol<S, FN, MXC>, MX_VOL_THREADS, mx_vol_smem());
+    if (e == cudaSuccess) e = resident_ctas((const void*)k_mx_pre<S, NP>, MX_THREADS, mx_pre_smem(), dev, &bp);
+    if (e == cudaSuccess) e = resident_ctas((const void*)k_mx_vol<S, FN, MXC>, MX_VOL_THREADS, mx_vol_smem(), dev, &bc);
     if (e != cudaSuccess) return e;
+    h->mx_pre_occ = api_p;
+    h->mx_vol_occ = api_c;
     bp = std::min(bp, 512 / MxPreSmem<S, NP>::NCOL);
     bc = std::min(bc, 512 / MxVolSmem<S, FN, MXC>::NCOL);
     if (bp < 1 || bc < 1) return cudaErrorInvalidConfiguration;
@@ -1301,6 +1335,16 @@ int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* ch
     choice_out[2] = h->mx_upd_var;
   }
   return check_status(h, st);
+}
+
+int afr_launch_shape(const afr_handle* h, int32_t* out) {
+  if (!h || !out) return AFR_EINVAL;
+  const bool mx = h->prec == AFR_PREC_MIXED;
+  const int32_t v[8] = {mx ? h->mx_pre_per_sm : -1, mx ? h->mx_pre_max_per_sm : -1, mx ? h->mx_pre_occ : -1,
+                        mx && h->n_sms ? h->mx_cell_blocks / h->n_sms : -1, mx ? h->mx_vol_occ : -1,
+                        mx ? h->mx_face_block : -1, mx ? h->mx_upd_var : -1, h->n_sms};
+  for (int i = 0; i < 8; ++i) out[i] = v[i];
+  return AFR_OK;
 }
 
 int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t which, double* out,

@@ -225,6 +225,14 @@ class B200FRSolver:
         check(LIB.afr_device_bytes(self._h, ctypes.byref(v)), self._h)
         return int(v.value)
 
+    def launch_shape(self) -> dict:
+        """Launch shapes of the mixed-form kernels (see afr_launch_shape)."""
+        out = (ctypes.c_int32 * 8)()
+        check(LIB.afr_launch_shape(self._h, out), self._h)
+        keys = ("pre_per_sm", "pre_max_per_sm", "pre_occupancy", "vol_per_sm", "vol_occupancy", "face_block",
+                "update_variant", "n_sms")
+        return dict(zip(keys, (int(x) for x in out)))
+
     def cleanup(self):
         """GPUFRSolver.cleanup (core/gpu/gpu_solver_io.py)."""
         if getattr(self, "_h", None) is not None and self._h.value:

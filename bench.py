@@ -538,6 +538,8 @@ def main():
         r = run_form(s, args.steps, args.warmup, stream, barrier, want_e2e=(i == 0),
                      clk_path=clk_path if (rank == 0 and i == 0) else None)
         r["device_bytes"] = s.device_bytes()
+        if form == "mixed":
+            r["launch_shape"] = s.launch_shape()
         s.cleanup()
         del s
         torch.cuda.empty_cache()
@@ -593,6 +595,7 @@ def main():
         "gpu_launches": bd.get("launches_per_step", 0) * args.steps,
         "breakdown_ms_per_step": bd.get("per_kernel_ms"),
         "device_bytes": head["device_bytes"],
+        "launch_shape": res["mixed"].get("launch_shape") if "mixed" in res else None,
         "state_finite": head["finite"],
     }
     if "fp64" in res and mixed_head:

@@ -214,6 +214,17 @@ int afr_rms_norm_noalloc(const double* x, int64_t n, double* out, void* stream);
  * counterpart in the reference (launch shapes have none there). */
 int afr_autotune(afr_handle* h, const double* U, const double* nu_t, int32_t* choice_out, void* stream);
 
+/* Current launch shapes of a handle (8 ints): pre-pass CTAs per SM, its
+ * maximum (the CTAs that fit by registers, shared memory and threads, capped
+ * by 512 tensor-memory columns per SM), the runtime occupancy query's value
+ * for the pre-pass (one for any kernel that uses tensor memory), volume-kernel
+ * CTAs per SM, the runtime query's value for it, face-kernel block,
+ * update-kernel variant (0 half, 1 base, 2 double cells per CTA) and the
+ * device's SM count.
+ * Plain-form handles report -1 except the SM count.  No counterpart in the
+ * reference. */
+int afr_launch_shape(const afr_handle* h, int32_t* out);
+
 /* Per-segment RMS residual norms of the last afr_step: segment i is cells
  * [cell_ptr[i], cell_ptr[i+1]) (host array of nseg+1).  which = 0: the norm
  * over all variables, sqrt(sum(dU/dt^2) / (cells * n_sps * n_vars)), as
