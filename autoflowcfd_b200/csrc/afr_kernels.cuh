@@ -56,88 +56,113 @@ __device__ __forceinline__ void block_gemm(double* out, int ldo, const double* _
   }
 }
 
-// Median-based outlier zeroing over the S points of one cell, per variable
-// (core/fr_operators/troubled_cell.py:346-408).  R is (S,5) in shared memory,
-// Uref the cell's state rows (stride ldU, first 5 columns).  work >= 10 doubles.
+// Median-based outlier zeroing (core/fr_operators/troubled_cell.py:346-408):
+// per cell and variable, |R| > 1e4 * max(median |R|, 1e-9 mean|U|, 1e-300)
+// is set to zero.  A column has nothing to zero when that threshold is at
+// least max |R|.  Two lower bounds of the median prove that without ranking:
+// the minimum, and p = max|R| * 1e-4 (raised until 1e4 * p >= max|R|) when at
+// least as many elements as lie at or above the median's rank are >= p.
+// Such columns (no NaN) skip the O(S^2) rank pass; the others take it, so the
+// result is the same element for element.
+constexpr int OUT_WORK = 25;  // [0,5) median or bound, [5,10) mean|U|, [10,20) middle pair, [20,25) rank flag
+
+// per column v of one block: mean |U| (rows Ur, stride ldU), the bound and the rank flag
 template <int S>
-__device__ void suppress_outliers(double* R, const double* Uref, int ldU, double* work) {
-  double* med = work;       // [5]
-  double* fmean = work + 5; // [5]
-  // rank every |R[s,v]| among its column (stable), pick the middle one(s)
-  for (int t = threadIdx.x; t < S * 5; t += blockDim.x) {
-    const int s = t / 5, v = t % 5;
+__device__ __forceinline__ void outlier_column(const double* R, const double* Ur, int ldU, int v, double* w) {
+  constexpr int NEED = S - ((S & 1) ? S / 2 : S / 2 - 1);  // elements at or above the (lower) middle rank
+  double acc = 0.0, lo = INFINITY, hi = 0.0;
+  bool nan = false;
+  for (int s = 0; s < S; ++s) {
+    acc += fabs(Ur[s * ldU + v]);
     const double x = fabs(R[s * 5 + v]);
-    int rank = 0;
-    for (int j = 0; j < S; ++j) {
-      const double y = fabs(R[j * 5 + v]);
-      rank += (y < x) || (y == x && j < s);
-    }
-    if (S & 1) {
-      if (rank == S / 2) med[v] = x;
-    } else {
-      // even: average of ranks S/2-1 and S/2, combined below through two slots
-      if (rank == S / 2 - 1) work[10 + v] = x;
-      if (rank == S / 2) work[15 + v] = x;
+    lo = fmin(lo, x);
+    hi = fmax(hi, x);
+    nan = nan || isnan(x);
+  }
+  w[5 + v] = acc / S;
+  const double fl = 1e-9 * w[5 + v];
+  bool skip = !nan && hi <= 1e4 * fmax(fmax(lo, fl), 1e-300);
+  double bound = lo;
+  if (!nan && !skip) {
+    double p = hi * 1e-4;
+    // next double up (p is finite and >= 0 here: its bit pattern plus one)
+    for (int it = 0; it < 4 && 1e4 * p < hi; ++it) p = __longlong_as_double(__double_as_longlong(p) + 1);
+    if (1e4 * p >= hi) {
+      int cnt = 0;
+      for (int s = 0; s < S; ++s) cnt += fabs(R[s * 5 + v]) >= p;
+      if (cnt >= NEED) {
+        skip = true;
+        bound = p;
+      }
     }
   }
+  w[v] = bound;
+  w[20 + v] = skip ? 0.0 : 1.0;
+}
+
+// stable rank of |R[s,v]| in its column; the middle one(s) into w
+template <int S>
+__device__ __forceinline__ void outlier_rank(const double* R, int s, int v, double* w) {
+  const double x = fabs(R[s * 5 + v]);
+  int rank = 0;
+  for (int j = 0; j < S; ++j) {
+    const double y = fabs(R[j * 5 + v]);
+    rank += (y < x) || (y == x && j < s);
+  }
+  if (S & 1) {
+    if (rank == S / 2) w[v] = x;
+  } else {
+    if (rank == S / 2 - 1) w[10 + v] = x;
+    if (rank == S / 2) w[15 + v] = x;
+  }
+}
+
+__device__ __forceinline__ void outlier_zero(double* R, int r, int v, const double* w, bool odd) {
+  const double med = odd ? w[v] : 0.5 * (w[10 + v] + w[15 + v]);
+  const double ref = fmax(fmax(med, 1e-9 * w[5 + v]), 1e-300);
+  if (fabs(R[r]) > 1e4 * ref) R[r] = 0.0;
+}
+
+// One cell: R is (S,5) in shared memory, Uref the cell's state rows (stride
+// ldU, first 5 columns).  work >= OUT_WORK doubles.
+template <int S>
+__device__ void suppress_outliers(double* R, const double* Uref, int ldU, double* work) {
+  if (threadIdx.x < 5) outlier_column<S>(R, Uref, ldU, threadIdx.x, work);
   __syncthreads();
-  if (threadIdx.x < 5) {
-    const int v = threadIdx.x;
-    if (!(S & 1)) med[v] = 0.5 * (work[10 + v] + work[15 + v]);
-    double acc = 0.0;
-    for (int s = 0; s < S; ++s) acc += fabs(Uref[s * ldU + v]);
-    fmean[v] = acc / S;
+  for (int t = threadIdx.x; t < S * 5; t += blockDim.x) {
+    const int s = t / 5, v = t % 5;
+    if (work[20 + v] != 0.0) outlier_rank<S>(R, s, v, work);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < S * 5; t += blockDim.x) {
     const int v = t % 5;
-    const double ref = fmax(fmax(med[v], 1e-9 * fmean[v]), 1e-300);
-    if (fabs(R[t]) > 1e4 * ref) R[t] = 0.0;
+    if (work[20 + v] != 0.0) outlier_zero(R, t, v, work, S & 1);
   }
   __syncthreads();
 }
 
-// The same zeroing for the inviscid and viscous residuals of nc cells at once
-// (one rank pass, one threshold pass): block b < nc is sRi of cell b, block
-// nc + b is sRv of cell b; cell rows of the reference field at sU + b*S*8.
-// work >= 20 doubles per block.
+// The same for the inviscid and viscous residuals of nc cells at once: block
+// b < nc is sRi of cell b, block nc + b is sRv of cell b; cell rows of the
+// reference field at sU + b*S*US.  work >= OUT_WORK doubles per block.
 template <int S>
 __device__ void suppress_outliers_cells(double* sRi, double* sRv, const double* sU, int nc, bool visc, double* work) {
   const int nb = nc * (visc ? 2 : 1);
-  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
-    const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
-    const double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
-    const double x = fabs(R[s * 5 + v]);
-    int rank = 0;
-    for (int j = 0; j < S; ++j) {
-      const double y = fabs(R[j * 5 + v]);
-      rank += (y < x) || (y == x && j < s);
-    }
-    double* w = work + bb * 20;
-    if (S & 1) {
-      if (rank == S / 2) w[v] = x;
-    } else {
-      if (rank == S / 2 - 1) w[10 + v] = x;
-      if (rank == S / 2) w[15 + v] = x;
-    }
-  }
-  __syncthreads();
   for (int t = threadIdx.x; t < nb * 5; t += blockDim.x) {
     const int bb = t / 5, v = t % 5;
-    double* w = work + bb * 20;
-    if (!(S & 1)) w[v] = 0.5 * (w[10 + v] + w[15 + v]);
-    const double* Ur = sU + (bb % nc) * S * US;
-    double acc = 0.0;
-    for (int s = 0; s < S; ++s) acc += fabs(Ur[s * US + v]);
-    w[5 + v] = acc / S;
+    const double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
+    outlier_column<S>(R, sU + (bb % nc) * S * US, US, v, work + bb * OUT_WORK);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    double* w = work + bb * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_rank<S>(bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5, s, v, w);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
     const int bb = t / (S * 5), r = t % (S * 5), v = r % 5;
-    double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
-    const double* w = work + bb * 20;
-    const double ref = fmax(fmax(w[v], 1e-9 * w[5 + v]), 1e-300);
-    if (fabs(R[r]) > 1e4 * ref) R[r] = 0.0;
+    const double* w = work + bb * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_zero(bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5, r, v, w, S & 1);
   }
   __syncthreads();
 }
@@ -349,8 +374,8 @@ struct CellSmem {
   static constexpr int oGt = oFt + CPB * FN * 15;  // CPB*S*15
   static constexpr int oJ = oGt + CPB * S * 15;    // staged jumps of the CTA's slots
   static constexpr int oWp = oJ + CPB * CELL_MAXSLOT * NPMAX * 10;  // 2 halves of the W divergence
-  static constexpr int work = oWp + 2 * CPB * S * 5;  // CPB*2*20 (outliers) + 32
-  static constexpr int total = work + CPB * 40 + 32;
+  static constexpr int work = oWp + 2 * CPB * S * 5;  // CPB*2*OUT_WORK (outliers) + 32
+  static constexpr int total = work + CPB * 2 * OUT_WORK + 32;
 };
 
 template <int S, int FN, int NP, int CPB>

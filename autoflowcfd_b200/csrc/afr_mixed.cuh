@@ -841,8 +841,8 @@ struct MxUpdSmem {
   static constexpr int oRv = oRi + CPB * S * 5;
   static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*US
   static constexpr int oU0 = oU + CPB * S * US;        // CPB*S*US step-start state
-  static constexpr int oW = oU0 + CPB * S * US;        // outliers: CPB*40
-  static constexpr int oP = oW + CPB * 40;             // 2*CPB*S: squared dU/dt, squared density column
+  static constexpr int oW = oU0 + CPB * S * US;        // outliers: CPB*2*OUT_WORK
+  static constexpr int oP = oW + CPB * 2 * OUT_WORK;   // 2*CPB*S: squared dU/dt, squared density column
   static constexpr int oG = oP + 2 * CPB * S;        // g_left, g_right (2*4)
   static constexpr int nD = (oG + 8 + 1) / 2 * 2;     // doubles (even: the jumps start 16-byte aligned)
   static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats

@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   __shared__ double R[CPB * S * 4];       // volume residuals, then with the interface corrections
   __shared__ double T[CPB * S * 5];       // transport k, w (+ padding for the outlier helper)
   __shared__ double Ref[CPB * S * 5];
-  __shared__ double work[24];
+  __shared__ double work[OUT_WORK];
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
