@@ -63,6 +63,7 @@ struct afr_handle {
   int mx_face_block = 128;  // threads per face-kernel CTA: 64, 128 or 256
   int mx_upd_var = 1;       // update-kernel cells per CTA: 0 = half, 1 = base, 2 = double
   std::vector<void*> allocs;
+  size_t mat_elems[4] = {0, 0, 0, 0};  // doubles of each interpolation-matrix allocation (0: shares the first)
   uint64_t bytes = 0;
   std::string err;
 };
@@ -112,12 +113,6 @@ int upload_i32(afr_handle* h, int32_t** dst, const T* src, size_t n, cudaStream_
   if (rc) return rc;
   cudaError_t e = cudaStreamSynchronize(st);  // tmp is reused by the caller
   return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "upload sync");
-}
-
-__global__ void k_expand_mats(const double* table, const int32_t* index, size_t n, size_t per, double* out) {
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n * per) return;
-  out[t] = table[(size_t)index[t / per] * per + t % per];
 }
 
 __global__ void k_form_adj(const double* det, const double* inv, double* adj, size_t npts) {
@@ -781,14 +776,14 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
     bool all_matched = true;
     for (uint8_t v : o) all_matched = all_matched && v != MX_OFP_GENERAL;
     if (all_matched) {
+      // (an indexed mesh's four pointers share one table: freed once)
       const double* mats[4] = {h->fc.nb_m0, h->fc.nb_m1, h->fc.ow_m0, h->fc.ow_m1};
-      const size_t rows[4] = {(size_t)h->F, (size_t)m->n_nb_src1, (size_t)h->F, (size_t)m->n_ow_src1};
       for (int i = 0; i < 4; ++i) {
         auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)mats[i]);
         if (it == h->allocs.end()) continue;
         h->allocs.erase(it);
         cudaFree((void*)mats[i]);
-        h->bytes -= std::max<size_t>(rows[i] * P * S, 1) * sizeof(double);
+        h->bytes -= std::max<size_t>(h->mat_elems[i], 1) * sizeof(double);
       }
       h->fc.nb_m0 = h->fc.nb_m1 = h->fc.ow_m0 = h->fc.ow_m1 = nullptr;
     }
@@ -971,40 +966,43 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload_i32(h, &c0n, m->nb_src0_cell, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &i1n, m->nb_src1_idx, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &c1n, m->nb_src1_cell, (size_t)m->n_nb_src1, st, tmp))) return bail(rc);
+    // interpolation matrices: an indexed mesh keeps its table of distinct
+    // matrices on the device with per-record row indices; a dense mesh keeps
+    // its per-record arrays with identity indices
     const bool indexed = m->src_mat_table != nullptr;
-    double* table = nullptr;
-    auto mats = [&](double** dst, const double* dense, const int32_t* index, size_t n) -> int {
-      if (!indexed) return upload(h, dst, dense, n * P * S, st);
-      for (size_t i = 0; i < n; ++i)
-        if (index[i] < 0 || index[i] >= m->n_src_mats) return fail(h, AFR_EINDEX, "matrix index out of range");
-      int r = dalloc(h, dst, n * P * S);
-      if (r) return r;
-      int32_t* di = nullptr;
-      if (cudaMalloc((void**)&di, std::max<size_t>(n, 1) * sizeof(int32_t)) != cudaSuccess)
-        return fail(h, AFR_ENOMEM, "index staging");
-      cudaMemcpyAsync(di, index, n * sizeof(int32_t), cudaMemcpyHostToDevice, st);
-      const size_t tot = n * P * S;
-      if (tot) k_expand_mats<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(table, di, n, P * S, *dst);
-      cudaError_t e = cudaStreamSynchronize(st);
-      cudaFree(di);
-      return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "matrix expansion");
-    };
+    const size_t n1n = (size_t)m->n_nb_src1, n1o = (size_t)m->n_ow_src1;
+    int32_t *m0ni, *m1ni, *m0oi, *m1oi;
     if (indexed) {
       if (m->n_src_mats <= 0) return bail(fail(h, AFR_EINVAL, "empty matrix table"));
-      if (cudaMalloc((void**)&table, (size_t)m->n_src_mats * P * S * sizeof(double)) != cudaSuccess)
-        return bail(fail(h, AFR_ENOMEM, "matrix table staging"));
-      cudaMemcpyAsync(table, m->src_mat_table, (size_t)m->n_src_mats * P * S * sizeof(double),
-                      cudaMemcpyHostToDevice, st);
+      const int32_t* idx[4] = {m->nb_src0_mat_index, m->nb_src1_mat_index, m->ow_src0_mat_index, m->ow_src1_mat_index};
+      const size_t cnt[4] = {F, n1n, F, n1o};
+      for (int k = 0; k < 4; ++k)
+        for (size_t r = 0; r < cnt[k]; ++r)
+          if (idx[k][r] < 0 || idx[k][r] >= m->n_src_mats) return bail(fail(h, AFR_EINDEX, "matrix index out of range"));
+      if ((rc = upload(h, &m0n, m->src_mat_table, (size_t)m->n_src_mats * P * S, st))) return bail(rc);
+      m1n = m0o = m1o = m0n;
+      if ((rc = upload_i32(h, &m0ni, idx[0], F, st, tmp))) return bail(rc);
+      if ((rc = upload_i32(h, &m1ni, idx[1], n1n, st, tmp))) return bail(rc);
+      if ((rc = upload_i32(h, &m0oi, idx[2], F, st, tmp))) return bail(rc);
+      if ((rc = upload_i32(h, &m1oi, idx[3], n1o, st, tmp))) return bail(rc);
+      h->mat_elems[0] = (size_t)m->n_src_mats * P * S;
+    } else {
+      if ((rc = upload(h, &m0n, m->nb_src0_mat, F * P * S, st))) return bail(rc);
+      if ((rc = upload(h, &m1n, m->nb_src1_mat, n1n * P * S, st))) return bail(rc);
+      if ((rc = upload(h, &m0o, m->ow_src0_mat, F * P * S, st))) return bail(rc);
+      if ((rc = upload(h, &m1o, m->ow_src1_mat, n1o * P * S, st))) return bail(rc);
+      std::vector<int32_t> iota(std::max<size_t>(F, std::max(n1n, n1o)));
+      for (size_t r = 0; r < iota.size(); ++r) iota[r] = (int32_t)r;
+      if ((rc = upload(h, &m0ni, iota.data(), F, st))) return bail(rc);
+      m0oi = m0ni;
+      if ((rc = upload(h, &m1ni, iota.data(), n1n, st))) return bail(rc);
+      if ((rc = upload(h, &m1oi, iota.data(), n1o, st))) return bail(rc);
+      cudaStreamSynchronize(st);  // iota leaves scope
+      h->mat_elems[0] = F * P * S;
+      h->mat_elems[1] = n1n * P * S;
+      h->mat_elems[2] = F * P * S;
+      h->mat_elems[3] = n1o * P * S;
     }
-    int rm = mats(&m0n, m->nb_src0_mat, m->nb_src0_mat_index, F);
-    if (!rm) rm = mats(&m1n, m->nb_src1_mat, m->nb_src1_mat_index, (size_t)m->n_nb_src1);
-    if (!rm) rm = mats(&m0o, m->ow_src0_mat, m->ow_src0_mat_index, F);
-    if (!rm) rm = mats(&m1o, m->ow_src1_mat, m->ow_src1_mat_index, (size_t)m->n_ow_src1);
-    if (table) {
-      cudaStreamSynchronize(st);
-      cudaFree(table);
-    }
-    if (rm) return bail(rm);
     if ((rc = upload_i32(h, &c0o, m->ow_src0_cell, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &i1o, m->ow_src1_idx, F, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &c1o, m->ow_src1_cell, (size_t)m->n_ow_src1, st, tmp))) return bail(rc);
@@ -1012,6 +1010,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     fc.owner = own; fc.neighbor = nbr; fc.o_axis = oax; fc.n_axis = nax; fc.o_side = osd; fc.n_side = nsd;
     fc.is_bnd = isb; fc.tnormal = tn; fc.nb_c0 = c0n; fc.nb_m0 = m0n; fc.nb_i1 = i1n; fc.nb_c1 = c1n; fc.nb_m1 = m1n;
     fc.ow_c0 = c0o; fc.ow_m0 = m0o; fc.ow_i1 = i1o; fc.ow_c1 = c1o; fc.ow_m1 = m1o; fc.bc_group = bcg;
+    fc.nb_m0i = m0ni; fc.nb_m1i = m1ni; fc.ow_m0i = m0oi; fc.ow_m1i = m1oi;
   }
   // slot lists: faces visited in ascending (color, face index)
   {

@@ -72,16 +72,24 @@ struct Faces {
   const double* n_side;       // (F)
   const uint8_t* is_bnd;      // (F)
   const double* tnormal;      // (F, P, 3)
+  // Interpolation matrices (rows, P, S), one row per record through a row
+  // index: a shared table of the distinct matrices when the mesh gives one
+  // (a few dozen on generated meshes), else the dense per-record arrays with
+  // identity indices.  fmat() resolves record r's face point i.
   const int32_t* nb_c0;       // (F) neighbor-side sources (owner side reads)
-  const double* nb_m0;        // (F, P, S)
+  const double* nb_m0;        // matrices of nb_m0i
+  const int32_t* nb_m0i;      // (F)
   const int32_t* nb_i1;       // (F) index into the compact second source, -1 if none
   const int32_t* nb_c1;       // (n1)
-  const double* nb_m1;        // (n1, P, S)
+  const double* nb_m1;
+  const int32_t* nb_m1i;      // (n1)
   const int32_t* ow_c0;       // owner-side sources (neighbor side reads)
   const double* ow_m0;
+  const int32_t* ow_m0i;
   const int32_t* ow_i1;
   const int32_t* ow_c1;
   const double* ow_m1;
+  const int32_t* ow_m1i;
   const int32_t* bc_group;    // (F) row of the BC table
   // residual slots: primary sides, ascending color
   const int32_t* slot_ptr;    // (N+1)
@@ -90,6 +98,11 @@ struct Faces {
   const int32_t* tslot_ptr;   // (N+1)
   const int32_t* tslot;       // face << 4 | axis << 2 | (neighbor side) << 1 | (side > 0)
 };
+
+// row of face point i of record r in an indexed matrix array
+__device__ __forceinline__ const double* fmat(const double* m, const int32_t* mi, size_t r, int i, int NP, int S) {
+  return m + ((size_t)mi[r] * NP + i) * S;
+}
 
 struct Bc {
   int32_t n;

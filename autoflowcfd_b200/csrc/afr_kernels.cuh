@@ -291,8 +291,10 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
     for (int src = 0; src < 2; ++src) {
       const int c = src == 0 ? st.c0[sl] : st.c1[sl];
       if (c < 0) continue;
-      const double* M = src == 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S
-                                 : (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S;
+      const double* M = src == 0 ? (is_owner ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S)
+                                             : fmat(fc.ow_m0, fc.ow_m0i, f, i, NP, S))
+                                 : (is_owner ? fmat(fc.nb_m1, fc.nb_m1i, st.i1[sl], i, NP, S)
+                                             : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], i, NP, S));
       const double* pf = PF + (size_t)c * S * PFW;
 #pragma unroll 3
       for (int s = 0; s < S; ++s) {

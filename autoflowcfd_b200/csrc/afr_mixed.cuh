@@ -475,8 +475,10 @@ __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, 
     for (int src = 0; src < 2; ++src) {
       const int c = src == 0 ? st.c0[sl] : st.c1[sl];
       if (c < 0) continue;
-      const double* M = src == 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S
-                                 : (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S;
+      const double* M = src == 0 ? (is_owner ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S)
+                                             : fmat(fc.ow_m0, fc.ow_m0i, f, i, NP, S))
+                                 : (is_owner ? fmat(fc.nb_m1, fc.nb_m1i, st.i1[sl], i, NP, S)
+                                             : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], i, NP, S));
       const float* pf = mb.PFm + (size_t)c * S * 20;
       for (int s = 0; s < S; ++s) {
         const float w = float(__ldg(M + s));
@@ -1059,8 +1061,11 @@ __global__ void k_mx_match(Geom g, Ops ops, Faces fc, SlotTable st, float4* arow
     ofp[t] = MX_OFP_GENERAL;
     return;
   }
-  const double* M0 = c0 >= 0 ? (is_owner ? fc.nb_m0 : fc.ow_m0) + ((size_t)f * NP + i) * S : nullptr;
-  const double* M1 = c1 >= 0 ? (is_owner ? fc.nb_m1 : fc.ow_m1) + ((size_t)st.i1[sl] * NP + i) * S : nullptr;
+  const double* M0 =
+      c0 >= 0 ? (is_owner ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S) : fmat(fc.ow_m0, fc.ow_m0i, f, i, NP, S)) : nullptr;
+  const double* M1 = c1 >= 0 ? (is_owner ? fmat(fc.nb_m1, fc.nb_m1i, st.i1[sl], i, NP, S)
+                                         : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], i, NP, S))
+                             : nullptr;
   const int oax = is_owner ? fc.n_axis[f] : fc.o_axis[f];
   const int osb = (is_owner ? fc.n_side[f] : fc.o_side[f]) > 0.0 ? 1 : 0;
   const int oct = cell_type(g, expect);

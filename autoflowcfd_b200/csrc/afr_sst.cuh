@@ -222,7 +222,7 @@ __global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
     for (int src = 0; src < 2; ++src) {
       const int c = src == 0 ? c0 : (i1 >= 0 ? fc.nb_c1[i1] : -1);
       if (c < 0) continue;
-      const double* M = src == 0 ? fc.nb_m0 + ((size_t)f * NP + i) * S : fc.nb_m1 + ((size_t)i1 * NP + i) * S;
+      const double* M = src == 0 ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S) : fmat(fc.nb_m1, fc.nb_m1i, i1, i, NP, S);
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
       for (int s = 0; s < S; ++s) {
         const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)c * S + s) * 8 + 4);

@@ -123,8 +123,9 @@ typedef struct afr_mesh_desc {
   const double* true_area_weight;   /* (F,P) or NULL */
   /* optional indexed form of the interpolation matrices: when src_mat_table
    * is non-NULL the four *_mat arrays above are ignored and record f's
-   * matrix is src_mat_table[*_mat_index[f]]; the library expands them to the
-   * same dense per-record device layout */
+   * matrix is src_mat_table[*_mat_index[f]]; the library keeps the table on
+   * the device and reads each record's rows through its index (dense inputs
+   * are read through identity indices) */
   int32_t n_src_mats;
   const double* src_mat_table;      /* (n_src_mats,P,S) */
   const int32_t* nb_src0_mat_index; /* (F) */
