@@ -123,20 +123,25 @@ __device__ __forceinline__ void outlier_zero(double* R, int r, int v, const doub
   if (fabs(R[r]) > 1e4 * ref) R[r] = 0.0;
 }
 
-// One cell: R is (S,5) in shared memory, Uref the cell's state rows (stride
-// ldU, first 5 columns).  work >= OUT_WORK doubles.
+// nb contiguous (S,5) blocks R + b*S*5 in shared memory, reference rows
+// Uref + b*S*ldU (first 5 columns), all blocks in one pass per phase.  work >= OUT_WORK doubles per block.
 template <int S>
-__device__ void suppress_outliers(double* R, const double* Uref, int ldU, double* work) {
-  if (threadIdx.x < 5) outlier_column<S>(R, Uref, ldU, threadIdx.x, work);
-  __syncthreads();
-  for (int t = threadIdx.x; t < S * 5; t += blockDim.x) {
-    const int s = t / 5, v = t % 5;
-    if (work[20 + v] != 0.0) outlier_rank<S>(R, s, v, work);
+__device__ void suppress_outliers_blocks(double* R, const double* Uref, int ldU, int nb, double* work) {
+  for (int t = threadIdx.x; t < nb * 5; t += blockDim.x) {
+    const int b = t / 5, v = t % 5;
+    outlier_column<S>(R + b * S * 5, Uref + b * S * ldU, ldU, v, work + b * OUT_WORK);
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < S * 5; t += blockDim.x) {
-    const int v = t % 5;
-    if (work[20 + v] != 0.0) outlier_zero(R, t, v, work, S & 1);
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    double* w = work + b * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_rank<S>(R + b * S * 5, s, v, w);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int b = t / (S * 5), r = t % (S * 5), v = r % 5;
+    const double* w = work + b * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_zero(R + b * S * 5, r, v, w, S & 1);
   }
   __syncthreads();
 }

@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   __shared__ double R[CPB * S * 4];       // volume residuals, then with the interface corrections
   __shared__ double T[CPB * S * 5];       // transport k, w (+ padding for the outlier helper)
   __shared__ double Ref[CPB * S * 5];
-  __shared__ double work[OUT_WORK];
+  __shared__ double work[CPB * OUT_WORK];
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     Ref[p * 5 + 2] = 0.0; Ref[p * 5 + 3] = 0.0; Ref[p * 5 + 4] = 0.0;
   }
   __syncthreads();
-  for (int b = 0; b < nc; ++b) suppress_outliers<S>(T + b * S * 5, Ref + b * S * 5, 5, work);
+  suppress_outliers_blocks<S>(T, Ref, 5, nc, work);
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
     const size_t p = (size_t)e0 * S + t;
     const double rho = fmax(a.U[p * a.nv], 1e-10);
