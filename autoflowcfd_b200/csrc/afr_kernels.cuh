@@ -56,6 +56,36 @@ __device__ __forceinline__ void block_gemm(double* out, int ldo, const double* _
   }
 }
 
+// Small FP64 products C (M x N) = A (M x K) * B (K x N) on the FP64 tensor
+// path: mma.sync m8n8k4 .f64, one 8 x 8 output tile per warp at a time,
+// K in steps of 4 (padding rows / columns read as zero).  a(m, k), b(k, n)
+// fetch operands and c(m, n, value) stores results; block-wide work split by
+// warp, no barrier inside.  The sum order over k is the unit's, so results
+// can differ from a sequential FP64 sum in the last bits.
+template <class FA, class FB, class FC>
+__device__ __forceinline__ void dmma_product(int M, int N, int K, FA a, FB b, FC c) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
+  for (int tile = threadIdx.x >> 5; tile < mt * nt; tile += nw) {
+    const int m = (tile / nt) * 8 + g, n0 = (tile % nt) * 8;
+    double c0 = 0.0, c1 = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + t;
+      const double a0 = (m < M && k < K) ? a(m, k) : 0.0;
+      const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(c0), "+d"(c1)
+                   : "d"(a0), "d"(b0));
+    }
+    const int n = n0 + 2 * t;
+    if (m < M) {
+      if (n < N) c(m, n, c0);
+      if (n + 1 < N) c(m, n + 1, c1);
+    }
+  }
+}
+
 // Median-based outlier zeroing (core/fr_operators/troubled_cell.py:346-408):
 // per cell and variable, |R| > 1e4 * max(median |R|, 1e-9 mean|U|, 1e-300)
 // is set to zero.  A column has nothing to zero when that threshold is at

@@ -989,26 +989,16 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     part[CPB * S + p] = Lr[0] * Lr[0];
   }
   __syncthreads();
-  // modal filter, each output summed over j in order; one thread per (s, v)
-  // for all cells of the tile (the filter row is loaded once per j); the
+  // modal filter as one FP64 tensor-core product per tile: rows s, columns
+  // (cell, variable) of the first five variables, K = the cell's points; the
   // outputs are assembled in the residual buffers (no longer needed) and
   // stored as one contiguous block
   double* sOut = sRi;  // (nc*S, nv) row-major, fits in sRi + sRv
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < S * 5; t += blockDim.x) {
-    const int s = t / 5, v = t % 5;
-    double acc[CPB];
-#pragma unroll
-    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-    for (int j = 0; j < S; ++j) {
-      const double f = __ldg(Fm + s * S + j);
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] += f * sU[(b * S + j) * US + v];
-    }
-#pragma unroll
-    for (int b = 0; b < CPB; ++b)
-      if (b < nc) sOut[(b * S + s) * nv + v] = acc[b];
-  }
+  dmma_product(
+      S, 5 * nc, S, [&](int s, int j) { return __ldg(Fm + s * S + j); },
+      [&](int j, int col) { return sU[((col / 5) * S + j) * US + col % 5]; },
+      [&](int s, int col, double x) { sOut[((col / 5) * S + s) * nv + col % 5] = x; });
   for (int p = tid; p < nc * S; p += blockDim.x)
     for (int v = 5; v < nv; ++v) sOut[p * nv + v] = sU[p * US + v];
   __syncthreads();

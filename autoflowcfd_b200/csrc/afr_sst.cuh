@@ -86,21 +86,14 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     f[t * 5 + 4] = a.w[p];
   }
   __syncthreads();
-  // reference-space gradients, rows s*3+m of D3g, summed in ascending j
-  for (int t = threadIdx.x; t < S * 3 * 5; t += blockDim.x) {
-    const int r = t / 5, q = t % 5;
-    const double* Dr = ops.D3g[ct] + (size_t)r * S;
-    double acc[CPB];
-#pragma unroll
-    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-    for (int j = 0; j < S; ++j) {
-      const double w = __ldg(Dr + j);
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] += w * f[(b * S + j) * 5 + q];
-    }
-#pragma unroll
-    for (int b = 0; b < CPB; ++b)
-      if (b < nc) gc[(b * S * 3 + r) * 5 + q] = acc[b];
+  // reference-space gradients (rows s*3+m of D3g) as one FP64 tensor-core
+  // product: columns (cell, field)
+  {
+    const double* D = ct ? ops.D3g[1] : ops.D3g[0];
+    dmma_product(
+        3 * S, 5 * nc, S, [&](int r, int j) { return __ldg(D + r * S + j); },
+        [&](int j, int col) { return f[((col / 5) * S + j) * 5 + col % 5]; },
+        [&](int r, int col, double x) { gc[((col / 5) * S * 3 + r) * 5 + col % 5] = x; });
   }
   __syncthreads();
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
@@ -272,21 +265,14 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     fl[t * 4 + 3] = v1.y;
   }
   __syncthreads();
-  // grad k, grad w in reference space (D3g rows s*3+m, ascending j)
-  for (int t = threadIdx.x; t < S * 3 * 2; t += blockDim.x) {
-    const int r = t / 2, q = t % 2;
-    const double* Dr = ops.D3g[ct] + (size_t)r * S;
-    double acc[CPB];
-#pragma unroll
-    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-    for (int j = 0; j < S; ++j) {
-      const double w = __ldg(Dr + j);
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] += w * fl[(b * S + j) * 4 + q];
-    }
-#pragma unroll
-    for (int b = 0; b < CPB; ++b)
-      if (b < nc) gc[(b * S * 3 + r) * 2 + q] = acc[b];
+  // grad k, grad w in reference space (D3g rows s*3+m) as one FP64
+  // tensor-core product: columns (cell, field)
+  {
+    const double* D = ct ? ops.D3g[1] : ops.D3g[0];
+    dmma_product(
+        3 * S, 2 * nc, S, [&](int r, int j) { return __ldg(D + r * S + j); },
+        [&](int j, int col) { return fl[((col >> 1) * S + j) * 4 + (col & 1)]; },
+        [&](int r, int col, double x) { gc[((col >> 1) * S * 3 + r) * 2 + (col & 1)] = x; });
   }
   __syncthreads();
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
@@ -317,29 +303,18 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     }
   }
   __syncthreads();
-  // divergence: sum over m of (sum_j Ft[j,m] D[s,j,m]); then the face
-  // corrections of every face side in ascending color order
-  for (int t = threadIdx.x; t < S * 4; t += blockDim.x) {
-    const int s = t / 4, q = t % 4;
-    const double* Dr = ops.D3[ct] + (size_t)s * S * 3;
-    double div[CPB];
-#pragma unroll
-    for (int b = 0; b < CPB; ++b) div[b] = 0.0;
-    for (int m = 0; m < 3; ++m) {
-      double acc[CPB];
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-      for (int j = 0; j < S; ++j) {
-        const double d = __ldg(Dr + j * 3 + m);
-#pragma unroll
-        for (int b = 0; b < CPB; ++b) acc[b] += Ft[((b * S + j) * 3 + m) * 4 + q] * d;
-      }
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) div[b] += acc[b];
-    }
-#pragma unroll
-    for (int b = 0; b < CPB; ++b)
-      if (b < nc) R[(b * S + s) * 4 + q] = -div[b] / g.det[(size_t)(e0 + b) * S + s];
+  // divergence sum_{j,m} D[s,j,m] Ft[j,m] as one FP64 tensor-core product
+  // (K = (j, m), columns (cell, field)); then the face corrections of every
+  // face side in ascending color order
+  {
+    const double* D = ct ? ops.D3[1] : ops.D3[0];
+    dmma_product(
+        S, 4 * nc, 3 * S, [&](int s, int k) { return __ldg(D + s * S * 3 + k); },
+        [&](int k, int col) { return Ft[((col >> 2) * S * 3 + k) * 4 + (col & 3)]; },
+        [&](int s, int col, double x) {
+          const int b = col >> 2;
+          R[(b * S + s) * 4 + (col & 3)] = -x / g.det[(size_t)(e0 + b) * S + s];
+        });
   }
   // one thread per point, all four fields; the slots are fetched four at a time
   // (independent loads) and summed in slot order
