@@ -726,6 +726,9 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if ((rc = dalloc(h, &md, N * S * 3)) || (rc = dalloc(h, &hc, N))) return rc;
   h->mo.MD = md;
   h->mo.hcell = hc;
+  float4* adjf32;
+  if ((rc = dalloc(h, &adjf32, N * (size_t)h->Fn * 3))) return rc;
+  h->mo.adjf = adjf32;
   const int FW = h->order <= 2 ? 18 : 5;
   float *xf, *pfm, *jm;
   const size_t ns = h->slots.n;
@@ -756,6 +759,8 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
               if (ns) k_mx_match<64, 16><<<(unsigned)((ns * 16 + 127) / 128), 128, 0, st>>>(h->g, h->ops, h->fc, h->slots, arow, ofp, 1e-6);
               break;
     }
+    const size_t nrows = N * (size_t)h->Fn * 3;
+    k_mx_adjf<<<(unsigned)((nrows + 255) / 256), 256, 0, st>>>(h->g.adj_fine, nrows, adjf32);
     cudaError_t r = cudaGetLastError();
     return r != cudaSuccess ? r : LL::mx_grids(h);
   });
@@ -766,6 +771,16 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
   cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
   h->prec = AFR_PREC_MIXED;
+  // the FP64 fine-point adjugates were needed only for MD and the FP32 copy
+  {
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)h->g.adj_fine);
+    if (it != h->allocs.end()) {
+      h->allocs.erase(it);
+      cudaFree((void*)h->g.adj_fine);
+      h->bytes -= N * (size_t)h->Fn * 9 * sizeof(double);
+      h->g.adj_fine = nullptr;
+    }
+  }
   // The dense per-record interpolation matrices are read afterwards only by
   // the general (unmatched) face points and by the SST face kernel: release
   // them when neither exists.

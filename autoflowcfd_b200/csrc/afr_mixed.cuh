@@ -57,6 +57,7 @@ struct MxOps {
   const uint16_t* D3g[2];  // B: rows m*Sq + s, K = Sq (j)
   const uint16_t* E[2];    // A: rows fp = (ax*2+side)*NP + i (128 rows), K = Sq
   const double* MD;        // (N, S, 3) metric divergence of the folded W
+  const float4* adjf;      // (N, FN, 3) FP32 fine-point adjugate rows (4th entry zero)
   const double* hcell;     // (N) interior-penalty length, cube root of the mean det
 };
 
@@ -622,7 +623,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
       const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
       const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
       mxd::prefetch_l2(Ucur, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
-      mxd::prefetch_l2(g.adj_fine, (size_t)g.N * FN * 72, en * FN * 72, nn * FN * 72);
+      mxd::prefetch_l2(mo.adjf, (size_t)g.N * FN * 48, en * FN * 48, nn * FN * 48);
       mxd::prefetch_l2(g.det, NS * 8, en * S * 8, nn * S * 8);
       mxd::prefetch_l2(mo.MD, NS * 24, en * S * 24, nn * S * 24);
       if (visc) {
@@ -740,7 +741,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
 #pragma unroll
         for (int v = 0; v < 5; ++v) Ft[m][v] = 0.f;
       if (c < nc && i < FN) {
-        const double* ad = g.adj_fine + ((size_t)(e0 + c) * FN + i) * 9;
+        const float4* ad = mo.adjf + ((size_t)(e0 + c) * FN + i) * 3;
         float qb[5], dq[5], dF[3][5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -750,9 +751,9 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         mxd::euler_flux_delta(qb, dq, dF);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          const float x0 = float(__ldg(ad + m * 3)), x1 = float(__ldg(ad + m * 3 + 1)), x2 = float(__ldg(ad + m * 3 + 2));
+          const float4 x = __ldg(ad + m);
 #pragma unroll
-          for (int v = 0; v < 5; ++v) Ft[m][v] = x0 * dF[0][v] + x1 * dF[1][v] + x2 * dF[2][v];
+          for (int v = 0; v < 5; ++v) Ft[m][v] = x.x * dF[0][v] + x.y * dF[1][v] + x.z * dF[2][v];
         }
       }
 #pragma unroll
@@ -1075,6 +1076,15 @@ __global__ void k_mx_match(Geom g, Ops ops, Faces fc, SlotTable st, float4* arow
   }
   ofp[t] = (best >= 0 && best_err <= tol * fmax(mmax, 1e-300)) ? (uint8_t)((oax * 2 + osb) * NP + best)
                                                                  : MX_OFP_GENERAL;
+}
+
+// FP32 copies of the fine-point adjugate rows (the volume kernel rounds them to
+// FP32 before use; one row of 3 per float4)
+__global__ void k_mx_adjf(const double* __restrict__ adj_fine, size_t nrows, float4* __restrict__ out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const double* a = adj_fine + t * 3;
+  out[t] = make_float4(float(a[0]), float(a[1]), float(a[2]), 0.f);
 }
 
 // MD[c,s,n] = sum_{i,m} W[s, i*3+m] adj_fine[c,i,m,n]  (W's columns follow D_fine: i*3+m)
