@@ -333,7 +333,7 @@ struct Launch {
   template <int CPB>
   static void mx_update_launch(afr_handle* h, const StageArgs& a, int n, cudaStream_t st) {
     k_mx_update<S, NP, CPB><<<(n + CPB - 1) / CPB, MxUpdSmem<S, NP, CPB>::THREADS, MxUpdSmem<S, NP, CPB>::total, st>>>(
-        h->g, h->ops, h->fc, a, h->mb.RV, h->mb.Jm);
+        h->g, h->ops, h->fc, a, h->mb.RV, h->mb.Jm, h->mo.rdet);
   }
   static int n_ranges(const afr_handle* h) { return (h->n_prism > 0 ? 1 : 0) + (h->N > h->n_prism ? 1 : 0); }
   static cudaError_t mx_pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
@@ -726,9 +726,16 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if ((rc = dalloc(h, &md, N * S * 3)) || (rc = dalloc(h, &hc, N))) return rc;
   h->mo.MD = md;
   h->mo.hcell = hc;
-  float4* adjf32;
-  if ((rc = dalloc(h, &adjf32, N * (size_t)h->Fn * 3))) return rc;
+  float4 *adjf32, *adjs32, *invs32;
+  if ((rc = dalloc(h, &adjf32, N * (size_t)h->Fn * 3)) || (rc = dalloc(h, &adjs32, N * (size_t)S * 3)) ||
+      (rc = dalloc(h, &invs32, N * (size_t)S * 3)))
+    return rc;
   h->mo.adjf = adjf32;
+  h->mo.adjs = adjs32;
+  h->mo.invs = invs32;
+  double* rdet;
+  if ((rc = dalloc(h, &rdet, N * (size_t)S))) return rc;
+  h->mo.rdet = rdet;
   const int FW = h->order <= 2 ? 18 : 5;
   float *xf, *pfm, *jm;
   const size_t ns = h->slots.n;
@@ -759,8 +766,11 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
               if (ns) k_mx_match<64, 16><<<(unsigned)((ns * 16 + 127) / 128), 128, 0, st>>>(h->g, h->ops, h->fc, h->slots, arow, ofp, 1e-6);
               break;
     }
-    const size_t nrows = N * (size_t)h->Fn * 3;
-    k_mx_adjf<<<(unsigned)((nrows + 255) / 256), 256, 0, st>>>(h->g.adj_fine, nrows, adjf32);
+    const size_t nrows = N * (size_t)h->Fn * 3, nsrows = N * (size_t)S * 3;
+    k_mx_rows_f32<<<(unsigned)((nrows + 255) / 256), 256, 0, st>>>(h->g.adj_fine, nrows, adjf32);
+    k_mx_rows_f32<<<(unsigned)((nsrows + 255) / 256), 256, 0, st>>>(h->g.adj, nsrows, adjs32);
+    k_mx_rows_f32<<<(unsigned)((nsrows + 255) / 256), 256, 0, st>>>(h->g.inv, nsrows, invs32);
+    k_mx_rdet<<<(unsigned)((N * (size_t)S + 255) / 256), 256, 0, st>>>(h->g.det, N * (size_t)S, rdet);
     cudaError_t r = cudaGetLastError();
     return r != cudaSuccess ? r : LL::mx_grids(h);
   });

@@ -58,6 +58,9 @@ struct MxOps {
   const uint16_t* E[2];    // A: rows fp = (ax*2+side)*NP + i (128 rows), K = Sq
   const double* MD;        // (N, S, 3) metric divergence of the folded W
   const float4* adjf;      // (N, FN, 3) FP32 fine-point adjugate rows (4th entry zero)
+  const float4* adjs;      // (N, S, 3) FP32 solution-point adjugate rows
+  const float4* invs;      // (N, S, 3) FP32 inverse-Jacobian rows
+  const double* rdet;      // (N, S) 1 / det, FP64
   const double* hcell;     // (N) interior-penalty length, cube root of the mean det
 };
 
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
       const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
       mxd::prefetch_l2(U, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
-      if (visc) mxd::prefetch_l2(g.inv, NS * 72, en * S * 72, nn * S * 72);
+      if (visc) mxd::prefetch_l2(mo.invs, NS * 48, en * S * 48, nn * S * 48);
       if (nut) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
     }
     // primitives and temperature in FP64
@@ -365,10 +368,15 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         const int c = t % C, s = t / C;
         float gr[12];
         if (c < nc) {
-          const double* inv = g.inv + ((size_t)(e0 + c) * S + s) * 9;
+          const float4* inv = mo.invs + ((size_t)(e0 + c) * S + s) * 3;
           float iv[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) iv[k] = float(__ldg(inv + k));
+          for (int m = 0; m < 3; ++m) {
+            const float4 x = __ldg(inv + m);
+            iv[m * 3 + 0] = x.x;
+            iv[m * 3 + 1] = x.y;
+            iv[m * 3 + 2] = x.z;
+          }
           const float* gs = sG + (c * S + s) * 12;
 #pragma unroll
           for (int f = 0; f < 4; ++f)
@@ -628,7 +636,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
       mxd::prefetch_l2(mo.MD, NS * 24, en * S * 24, nn * S * 24);
       if (visc) {
         mxd::prefetch_l2(PFm, NS * 80, en * S * 80, nn * S * 80);
-        mxd::prefetch_l2(g.adj, NS * 72, en * S * 72, nn * S * 72);
+        mxd::prefetch_l2(mo.adjs, NS * 48, en * S * 48, nn * S * 48);
       }
     }
     // ---- primitives (FP64), det and metric divergence of the tile ----
@@ -639,7 +647,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         const size_t p = (size_t)e0 * S + t;
         mxd::prim_T(Ucur + p * nv, q);
         if (L::VP) {
-          sDet[t] = 1.0 / g.det[p];  // reciprocal: the readouts multiply
+          sDet[t] = __ldg(mo.rdet + p);  // reciprocal: the readouts multiply
           sMD[t * 3 + 0] = mo.MD[p * 3 + 0];
           sMD[t * 3 + 1] = mo.MD[p * 3 + 1];
           sMD[t * 3 + 2] = mo.MD[p * 3 + 2];
@@ -683,7 +691,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
           const size_t p = (size_t)(e0 + c) * S + s;
           const float4* pf = reinterpret_cast<const float4*>(PFm + p * 20);
           const float4 g0 = __ldg(pf), g1 = __ldg(pf + 1), g2 = __ldg(pf + 2), g3 = __ldg(pf + 3);
-          const double* am = g.adj + p * 9;
+          const float4* am = mo.adjs + p * 3;
           float q[5];
 #pragma unroll
           for (int v = 0; v < 5; ++v) q[v] = float(sQ[(c * S + s) * 5 + v]);
@@ -693,9 +701,9 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
           viscous_flux<float>(q, gv, gT, mu, g3.x, G);
 #pragma unroll
           for (int m = 0; m < 3; ++m) {
-            const float x0 = float(__ldg(am + m * 3)), x1 = float(__ldg(am + m * 3 + 1)), x2 = float(__ldg(am + m * 3 + 2));
+            const float4 x = __ldg(am + m);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) Gt[m][v] = x0 * G[0][v] + x1 * G[1][v] + x2 * G[2][v];
+            for (int v = 0; v < 5; ++v) Gt[m][v] = x.x * G[0][v] + x.y * G[1][v] + x.z * G[2][v];
           }
         }
 #pragma unroll
@@ -807,7 +815,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
             if (s < S && c < nc) {
               const size_t p = (size_t)(e0 + c) * S + s;
               const double* md = L::VP ? sMD + (c * S + s) * 3 : mo.MD + p * 3;
-              const double rdj = L::VP ? sDet[c * S + s] : 1.0 / g.det[p];
+              const double rdj = L::VP ? sDet[c * S + s] : __ldg(mo.rdet + p);
               const double mdf = md[0] * sFb[c * 15 + v] + md[1] * sFb[c * 15 + 5 + v] + md[2] * sFb[c * 15 + 10 + v];
               sR[(c * S + s) * 10 + v] = float(-(double(v8[j] + w8[j]) + mdf) * rdj);
             }
@@ -856,7 +864,8 @@ struct MxUpdSmem {
 
 template <int S, int NP, int CPB>
 __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
-    k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm) {
+    k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm,
+                const double* __restrict__ rdet) {
   using L = MxUpdSmem<S, NP, CPB>;
   extern __shared__ double smu[];
   double* sRi = smu + L::oRi;
@@ -915,7 +924,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
     const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     const int e = e0 + b;
-    const double rdj = 1.0 / g.det[(size_t)e * S + s];  // one division per point (no bitwise target here)
+    const double rdj = __ldg(rdet + (size_t)e * S + s);  // reciprocal formed at create
     double ci = 0.0, cv = 0.0;
     for (int k = sPtr[b]; k < sPtr[b + 1]; ++k) {
       const int fl = staged ? sFl[k - k_beg] : a.slot_flags[k];
@@ -1078,9 +1087,15 @@ __global__ void k_mx_match(Geom g, Ops ops, Faces fc, SlotTable st, float4* arow
                                                                  : MX_OFP_GENERAL;
 }
 
-// FP32 copies of the fine-point adjugate rows (the volume kernel rounds them to
-// FP32 before use; one row of 3 per float4)
-__global__ void k_mx_adjf(const double* __restrict__ adj_fine, size_t nrows, float4* __restrict__ out) {
+// 1 / det per solution point
+__global__ void k_mx_rdet(const double* __restrict__ det, size_t n, double* __restrict__ out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = 1.0 / det[t];
+}
+
+// FP32 copies of 3 x 3 metric rows (adjugates, inverse Jacobians: the mixed
+// kernels round them to FP32 before use); one row of 3 per float4
+__global__ void k_mx_rows_f32(const double* __restrict__ adj_fine, size_t nrows, float4* __restrict__ out) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nrows) return;
   const double* a = adj_fine + t * 3;
