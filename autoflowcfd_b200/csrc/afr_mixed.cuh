@@ -134,6 +134,15 @@ __device__ __forceinline__ void cell_pair(int idx, int npts, int& c, int& p0) {
   c = (rest / (npts / 2)) * 8 + (idx & 7);
 }
 
+// asynchronous 8-byte copy global -> shared (both 8-byte aligned); completed
+// by cp_async_wait_all before the block barrier that publishes the data
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // 16-byte copy global -> shared of an operator image
 __device__ __forceinline__ void copy_img(void* dst, const void* src, int bytes) {
   const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -843,7 +852,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
 // color order (staged in shared memory), outlier zeroing, then the SSP-RK3
 // combination, positivity and filter in FP64 (or the residual-only outputs).
 // ---------------------------------------------------------------------------
-constexpr int MX_UPD_MAXSLOT = 8;  // slots per cell staged in shared memory (more: read from global)
+constexpr int MX_UPD_MAXSLOT = 6;  // slots per cell staged in shared memory (more: read from global)
 
 template <int S, int NP, int CPB>
 struct MxUpdSmem {
@@ -855,11 +864,14 @@ struct MxUpdSmem {
   static constexpr int oW = oU0 + CPB * S * US;        // outliers: CPB*2*OUT_WORK
   static constexpr int oP = oW + CPB * 2 * OUT_WORK;   // 2*CPB*S: squared dU/dt, squared density column
   static constexpr int oG = oP + 2 * CPB * S;        // g_left, g_right (2*4)
-  static constexpr int nD = (oG + 8 + 1) / 2 * 2;     // doubles (even: the jumps start 16-byte aligned)
-  static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats
+  static constexpr int oRd = oG + 8;                  // CPB*S reciprocal det
+  static constexpr int oDt = oRd + CPB * S;           // CPB*S local dt
+  static constexpr int nD = (oDt + CPB * S + 1) / 2 * 2;  // doubles (even: the jumps start 16-byte aligned)
+  static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats: staged jumps
+  static constexpr int nR = CPB * S * 10;                    // floats: the tile's volume terms
   // ints: slot flags of the staged slots, per-cell slot pointers, distribution maps
   static constexpr int nI = CPB * MX_UPD_MAXSLOT + CPB + 1 + 6 * S;
-  static constexpr int total = nD * 8 + nJ * 4 + nI * 4;
+  static constexpr int total = nD * 8 + nJ * 4 + nR * 4 + nI * 4;
 };
 
 template <int S, int NP, int CPB>
@@ -875,8 +887,11 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
   double* sU0 = smu + L::oU0;
   double* part = smu + L::oP;
   double* sGw = smu + L::oG;  // [0..3] g_left, [4..7] g_right
+  double* sRd = smu + L::oRd;
+  double* sDt = smu + L::oDt;
   float* sJ = reinterpret_cast<float*>(smu + L::nD);
-  int* sFl = reinterpret_cast<int*>(sJ + L::nJ);
+  float* sRVf = sJ + L::nJ;
+  int* sFl = reinterpret_cast<int*>(sRVf + L::nR);
   int* sPtr = sFl + CPB * MX_UPD_MAXSLOT;
   int* sDfp = sPtr + CPB + 1;
   int* sDco = sDfp + 3 * S;
@@ -896,35 +911,38 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     sGw[4 + tid] = ops.g_right[tid];
   }
   if (tid <= nc) sPtr[tid] = fc.slot_ptr[e0 + tid];
-  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
-    const size_t p = (size_t)e0 * S + t / 5;
-    sRi[t] = double(RV[p * 10 + t % 5]);
-    sRv[t] = visc ? double(RV[p * 10 + 5 + t % 5]) : 0.0;
-  }
-  // the tile's current and step-start states are contiguous blocks: coalesced
-  // loads (t -> point t/nv, variable t%nv through an exact float reciprocal)
+  const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
+  const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
+  // The tile's inputs are contiguous blocks: asynchronous 8-byte copies, all
+  // in flight at once (state rows t -> point t/nv, variable t%nv through an
+  // exact float reciprocal; volume terms and jumps as float pairs)
   {
     const float rnv = 1.0f / float(nv);
     const double* uc = a.Ucur + (size_t)e0 * S * nv;
     const double* u0 = a.U0 + (size_t)e0 * S * nv;
     for (int t = tid; t < nc * S * nv; t += blockDim.x) {
       const int p = __float2int_rz((float(t) + 0.5f) * rnv), v = t - p * nv;
-      sU[p * US + v] = uc[t];
-      if (a.stage >= 0) sU0[p * US + v] = u0[t];
+      mxd::cp_async8(sU + p * US + v, uc + t);
+      if (a.stage >= 0) mxd::cp_async8(sU0 + p * US + v, u0 + t);
     }
-  }
-  const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
-  const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
-  if (staged) {
-    mxd::copy_f32(sJ, Jm + (size_t)k_beg * NP * 10, (k_end - k_beg) * NP * 10);
-    for (int t = tid; t < k_end - k_beg; t += blockDim.x) sFl[t] = a.slot_flags[k_beg + t];
+    const float* rv = RV + (size_t)e0 * S * 10;
+    for (int t = tid; t < nc * S * 5; t += blockDim.x) mxd::cp_async8(sRVf + 2 * t, rv + 2 * t);
+    for (int t = tid; t < nc * S; t += blockDim.x) {
+      mxd::cp_async8(sRd + t, rdet + (size_t)e0 * S + t);
+      if (a.stage >= 0) mxd::cp_async8(sDt + t, a.dt + (size_t)e0 * S + t);
+    }
+    if (staged) {
+      const float* jb = Jm + (size_t)k_beg * NP * 10;
+      for (int t = tid; t < (k_end - k_beg) * NP * 5; t += blockDim.x) mxd::cp_async8(sJ + 2 * t, jb + 2 * t);
+      for (int t = tid; t < k_end - k_beg; t += blockDim.x) sFl[t] = a.slot_flags[k_beg + t];
+    }
+    mxd::cp_async_wait_all();
   }
   __syncthreads();
   // lift the jumps of each cell's slots, ascending color order
   for (int t = tid; t < nc * S * 5; t += blockDim.x) {
     const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
-    const int e = e0 + b;
-    const double rdj = __ldg(rdet + (size_t)e * S + s);  // reciprocal formed at create
+    const double rdj = sRd[b * S + s];  // reciprocal formed at create
     double ci = 0.0, cv = 0.0;
     for (int k = sPtr[b]; k < sPtr[b + 1]; ++k) {
       const int fl = staged ? sFl[k - k_beg] : a.slot_flags[k];
@@ -937,8 +955,9 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
     }
     ci *= rdj;
     cv *= rdj;
-    sRi[t] = sRi[t] + ci;
-    if (visc) sRv[t] = sRv[t] + cv;
+    const float* rp = sRVf + (b * S + s) * 10;
+    sRi[t] = double(rp[v]) + ci;
+    sRv[t] = visc ? double(rp[5 + v]) + cv : 0.0;
   }
   __syncthreads();
   suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
@@ -962,8 +981,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
 #pragma unroll
     for (int v = 0; v < 8; ++v)
       if (v < nv) sq_sum += Lr[v] * Lr[v];
-    const size_t gp = (size_t)e0 * S + p;
-    const double dts = a.dt[gp];
+    const double dts = sDt[p];
     const double* u0 = sU0 + p * US;
     double* uc = sU + p * US;
     if (a.stage == 0) {
