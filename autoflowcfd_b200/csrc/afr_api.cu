@@ -781,16 +781,18 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
   cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
   h->prec = AFR_PREC_MIXED;
-  // the FP64 fine-point adjugates were needed only for MD and the FP32 copy
-  {
-    auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)h->g.adj_fine);
-    if (it != h->allocs.end()) {
-      h->allocs.erase(it);
-      cudaFree((void*)h->g.adj_fine);
-      h->bytes -= N * (size_t)h->Fn * 9 * sizeof(double);
-      h->g.adj_fine = nullptr;
-    }
-  }
+  // The FP64 fine-point adjugates were needed only for MD and the FP32 copy;
+  // the FP64 solution-point adjugates only for the set-up and the SST kernels.
+  auto release = [&](const double*& p, size_t n) {
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)p);
+    if (it == h->allocs.end()) return;
+    h->allocs.erase(it);
+    cudaFree((void*)p);
+    h->bytes -= n * sizeof(double);
+    p = nullptr;
+  };
+  release(h->g.adj_fine, N * (size_t)h->Fn * 9);
+  if (h->prm.turb != AFR_TURB_SST) release(h->g.adj, N * (size_t)S * 9);
   // The dense per-record interpolation matrices are read afterwards only by
   // the general (unmatched) face points and by the SST face kernel: release
   // them when neither exists.
@@ -1136,7 +1138,9 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     cudaStreamSynchronize(st);
   }
   // ---- scratch ----
-  if ((rc = dalloc(h, &h->PF, N * S * PFW))) return bail(rc);
+  // FP64 point fields: every evaluation of the plain form; the mixed form needs
+  // them only for the force integral, which allocates them for its call
+  if (prm->precision != AFR_PREC_MIXED && (rc = dalloc(h, &h->PF, N * S * PFW))) return bail(rc);
   if ((rc = dalloc(h, &h->Ua, N * S * h->nv))) return bail(rc);
   if ((rc = dalloc(h, &h->Ub, N * S * h->nv))) return bail(rc);
   if ((rc = dalloc(h, &h->dt, N * S))) return bail(rc);
@@ -1426,10 +1430,23 @@ int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double referen
   if (!h || !U || !out3) return AFR_EINVAL;
   if (!h->cd_faces) return fail(h, AFR_EINVAL, "handle was created without wall-face force tables");
   cudaStream_t st = (cudaStream_t)stream;
+  // mixed handles keep no FP64 point fields between calls: a temporary set here
+  double* pf_tmp = nullptr;
+  if (!h->PF) {
+    if (cudaMalloc((void**)&pf_tmp, (size_t)h->N * h->S * PFW * sizeof(double)) != cudaSuccess)
+      return fail(h, AFR_ENOMEM, "force: point fields");
+    h->PF = pf_tmp;
+  }
   cudaError_t e = dispatch(h, [&](auto L) {
     cudaError_t r = L.pre(h, U, nu_t, true, st);
     return r != cudaSuccess ? r : L.force(h, U, nu_t, st);
   });
+  if (pf_tmp) {
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    cudaFree(pf_tmp);
+    h->PF = nullptr;
+  }
   if (e != cudaSuccess) return cuda_fail(h, e, "force");
   std::vector<double> part((size_t)h->n_cd_faces * 6);
   e = cudaMemcpyAsync(part.data(), h->cd_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st);

@@ -106,23 +106,25 @@ def mixed_algorithmic_bytes(case, nv=7):
     """Minimum bytes each per-stage kernel of the mixed form must move (every
     array it reads or writes once, in the layout the form stores).
 
-    k_mx_pre: state, inverse Jacobians, nu_t in; FP32 point fields (20 per
-    point) and face-point fields (18 per face point, 6*P per cell) out.
+    k_mx_pre: state, FP32 inverse-Jacobian rows (3 x 16 B), nu_t in; FP32
+    point fields (20 per point) and face-point fields (18 per face point, 6*P
+    per cell) out.
     k_mx_face: both sides' face-point fields, the slot's adjugate row (16 B),
     other-side index (1 B), true normal (24 B) per slot flux point, jumps out.
-    k_mx_vol: state, FP32 point fields, adjugates at solution and fine points,
-    det, metric divergence in; FP32 volume terms (10 per point) out.
-    k_mx_update: volume terms, jumps, current and step-start state, dt, det in;
-    next state out."""
+    k_mx_vol: state, FP32 point fields, FP32 adjugate rows at solution and fine
+    points (3 x 16 B each), reciprocal det, metric divergence in; FP32 volume
+    terms (10 per point) out.
+    k_mx_update: volume terms, jumps, current and step-start state, dt,
+    reciprocal det in; next state out."""
     N, S, Fn = int(case["n_cells"]), int(case["n_sps"]), int(case["n_fine"])
     P = case["true_normal"].shape[1]
     isb = case["is_boundary"].astype(bool)
     slots = int(np.sum(case["owner_is_primary"].astype(bool))) + \
         int(np.sum(~isb & case["neighbor_is_primary"].astype(bool)))
     sp = slots * P
-    pre = N * S * 8 * (nv + 9 + 1) + N * S * 20 * 4 + N * 18 * 6 * P * 4
+    pre = N * S * (8 * (nv + 1) + 48) + N * S * 20 * 4 + N * 18 * 6 * P * 4
     face = sp * (2 * 18 * 4 + 16 + 1 + 24 + 10 * 4) + slots * 24
-    vol = N * S * 8 * (nv + 9 + 1 + 3) + N * S * 20 * 4 + N * Fn * 9 * 8 + N * S * 10 * 4
+    vol = N * S * (8 * (nv + 1 + 3) + 48) + N * S * 20 * 4 + N * Fn * 48 + N * S * 10 * 4
     upd = N * S * 10 * 4 + sp * 10 * 4 + N * S * 8 * (3 * nv + 2) + slots * 4
     return {"k_mx_pre": pre, "k_mx_face": face, "k_mx_vol": vol, "k_mx_update": upd}
 
@@ -262,54 +264,59 @@ def replica_throughput(world, units_per_rank_step, ms_per_step):
 def e2e_pipelined(s, starts, steps, stream, barrier):
     """End to end through the C-ABI: every step copies its inputs (U, k,
     omega, nu_t) from pinned host memory and its result state back to pinned
-    host memory.  Two device state sets alternate: while step i computes on one,
-    a copy stream writes back step i-1's result and loads step i+1's inputs
-    into the other, so transfers overlap compute.  Each step starts from the
-    same host start state (the C2 state diverges under long runs)."""
+    host memory.  Three device state sets rotate: while step i computes on one,
+    one copy stream writes back step i-1's result from the second and another
+    loads step i+1's inputs into the third, so both transfer directions run at
+    once and overlap compute.  Each step starts from the same host start state
+    (the C2 state diverges under long runs)."""
     import torch
 
-    n = max(2, steps // 2)
+    K = 3
+    n = max(K, steps)
     host_in = [t.cpu().pin_memory() for t in starts]
-    host_out = [[torch.empty_like(t).pin_memory() for t in host_in] for _ in range(2)]
-    dev = [[torch.empty_like(t) for t in starts] for _ in range(2)]
-    copy = torch.cuda.Stream(device=starts[0].device)
-    loaded = [torch.cuda.Event() for _ in range(2)]
-    computed = [torch.cuda.Event() for _ in range(2)]
-    saved = [torch.cuda.Event() for _ in range(2)]
+    host_out = [[torch.empty_like(t).pin_memory() for t in host_in] for _ in range(K)]
+    dev = [[torch.empty_like(t) for t in starts] for _ in range(K)]
+    h2d = torch.cuda.Stream(device=starts[0].device)
+    d2h = torch.cuda.Stream(device=starts[0].device)
+    loaded = [torch.cuda.Event() for _ in range(K)]
+    computed = [torch.cuda.Event() for _ in range(K)]
+    saved = [torch.cuda.Event() for _ in range(K)]
     orig = (s.U, s.k, s.omega, s.nu_t)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    copy.wait_event(e0)
-    with torch.cuda.stream(copy):
+    h2d.wait_event(e0)
+    d2h.wait_event(e0)
+    with torch.cuda.stream(h2d):
         for d, h in zip(dev[0], host_in):
             d.copy_(h, non_blocking=True)
-        loaded[0].record(copy)
+        loaded[0].record(h2d)
     for i in range(n):
-        b = i % 2
-        if i + 1 < n:  # next inputs into the other set once its previous result is saved
-            with torch.cuda.stream(copy):
-                if i >= 1:
-                    copy.wait_event(saved[1 - b])
-                for d, h in zip(dev[1 - b], host_in):
+        b = i % K
+        if i + 1 < n:  # next inputs into the next set once its previous result is saved
+            nb = (i + 1) % K
+            with torch.cuda.stream(h2d):
+                if i + 1 >= K:
+                    h2d.wait_event(saved[nb])
+                for d, h in zip(dev[nb], host_in):
                     d.copy_(h, non_blocking=True)
-                loaded[1 - b].record(copy)
+                loaded[nb].record(h2d)
         stream.wait_event(loaded[b])
         s.U, s.k, s.omega, s.nu_t = dev[b]
         s.step(want_norm=False)
         computed[b].record(stream)
-        with torch.cuda.stream(copy):
-            copy.wait_event(computed[b])
+        with torch.cuda.stream(d2h):
+            d2h.wait_event(computed[b])
             for o, d in zip(host_out[b], dev[b]):
                 o.copy_(d, non_blocking=True)
-            saved[b].record(copy)
-    stream.wait_event(saved[(n - 1) % 2])
-    stream.wait_event(saved[n % 2])
+            saved[b].record(d2h)
+    for b in range(K):
+        stream.wait_event(saved[b])
     e1.record(stream)
     barrier()
     s.U, s.k, s.omega, s.nu_t = orig
-    h2d = sum(t.numel() * 8 for t in host_in)
-    return {"e2e_ms": e0.elapsed_time(e1) / n, "h2d": h2d, "d2h": h2d}
+    h2d_bytes = sum(t.numel() * 8 for t in host_in)
+    return {"e2e_ms": e0.elapsed_time(e1) / n, "h2d": h2d_bytes, "d2h": h2d_bytes}
 
 
 def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):

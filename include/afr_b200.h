@@ -179,7 +179,10 @@ int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, d
 int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* ms_out, int n_ms,
                      int* launches, void* stream);
 
-/* Wall force coefficients (Cd, Cl, Cs) of state U into out3 (host). */
+/* Wall force coefficients (Cd, Cl, Cs) of state U into out3 (host), in
+ * FP64.  Mixed-precision handles keep no FP64 point fields between calls:
+ * this call allocates them (N x S x 18 doubles) for its duration and
+ * synchronises the stream. */
 int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3,
               void* stream);
 
