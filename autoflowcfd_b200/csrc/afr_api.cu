@@ -274,7 +274,7 @@ struct Launch {
     return cudaGetLastError();
   }
   // ---- mixed-precision form ----
-  static constexpr int MXC = S <= 27 ? 24 : 16;            // cells per volume-kernel tile
+  static constexpr int MXC = 16;                            // cells per volume-kernel tile
   static constexpr int MXU = S <= 8 ? 16 : (S <= 27 ? 4 : 2);  // cells per update-kernel CTA
   static size_t mx_pre_smem() { return MxPreSmem<S, NP>::total; }
   static size_t mx_vol_smem() { return MxVolSmem<S, FN, MXC>::total; }

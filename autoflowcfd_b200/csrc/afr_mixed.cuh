@@ -875,7 +875,7 @@ struct MxUpdSmem {
 };
 
 template <int S, int NP, int CPB>
-__global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS)
+__global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
     k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm,
                 const double* __restrict__ rdet) {
   using L = MxUpdSmem<S, NP, CPB>;
