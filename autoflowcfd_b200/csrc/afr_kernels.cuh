@@ -56,6 +56,16 @@ __device__ __forceinline__ void block_gemm(double* out, int ldo, const double* _
   }
 }
 
+// asynchronous 8-byte copy global -> shared (both 8-byte aligned); completed
+// by cp_async_wait_all before the block barrier that publishes the data
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Small FP64 products C (M x N) = A (M x K) * B (K x N) on the FP64 tensor
 // path: mma.sync m8n8k4 .f64, one 8 x 8 output tile per warp at a time,
 // K in steps of 4 (padding rows / columns read as zero).  a(m, k), b(k, n)

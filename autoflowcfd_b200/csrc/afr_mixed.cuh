@@ -134,14 +134,8 @@ __device__ __forceinline__ void cell_pair(int idx, int npts, int& c, int& p0) {
   c = (rest / (npts / 2)) * 8 + (idx & 7);
 }
 
-// asynchronous 8-byte copy global -> shared (both 8-byte aligned); completed
-// by cp_async_wait_all before the block barrier that publishes the data
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
+using afr::cp_async8;
+using afr::cp_async_wait_all;
 
 // 16-byte copy global -> shared of an operator image
 __device__ __forceinline__ void copy_img(void* dst, const void* src, int bytes) {

@@ -62,7 +62,7 @@ __device__ __forceinline__ double sst_F2(double k, double w, double d, double nu
 // SST cells per CTA (the three per-cell SST kernels)
 template <int S>
 struct SstTile {
-  static constexpr int CPB = S <= 8 ? 16 : (S <= 27 ? 4 : 2);
+  static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 4 : 2);
   static constexpr int THREADS = 128;
 };
 
@@ -71,19 +71,30 @@ struct SstTile {
 template <int S>
 __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, int cell_base, int cell_end) {
   constexpr int CPB = SstTile<S>::CPB;
-  __shared__ double f[CPB * S * 5];
+  __shared__ double f[CPB * S * 5];     // rho u, rho v, rho w, k, omega; then the pt outputs
   __shared__ double gc[CPB * S * 3 * 5];
+  __shared__ double sInv[CPB * S * 9];  // inverse Jacobians; then the sp8 outputs (row stride 9)
+  __shared__ double sU[CPB * S * 8];    // state rows (stride nv <= 8)
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
-  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
-    const size_t p = (size_t)e0 * S + t;
-    const double* u = a.U + p * a.nv;
-    f[t * 5 + 0] = u[1];
-    f[t * 5 + 1] = u[2];
-    f[t * 5 + 2] = u[3];
-    f[t * 5 + 3] = a.k[p];
-    f[t * 5 + 4] = a.w[p];
+  const int nv = a.nv;
+  // the tile's blocks are contiguous: asynchronous 8-byte copies, all in flight at once
+  {
+    const float rnv = 1.0f / float(nv);
+    const double* ub = a.U + (size_t)e0 * S * nv;
+    for (int t = threadIdx.x; t < nc * S * nv; t += blockDim.x) {
+      cp_async8(sU + t, ub + t);
+      const int p = __float2int_rz((float(t) + 0.5f) * rnv), v = t - p * nv;
+      if (v >= 1 && v <= 3) cp_async8(f + p * 5 + v - 1, ub + t);
+    }
+    const double* ib = g.inv + (size_t)e0 * S * 9;
+    for (int t = threadIdx.x; t < nc * S * 9; t += blockDim.x) cp_async8(sInv + t, ib + t);
+    for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+      cp_async8(f + t * 5 + 3, a.k + (size_t)e0 * S + t);
+      cp_async8(f + t * 5 + 4, a.w + (size_t)e0 * S + t);
+    }
+    cp_async_wait_all();
   }
   __syncthreads();
   // reference-space gradients (rows s*3+m of D3g) as one FP64 tensor-core
@@ -99,7 +110,9 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
     const int s = t % S;
     const size_t p = (size_t)e0 * S + t;
-    const double* inv = g.inv + p * 9;
+    double inv[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) inv[k] = sInv[t * 9 + k];
     const double* gcs = gc + (size_t)(t - s) * 3 * 5;  // this cell's rows
     double gp[5][3];
     for (int q = 0; q < 5; ++q)
@@ -117,9 +130,9 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
         for (int n = 0; n < 3; ++n) gp[q][n] *= sc;
       }
     }
-    const double* u = a.U + p * a.nv;
+    const double* u = sU + t * nv;
     const double rho = fmax(u[0], 1e-10);
-    const double kf = a.k[p], wf = a.w[p];
+    const double kf = f[t * 5 + 3], wf = f[t * 5 + 4];
     const double d = g.wall_dist[p];
     // strain magnitude of the conserved-momentum gradient
     double ss = 0.0;
@@ -160,22 +173,31 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     const double sw = F1t * SST_SW1 + (1.0 - F1t) * SST_SW2;
     const double rnut = rho * nut;
     a.nut[p] = nut;
-    double* o = a.pt + p * 5;
+    // outputs staged in this point's own rows (read above by this thread only),
+    // then stored as contiguous blocks
+    const double gk = a.mu + sk * rnut, gw = a.mu + sw * rnut;
+    const double r1 = u[1] / rho, r2 = u[2] / rho, r3 = u[3] / rho;
+    double* o = f + t * 5;
     o[0] = Sk;
     o[1] = Sw;
     o[2] = beta;
-    o[3] = a.mu + sk * rnut;
-    o[4] = a.mu + sw * rnut;
-    double* o8 = a.sp8 + p * 8;
+    o[3] = gk;
+    o[4] = gw;
+    double* o8 = sInv + t * 9;
     o8[0] = rho;
-    o8[1] = u[1] / rho;
-    o8[2] = u[2] / rho;
-    o8[3] = u[3] / rho;
+    o8[1] = r1;
+    o8[2] = r2;
+    o8[3] = r3;
     o8[4] = kf;
     o8[5] = wf;
-    o8[6] = o[3];
-    o8[7] = o[4];
+    o8[6] = gk;
+    o8[7] = gw;
   }
+  __syncthreads();
+  double* pt = a.pt + (size_t)e0 * S * 5;
+  for (int t = threadIdx.x; t < nc * S * 5; t += blockDim.x) pt[t] = f[t];
+  double* p8 = a.sp8 + (size_t)e0 * S * 8;
+  for (int t = threadIdx.x; t < nc * S * 8; t += blockDim.x) p8[t] = sInv[(t >> 3) * 9 + (t & 7)];
 }
 
 // per face flux point: upwind convection and BR1-style diffusion corrections
@@ -246,42 +268,54 @@ template <int S, int NP>
 __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a, int cell_base,
                                                     int cell_end) {
   constexpr int CPB = SstTile<S>::CPB;
-  __shared__ double fl[CPB * S * 4];      // k, w, gamma_k, gamma_w
+  // point values packed by k_sst_point, row stride 9: rho (clamped as the
+  // reference's), u, v, w, k, omega, gamma_k, gamma_w
+  __shared__ double sP[CPB * S * 9];
   __shared__ double gc[CPB * S * 3 * 2];  // reference-space grads of k, w
   __shared__ double Ft[CPB * S * 3 * 4];  // contravariant fluxes: conv k, diff k, conv w, diff w
-  __shared__ double R[CPB * S * 4];       // volume residuals, then with the interface corrections
-  __shared__ double T[CPB * S * 5];       // transport k, w (+ padding for the outlier helper)
-  __shared__ double Ref[CPB * S * 5];
+  // inverse Jacobians and adjugates (rows of 9) until the fluxes are formed;
+  // then R (volume residuals, then with the interface corrections), T
+  // (transport k, w + padding for the outlier helper) and Ref
+  __shared__ double X[CPB * S * 18];
   __shared__ double work[CPB * OUT_WORK];
+  double* sInv = X;
+  double* sAdj = X + CPB * S * 9;
+  double* R = X;
+  double* T = X + CPB * S * 4;
+  double* Ref = X + CPB * S * 9;
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
-  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
-    const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)e0 * S + t) * 8 + 4);
-    const double2 v0 = x[0], v1 = x[1];
-    fl[t * 4 + 0] = v0.x;
-    fl[t * 4 + 1] = v0.y;
-    fl[t * 4 + 2] = v1.x;
-    fl[t * 4 + 3] = v1.y;
+  // the tile's blocks are contiguous: asynchronous 8-byte copies, all in flight at once
+  {
+    const double* pb = a.sp8 + (size_t)e0 * S * 8;
+    for (int t = threadIdx.x; t < nc * S * 8; t += blockDim.x) cp_async8(sP + (t >> 3) * 9 + (t & 7), pb + t);
+    const double* ib = g.inv + (size_t)e0 * S * 9;
+    const double* ab = g.adj + (size_t)e0 * S * 9;
+    for (int t = threadIdx.x; t < nc * S * 9; t += blockDim.x) {
+      cp_async8(sInv + t, ib + t);
+      cp_async8(sAdj + t, ab + t);
+    }
+    cp_async_wait_all();
   }
   __syncthreads();
+  const double* fl = sP + 4;  // k, w, gamma_k, gamma_w of point p at fl[p * 9 + 0..3]
   // grad k, grad w in reference space (D3g rows s*3+m) as one FP64
   // tensor-core product: columns (cell, field)
   {
     const double* D = ct ? ops.D3g[1] : ops.D3g[0];
     dmma_product(
         3 * S, 2 * nc, S, [&](int r, int j) { return __ldg(D + r * S + j); },
-        [&](int j, int col) { return fl[((col >> 1) * S + j) * 4 + (col & 1)]; },
+        [&](int j, int col) { return fl[((col >> 1) * S + j) * 9 + (col & 1)]; },
         [&](int r, int col, double x) { gc[((col >> 1) * S * 3 + r) * 2 + (col & 1)] = x; });
   }
   __syncthreads();
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
-    const size_t p = (size_t)e0 * S + t;
-    const double* inv = g.inv + p * 9;
-    const double* adj = g.adj + p * 9;
-    const double* u = a.U + p * a.nv;
-    const double rho = fmax(u[0], 1e-10);
-    const double vel[3] = {u[1] / rho, u[2] / rho, u[3] / rho};
+    const double* inv = sInv + t * 9;
+    const double* adj = sAdj + t * 9;
+    const double* pv = sP + t * 9;  // rho = max(U0, 1e-10) and u = U1..3 / rho, as formed by k_sst_point
+    const double rho = pv[0];
+    const double vel[3] = {pv[1], pv[2], pv[3]};
     for (int q = 0; q < 2; ++q) {
       double gphys[3];
       for (int n = 0; n < 3; ++n) {
@@ -289,8 +323,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
         for (int m = 0; m < 3; ++m) acc += gc[(t * 3 + m) * 2 + q] * inv[m * 3 + n];
         gphys[n] = acc;
       }
-      const double phi = fl[t * 4 + q];
-      const double gam = fl[t * 4 + 2 + q];
+      const double phi = fl[t * 9 + q];
+      const double gam = fl[t * 9 + 2 + q];
       double Fc[3], Fd[3];
       for (int d = 0; d < 3; ++d) {
         Fc[d] = (rho * vel[d]) * phi;
@@ -358,7 +392,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   }
   __syncthreads();
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
-    const double rho = fmax(a.U[((size_t)e0 * S + p) * a.nv], 1e-10);
+    const double rho = sP[p * 9];
     const double* Cp = Ref + p * 4;
     const double conv_k = R[p * 4 + 0] + Cp[0];
     const double diff_k = R[p * 4 + 1] - Cp[1];
@@ -370,20 +404,20 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   }
   __syncthreads();
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
-    Ref[p * 5 + 0] = fl[p * 4 + 0];
-    Ref[p * 5 + 1] = fl[p * 4 + 1];
+    Ref[p * 5 + 0] = fl[p * 9 + 0];
+    Ref[p * 5 + 1] = fl[p * 9 + 1];
     Ref[p * 5 + 2] = 0.0; Ref[p * 5 + 3] = 0.0; Ref[p * 5 + 4] = 0.0;
   }
   __syncthreads();
   suppress_outliers_blocks<S>(T, Ref, 5, nc, work);
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
     const size_t p = (size_t)e0 * S + t;
-    const double rho = fmax(a.U[p * a.nv], 1e-10);
+    const double rho = sP[t * 9];
     const double tk = dfinite(T[t * 5 + 0]);
     const double tw = dfinite(T[t * 5 + 1]);
     const double* pt = a.pt + p * 5;
     const double dts = a.dt[p];
-    const double kf = fl[t * 4 + 0], wf = fl[t * 4 + 1];
+    const double kf = fl[t * 9 + 0], wf = fl[t * 9 + 1];
     const double wo = fmax(wf, 1e-10);
     const double dkd = dfinite((pt[0] / fmax(rho, 1e-10)) / (1.0 + dts * (SST_BSTAR * wo)));
     const double dwd = dfinite((pt[1] / fmax(rho, 1e-10)) / (1.0 + dts * (pt[2] * wo)));
