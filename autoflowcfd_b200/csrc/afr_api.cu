@@ -217,6 +217,15 @@ struct StepTimer {
   }
 };
 
+// n matrices (P, S) row-major -> (S, P) each (face point fastest on the device)
+static std::vector<double> transpose_mats(const double* src, size_t n, int P, int S) {
+  std::vector<double> out(n * P * S);
+  for (size_t k = 0; k < n; ++k)
+    for (int i = 0; i < P; ++i)
+      for (int s = 0; s < S; ++s) out[(k * S + s) * P + i] = src[(k * P + i) * S + s];
+  return out;
+}
+
 // CTAs of a kernel that fit on one SM by registers (allocated per warp in
 // units of 256), shared memory (static + dynamic + the per-CTA reservation),
 // threads and the CTA limit
@@ -398,8 +407,8 @@ struct Launch {
       if (n > 0) k_sst_point<S><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, a, ranges[r], ranges[r + 1]);
     }
     if (tm) tm->mark(st);
-    const int nt = h->F * NP;
-    k_sst_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, a);
+    k_sst_face<S, NP><<<(h->F + SST_FACE_WARPS - 1) / SST_FACE_WARPS, 32 * SST_FACE_WARPS, 0, st>>>(h->g, h->ops,
+                                                                                                    h->fc, a);
     if (tm) tm->mark(st);
     for (int r = 0; r < 2; ++r) {
       const int n = ranges[r + 1] - ranges[r];
@@ -955,14 +964,18 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     h->ops.filt[t] = flt;
   }
   {
-    double *ex, *gl, *gr;
+    double *ex, *exT, *gl, *gr;
     int32_t *dfp, *dco;
     if ((rc = upload(h, &ex, m->boundary_extrap, 12 * P * S, st))) return bail(rc);
+    const std::vector<double> exT_h = transpose_mats(m->boundary_extrap, 12, P, S);
+    if ((rc = upload(h, &exT, exT_h.data(), exT_h.size(), st))) return bail(rc);
+    cudaStreamSynchronize(st);  // exT_h leaves scope
     if ((rc = upload(h, &gl, m->g_left, (size_t)n1d, st))) return bail(rc);
     if ((rc = upload(h, &gr, m->g_right, (size_t)n1d, st))) return bail(rc);
     if ((rc = upload_i32(h, &dfp, m->dist_fp_of_sp, 3 * S, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &dco, m->dist_axis_coord_of_sp, 3 * S, st, tmp))) return bail(rc);
     h->ops.extrap = ex;
+    h->ops.extrapT = exT;
     h->ops.g_left = gl;
     h->ops.g_right = gr;
     h->ops.dist_fp = dfp;
@@ -1006,7 +1019,9 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
       for (int k = 0; k < 4; ++k)
         for (size_t r = 0; r < cnt[k]; ++r)
           if (idx[k][r] < 0 || idx[k][r] >= m->n_src_mats) return bail(fail(h, AFR_EINDEX, "matrix index out of range"));
-      if ((rc = upload(h, &m0n, m->src_mat_table, (size_t)m->n_src_mats * P * S, st))) return bail(rc);
+      const std::vector<double> tabT = transpose_mats(m->src_mat_table, (size_t)m->n_src_mats, P, S);
+      if ((rc = upload(h, &m0n, tabT.data(), tabT.size(), st))) return bail(rc);
+      cudaStreamSynchronize(st);
       m1n = m0o = m1o = m0n;
       if ((rc = upload_i32(h, &m0ni, idx[0], F, st, tmp))) return bail(rc);
       if ((rc = upload_i32(h, &m1ni, idx[1], n1n, st, tmp))) return bail(rc);
@@ -1014,10 +1029,14 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
       if ((rc = upload_i32(h, &m1oi, idx[3], n1o, st, tmp))) return bail(rc);
       h->mat_elems[0] = (size_t)m->n_src_mats * P * S;
     } else {
-      if ((rc = upload(h, &m0n, m->nb_src0_mat, F * P * S, st))) return bail(rc);
-      if ((rc = upload(h, &m1n, m->nb_src1_mat, n1n * P * S, st))) return bail(rc);
-      if ((rc = upload(h, &m0o, m->ow_src0_mat, F * P * S, st))) return bail(rc);
-      if ((rc = upload(h, &m1o, m->ow_src1_mat, n1o * P * S, st))) return bail(rc);
+      const double* dense[4] = {m->nb_src0_mat, m->nb_src1_mat, m->ow_src0_mat, m->ow_src1_mat};
+      double** dst[4] = {&m0n, &m1n, &m0o, &m1o};
+      const size_t rows[4] = {F, n1n, F, n1o};
+      for (int k = 0; k < 4; ++k) {
+        const std::vector<double> t = transpose_mats(dense[k], rows[k], P, S);
+        if ((rc = upload(h, dst[k], t.data(), t.size(), st))) return bail(rc);
+        cudaStreamSynchronize(st);  // t leaves scope
+      }
       std::vector<int32_t> iota(std::max<size_t>(F, std::max(n1n, n1o)));
       for (size_t r = 0; r < iota.size(); ++r) iota[r] = (int32_t)r;
       if ((rc = upload(h, &m0ni, iota.data(), F, st))) return bail(rc);

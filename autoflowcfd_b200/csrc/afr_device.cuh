@@ -41,6 +41,7 @@ struct Ops {
   const double* W[2];       // (S, 3Fn) = f2c * D_fine, folded once at create
   const double* filt[2];    // (S, S)
   const double* extrap;     // (2, 3, 2, P, S)
+  const double* extrapT;    // (2, 3, 2, S, P): the same, face point fastest (lanes of a face read one line)
   const double* g_left;     // (n1d)
   const double* g_right;    // (n1d)
   const int32_t* dist_fp;   // (3, S)
@@ -72,10 +73,11 @@ struct Faces {
   const double* n_side;       // (F)
   const uint8_t* is_bnd;      // (F)
   const double* tnormal;      // (F, P, 3)
-  // Interpolation matrices (rows, P, S), one row per record through a row
-  // index: a shared table of the distinct matrices when the mesh gives one
-  // (a few dozen on generated meshes), else the dense per-record arrays with
-  // identity indices.  fmat() resolves record r's face point i.
+  // Interpolation matrices stored transposed, (rows, S, P) with the face
+  // point fastest, one matrix per record through a row index: a shared table
+  // of the distinct matrices when the mesh gives one (a few dozen on
+  // generated meshes), else the dense per-record arrays with identity
+  // indices.  fmat() gives record r's face point i; weight s is at [s * P].
   const int32_t* nb_c0;       // (F) neighbor-side sources (owner side reads)
   const double* nb_m0;        // matrices of nb_m0i
   const int32_t* nb_m0i;      // (F)
@@ -99,9 +101,9 @@ struct Faces {
   const int32_t* tslot;       // face << 4 | axis << 2 | (neighbor side) << 1 | (side > 0)
 };
 
-// row of face point i of record r in an indexed matrix array
+// face point i of record r in an indexed, transposed matrix array: weight s at [s * NP]
 __device__ __forceinline__ const double* fmat(const double* m, const int32_t* mi, size_t r, int i, int NP, int S) {
-  return m + ((size_t)mi[r] * NP + i) * S;
+  return m + (size_t)mi[r] * S * NP + i;
 }
 
 struct Bc {

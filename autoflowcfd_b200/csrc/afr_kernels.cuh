@@ -302,12 +302,12 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
 #pragma unroll
   for (int k = 0; k < 21; ++k) ow[k] = 0.0;
   {
-    const double* Er = ops.extrap + ((((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * NP + i) * S;
+    const double* Er = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * S * NP + i;
     const double* pf = PF + (size_t)e * S * PFW;
     const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
 #pragma unroll 3
     for (int s = 0; s < S; ++s) {
-      const double w = __ldg(Er + s);
+      const double w = __ldg(Er + s * NP);
       double x[18];
       ld18(pf + s * PFW, x);
 #pragma unroll
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
       const double* pf = PF + (size_t)c * S * PFW;
 #pragma unroll 3
       for (int s = 0; s < S; ++s) {
-        const double w = __ldg(M + s);
+        const double w = __ldg(M + s * NP);
         // the reference skips zero weights (inviscid_kernel_colored.py:117-121):
         // a zero weight adds exactly nothing, even next to a non-finite value
         const bool nz = w != 0.0;

@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, 
                                              : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], i, NP, S));
       const float* pf = mb.PFm + (size_t)c * S * 20;
       for (int s = 0; s < S; ++s) {
-        const float w = float(__ldg(M + s));
+        const float w = float(__ldg(M + s * NP));
         if (w == 0.f) continue;
         const float4* p4 = reinterpret_cast<const float4*>(pf + s * 20);
         const float4 x3 = __ldg(p4 + 3), x4 = __ldg(p4 + 4);
@@ -1082,14 +1082,14 @@ __global__ void k_mx_match(Geom g, Ops ops, Faces fc, SlotTable st, float4* arow
   const int osb = (is_owner ? fc.n_side[f] : fc.o_side[f]) > 0.0 ? 1 : 0;
   const int oct = cell_type(g, expect);
   double mmax = 0.0;
-  for (int s = 0; s < S; ++s) mmax = fmax(mmax, fabs((M0 ? M0[s] : 0.0) + (M1 ? M1[s] : 0.0)));
+  for (int s = 0; s < S; ++s) mmax = fmax(mmax, fabs((M0 ? M0[s * NP] : 0.0) + (M1 ? M1[s * NP] : 0.0)));
   int best = -1;
   double best_err = INFINITY;
   for (int j = 0; j < NP; ++j) {
     const double* Eo = ops.extrap + (((size_t)oct * 3 + oax) * 2 + osb) * NP * S + (size_t)j * S;
     double err = 0.0;
     for (int s = 0; s < S && err <= best_err; ++s)
-      err = fmax(err, fabs((M0 ? M0[s] : 0.0) + (M1 ? M1[s] : 0.0) - Eo[s]));
+      err = fmax(err, fabs((M0 ? M0[s * NP] : 0.0) + (M1 ? M1[s * NP] : 0.0) - Eo[s]));
     if (err < best_err) {
       best_err = err;
       best = j;

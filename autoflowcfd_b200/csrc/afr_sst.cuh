@@ -200,66 +200,106 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
   for (int t = threadIdx.x; t < nc * S * 8; t += blockDim.x) p8[t] = sInv[(t >> 3) * 9 + (t & 7)];
 }
 
-// per face flux point: upwind convection and BR1-style diffusion corrections
+// per face flux point: upwind convection and BR1-style diffusion corrections.
+// One warp per face.  The face-point values are small FP64 products on the
+// tensor path (mma.sync m8n8k4 .f64): owner side (face points x S) x (S x 8
+// packed point values), neighbour side per source cell (face points x S) x
+// (S x k, omega, gamma_k, gamma_w); the second source is added to the first as
+// in the reference.  Lanes 0..P-1 then form the corrections.
+constexpr int SST_FACE_WARPS = 4;
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a0, double b0) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a0), "d"(b0));
+}
+
 template <int S, int NP>
-__global__ void k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= fc.F * NP) return;
-  const int f = t / NP, i = t % NP;
+__global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
+  constexpr int W = SST_FACE_WARPS, RW = 17;  // RW: po (8), pn of the first (4) and second (4) source, pad
+  __shared__ double sR[W][NP * RW];
+  const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int f = blockIdx.x * W + wi;
+  if (f >= fc.F) return;  // whole warps: only warp-level synchronisation below
+  const int gq = lane >> 2, tq = lane & 3;
   const int oc = fc.owner[f];
-  const int ct = cell_type(g, oc);
-  const int ax = fc.o_axis[f];
-  const double* E = ops.extrap + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * NP * S + i * S;
-  // owner side: rho, u (3), k, w, gamma_k, gamma_w (point values packed by k_sst_point)
-  double po[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int s = 0; s < S; ++s) {
-    const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)oc * S + s) * 8);
-    const double we = __ldg(E + s);
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const double2 v = __ldg(x + h);
-      po[2 * h] += we * v.x;
-      po[2 * h + 1] += we * v.y;
-    }
-  }
-  // neighbour side: k, w, gamma_k, gamma_w
-  double pn[4];
   const int c0 = fc.nb_c0[f], i1 = fc.nb_i1[f];
-  if (c0 < 0 && i1 < 0) {
-    const bool wz = a.wall_face[f] != 0;
-    pn[0] = wz ? -po[4] : po[4];
-    pn[1] = po[5];
-    pn[2] = po[6];
-    pn[3] = po[7];
-  } else {
-    for (int q = 0; q < 4; ++q) pn[q] = 0.0;
-    // k, w, gamma_k, gamma_w of the source cells, each summed over s in order
-    for (int src = 0; src < 2; ++src) {
-      const int c = src == 0 ? c0 : (i1 >= 0 ? fc.nb_c1[i1] : -1);
-      if (c < 0) continue;
-      const double* M = src == 0 ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S) : fmat(fc.nb_m1, fc.nb_m1i, i1, i, NP, S);
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int s = 0; s < S; ++s) {
-        const double2* x = reinterpret_cast<const double2*>(a.sp8 + ((size_t)c * S + s) * 8 + 4);
-        const double w = __ldg(M + s);
-        const double2 v0 = __ldg(x), v1 = __ldg(x + 1);
-        acc[0] += w * v0.x;
-        acc[1] += w * v0.y;
-        acc[2] += w * v1.x;
-        acc[3] += w * v1.y;
+  const int c1 = i1 >= 0 ? fc.nb_c1[i1] : -1;
+  const bool bnd = c0 < 0 && i1 < 0;
+  double* R = sR[wi];
+  {
+    const int ct = cell_type(g, oc);
+    const int ax = fc.o_axis[f];
+    const double* ET = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * S * NP;
+    const double* X = a.sp8 + (size_t)oc * S * 8;
+    for (int m0 = 0; m0 < NP; m0 += 8) {
+      const int i = m0 + gq;
+      double d0 = 0.0, d1 = 0.0;
+      for (int k0 = 0; k0 < S; k0 += 4) {
+        const int s = k0 + tq;
+        const double a0 = (i < NP && s < S) ? __ldg(ET + s * NP + i) : 0.0;
+        const double b0 = s < S ? __ldg(X + s * 8 + gq) : 0.0;
+        dmma884(d0, d1, a0, b0);
       }
-      for (int q = 0; q < 4; ++q) pn[q] = src == 0 ? acc[q] : pn[q] + acc[q];
+      if (i < NP) {
+        R[i * RW + 2 * tq] = d0;
+        R[i * RW + 2 * tq + 1] = d1;
+      }
     }
   }
-  const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
-  const double mflux = ((po[0] * po[1]) * tn[0] + (po[0] * po[2]) * tn[1]) + (po[0] * po[3]) * tn[2];
-  double* o = a.cfp + ((size_t)f * NP + i) * 4;
-  const double upk = mflux >= 0.0 ? po[4] : pn[0];
-  const double upw = mflux >= 0.0 ? po[5] : pn[1];
-  o[0] = mflux * (upk - po[4]);
-  o[1] = (0.5 * (po[6] + pn[2])) * (0.5 * (po[4] + pn[0]) - po[4]);
-  o[2] = mflux * (upw - po[5]);
-  o[3] = (0.5 * (po[7] + pn[3])) * (0.5 * (po[5] + pn[1]) - po[5]);
+  if (!bnd) {
+    for (int src = 0; src < 2; ++src) {
+      const int c = src == 0 ? c0 : c1;
+      if (c < 0) continue;
+      const double* X = a.sp8 + (size_t)c * S * 8 + 4;
+      for (int m0 = 0; m0 < NP; m0 += 8) {
+        const int i = m0 + gq;
+        const double* M = i < NP ? (src == 0 ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S)
+                                             : fmat(fc.nb_m1, fc.nb_m1i, i1, i, NP, S))
+                                 : nullptr;
+        double d0 = 0.0, d1 = 0.0;
+        for (int k0 = 0; k0 < S; k0 += 4) {
+          const int s = k0 + tq;
+          const double a0 = (M && s < S) ? __ldg(M + s * NP) : 0.0;
+          const double b0 = (s < S && gq < 4) ? __ldg(X + s * 8 + gq) : 0.0;
+          dmma884(d0, d1, a0, b0);
+        }
+        if (i < NP && tq < 2) {
+          R[i * RW + 8 + src * 4 + 2 * tq] = d0;
+          R[i * RW + 8 + src * 4 + 2 * tq + 1] = d1;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  for (int i = lane; i < NP; i += 32) {
+    const double* r = R + i * RW;
+    double po[8], pn[4];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) po[c] = r[c];
+    if (bnd) {
+      const bool wz = a.wall_face[f] != 0;
+      pn[0] = wz ? -po[4] : po[4];
+      pn[1] = po[5];
+      pn[2] = po[6];
+      pn[3] = po[7];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double p0 = c0 >= 0 ? r[8 + q] : 0.0;
+        pn[q] = c1 >= 0 ? p0 + r[12 + q] : p0;
+      }
+    }
+    const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
+    const double mflux = ((po[0] * po[1]) * tn[0] + (po[0] * po[2]) * tn[1]) + (po[0] * po[3]) * tn[2];
+    double* o = a.cfp + ((size_t)f * NP + i) * 4;
+    const double upk = mflux >= 0.0 ? po[4] : pn[0];
+    const double upw = mflux >= 0.0 ? po[5] : pn[1];
+    o[0] = mflux * (upk - po[4]);
+    o[1] = (0.5 * (po[6] + pn[2])) * (0.5 * (po[4] + pn[0]) - po[4]);
+    o[2] = mflux * (upw - po[5]);
+    o[3] = (0.5 * (po[7] + pn[3])) * (0.5 * (po[5] + pn[1]) - po[5]);
+  }
 }
 
 // per cell: volume transport terms, gather of the face corrections, outlier
