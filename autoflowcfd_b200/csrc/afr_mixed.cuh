@@ -569,7 +569,12 @@ struct MxVolSmem {
   static constexpr int oX = oR2 + szR2;
   // doubles: qbar, F(qbar); with VP also det and the metric divergence of the tile
   static constexpr int nX = C * 5 + C * 15 + (VP ? C * S * 4 : 0);
-  static constexpr int total = oX + nX * 8;
+  // the next tile's state rows (stride nv <= 8), 1/det and MD, copied
+  // asynchronously (P1, P2; at P3 the tile's loads are direct: no room)
+  static constexpr bool STG = VP;
+  static constexpr int oStg = oX + nX * 8;
+  static constexpr int nStg = STG ? C * S * 12 : 0;
+  static constexpr int total = oStg + nStg * 8;
   // TMEM columns: each product holds two column blocks (stacked hi / lo operand)
   static constexpr int cFq = 0, cD3 = 2 * Fq, cW = 2 * Fq + (VP ? 2 * Sq : 0);
   static constexpr int NCOL = pow2_cols(cW + 2 * Sq);
@@ -626,40 +631,58 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
   const uint32_t lane_base = (uint32_t)(q4 * 32) << 16;
   const int wsplit = warp >> 2, nsplit = NT / 128;  // warps sharing a lane quarter split the columns
 
+  // asynchronous copies of a tile's contiguous state, 1/det and MD blocks into
+  // the staging buffer; issued one tile ahead, so they overlap the tile before
+  double* sStg = reinterpret_cast<double*>(smem + L::oStg);
+  auto stage = [&](int tl) {
+    if constexpr (L::STG) {
+      const size_t eb = (size_t)cell_base + (size_t)tl * C;
+      const int nn = min(C, cell_end - (int)eb);
+      const double* ub = Ucur + eb * S * nv;
+      for (int t = tid; t < nn * S * nv; t += NT) cp_async8(sStg + t, ub + t);
+      for (int t = tid; t < nn * S; t += NT) cp_async8(sStg + C * S * 8 + t, mo.rdet + eb * S + t);
+      for (int t = tid; t < nn * S * 3; t += NT) cp_async8(sStg + C * S * 9 + t, mo.MD + eb * S * 3 + t);
+      cp_async_commit();
+    }
+  };
+  if (blockIdx.x < ntiles) stage(blockIdx.x);
+
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = cell_base + tile * C;
     const int nc = min(C, cell_end - e0);
     if (tid == 0 && tile + (int)gridDim.x < ntiles) {
-      // the next tile's inputs (contiguous cell ranges) into L2 while this one runs
+      // the next tile's remaining inputs (contiguous cell ranges) into L2 while this one runs
       const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
       const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
-      mxd::prefetch_l2(Ucur, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
       mxd::prefetch_l2(mo.adjf, (size_t)g.N * FN * 48, en * FN * 48, nn * FN * 48);
-      mxd::prefetch_l2(g.det, NS * 8, en * S * 8, nn * S * 8);
-      mxd::prefetch_l2(mo.MD, NS * 24, en * S * 24, nn * S * 24);
+      if (!L::STG) mxd::prefetch_l2(Ucur, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
       if (visc) {
         mxd::prefetch_l2(PFm, NS * 80, en * S * 80, nn * S * 80);
         mxd::prefetch_l2(mo.adjs, NS * 48, en * S * 48, nn * S * 48);
       }
+    }
+    if constexpr (L::STG) {
+      cp_async_wait0();  // this thread's copies of the tile
+      __syncthreads();   // everyone's
     }
     // ---- primitives (FP64), det and metric divergence of the tile ----
     for (int t = tid; t < C * S; t += NT) {
       const int c = t / S;
       double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
       if (c < nc) {
-        const size_t p = (size_t)e0 * S + t;
-        mxd::prim_T(Ucur + p * nv, q);
+        mxd::prim_T(L::STG ? sStg + t * nv : Ucur + ((size_t)e0 * S + t) * nv, q);
         if (L::VP) {
-          sDet[t] = __ldg(mo.rdet + p);  // reciprocal: the readouts multiply
-          sMD[t * 3 + 0] = mo.MD[p * 3 + 0];
-          sMD[t * 3 + 1] = mo.MD[p * 3 + 1];
-          sMD[t * 3 + 2] = mo.MD[p * 3 + 2];
+          sDet[t] = sStg[C * S * 8 + t];  // reciprocal: the readouts multiply
+          sMD[t * 3 + 0] = sStg[C * S * 9 + t * 3 + 0];
+          sMD[t * 3 + 1] = sStg[C * S * 9 + t * 3 + 1];
+          sMD[t * 3 + 2] = sStg[C * S * 9 + t * 3 + 2];
         }
       }
 #pragma unroll
       for (int v = 0; v < 5; ++v) sQ[t * 5 + v] = q[v];
     }
     __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) stage(tile + (int)gridDim.x);  // the staging buffer is free again
     for (int t = tid; t < C * 5; t += NT) {
       const int c = t / 5, v = t % 5;
       double acc = 0.0;
@@ -833,6 +856,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     __syncthreads();
     tc::fence_after();
   }
+  if constexpr (L::STG) cp_async_wait0();  // copies still in flight after an aborted tile
   tc::fence_before();
   __syncthreads();
   if (warp == 0) {
