@@ -242,7 +242,11 @@ struct MxPreSmem {
   static constexpr int oG = oB2 + NB2MAX * Sq * 4;     // reference-space gradients [c][s][m][phi]
   static constexpr int oQ = oG + MX_PRE_CELLS * S * 12 * 4;  // q and T (FP64) [c][s][6]
   static constexpr int oM = oQ + MX_PRE_CELLS * S * 6 * 8;   // means (FP64) [c][9]
-  static constexpr int total = oM + MX_PRE_CELLS * 9 * 8;
+  // the next tile's state rows (stride nv <= 8) and nu_t, copied asynchronously
+  // (P1, P2; at P3 the tile's loads are direct: no room)
+  static constexpr bool STG = S <= 27;
+  static constexpr int oStg = oM + MX_PRE_CELLS * 9 * 8;
+  static constexpr int total = oStg + (STG ? MX_PRE_CELLS * S * 9 * 8 : 0);
   static constexpr int NCOL = pow2_cols(cmax(NB1, NB2MAX));
 };
 
@@ -290,22 +294,46 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
   uint32_t phase = 0;
   const int ntiles = (cell_end - cell_base + C - 1) / C;
 
+  // asynchronous copies of a tile's contiguous state and nu_t blocks into the
+  // staging buffer; issued one tile ahead, so they overlap the tile before
+  double* sStg = reinterpret_cast<double*>(smem + L::oStg);
+  auto stage = [&](int tl) {
+    if constexpr (L::STG) {
+      const size_t eb = (size_t)cell_base + (size_t)tl * C;
+      const int nn = min(C, cell_end - (int)eb);
+      const double* ub = U + eb * S * nv;
+      for (int t = tid; t < nn * S * nv; t += MX_THREADS) cp_async8(sStg + t, ub + t);
+      if (nut)
+        for (int t = tid; t < nn * S; t += MX_THREADS) cp_async8(sStg + C * S * 8 + t, nut + eb * S + t);
+      cp_async_commit();
+    }
+  };
+  if (blockIdx.x < ntiles) stage(blockIdx.x);
+
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = cell_base + tile * C;
     const int nc = min(C, cell_end - e0);
     if (tid == 0 && tile + (int)gridDim.x < ntiles) {
-      // the next tile's inputs (contiguous cell ranges) into L2 while this one runs
+      // the next tile's remaining inputs (contiguous cell ranges) into L2 while this one runs
       const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
       const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
-      mxd::prefetch_l2(U, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
+      if (!L::STG) mxd::prefetch_l2(U, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
       if (visc) mxd::prefetch_l2(mo.invs, NS * 48, en * S * 48, nn * S * 48);
-      if (nut) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
+      if (nut && !L::STG) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
     }
+    if constexpr (L::STG) {
+      cp_async_wait0();  // this thread's copies of the tile
+      __syncthreads();   // everyone's
+    }
+    // nu_t of the tile's point t = c*S + s
+    auto nut_at = [&](int c, int s) -> double {
+      return L::STG ? sStg[C * S * 8 + c * S + s] : nut[(size_t)(e0 + c) * S + s];
+    };
     // primitives and temperature in FP64
     for (int t = tid; t < C * S; t += MX_THREADS) {
       const int c = t % C, s = t / C;
       double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
-      if (c < nc) mxd::prim_T(U + ((size_t)(e0 + c) * S + s) * nv, q);
+      if (c < nc) mxd::prim_T(L::STG ? sStg + (c * S + s) * nv : U + ((size_t)(e0 + c) * S + s) * nv, q);
 #pragma unroll
       for (int v = 0; v < 6; ++v) sQ[(c * S + s) * 6 + v] = q[v];
     }
@@ -323,7 +351,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       const int c = t % C, s = t / C;
       const double* q = sQ + (c * S + s) * 6;
       if (c < nc) {
-        const float mutf = (visc && nut) ? float(q[0] * nut[(size_t)(e0 + c) * S + s]) : 0.f;
+        const float mutf = (visc && nut) ? float(q[0] * nut_at(c, s)) : 0.f;
         float4* o = reinterpret_cast<float4*>(mb.PFm + ((size_t)(e0 + c) * S + s) * 20);
         o[3] = make_float4(mutf, float(q[0]), float(q[1]), float(q[2]));
         o[4] = make_float4(float(q[3]), float(q[4]), 0.f, 0.f);
@@ -333,7 +361,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
 #pragma unroll
         for (int f = 0; f < 4; ++f)
           mxd::st_split(sA1, 128 * Sq, tc::kmajor_index(f * C + c, s, 128), float(phi[f] - sM[c * 9 + 5 + f]));
-        const double mut = (c < nc && nut) ? q[0] * nut[(size_t)(e0 + c) * S + s] : 0.0;
+        const double mut = (c < nc && nut) ? q[0] * nut_at(c, s) : 0.0;
         mxd::st_split(sB2, NB2 * Sq, tc::kmajor_index(17 * C + c, s, NB2), float(mut));
       }
 #pragma unroll
@@ -342,6 +370,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     }
     tc::fence_async_smem();
     __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) stage(tile + (int)gridDim.x);  // the staging buffer is free again
     if (visc) {
       if (tid == 0) {
         tc::fence_after();
@@ -431,6 +460,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     __syncthreads();
     tc::fence_after();
   }
+  if constexpr (L::STG) cp_async_wait0();  // copies still in flight after an aborted tile
   tc::fence_before();
   __syncthreads();
   if (warp == 0) {
