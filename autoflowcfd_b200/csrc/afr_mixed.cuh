@@ -988,24 +988,29 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   }
   __syncthreads();
   // lift the jumps of each cell's slots, ascending color order
-  for (int t = tid; t < nc * S * 5; t += blockDim.x) {
-    const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
-    const double rdj = sRd[b * S + s];  // reciprocal formed at create
-    double ci = 0.0, cv = 0.0;
+  // one thread per point: each slot's metadata decoded once for all variables
+  for (int p = tid; p < nc * S; p += blockDim.x) {
+    const int b = p / S, s = p - b * S;
+    const double rdj = sRd[p];  // reciprocal formed at create
+    double ci[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, cv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int k = sPtr[b]; k < sPtr[b + 1]; ++k) {
       const int fl = staged ? sFl[k - k_beg] : a.slot_flags[k];
       const int ax = (fl >> 2) & 3;
       const int fp = sDfp[ax * S + s];
       const double gw = sGw[((fl & 16) ? 4 : 0) + sDco[ax * S + s]];
       const float* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10;
-      ci -= gw * double(Jk[v]);
-      if (visc) cv += gw * double(Jk[5 + v]);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        ci[v] -= gw * double(Jk[v]);
+        if (visc) cv[v] += gw * double(Jk[5 + v]);
+      }
     }
-    ci *= rdj;
-    cv *= rdj;
-    const float* rp = sRVf + (b * S + s) * 10;
-    sRi[t] = double(rp[v]) + ci;
-    sRv[t] = visc ? double(rp[5 + v]) + cv : 0.0;
+    const float* rp = sRVf + p * 10;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      sRi[p * 5 + v] = double(rp[v]) + ci[v] * rdj;
+      sRv[p * 5 + v] = visc ? double(rp[5 + v]) + cv[v] * rdj : 0.0;
+    }
   }
   __syncthreads();
   suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
