@@ -99,7 +99,7 @@ def initial_state(case, spec):
 # DRAM bytes per cell and launch of the mixed stage kernels, measured with ncu
 # on the 76,800-prism P2 SST case (profiles/mixed_stage_kernels_p2_sst_prism_76800.md);
 # a full-size launch moves these times the number of cells.
-MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 8372.0, "k_mx_face": 7077.0, "k_mx_vol": 11389.0, "k_mx_update": 6115.0}
+MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 8383.0, "k_mx_face": 7075.0, "k_mx_vol": 9912.0, "k_mx_update": 6126.0}
 
 
 def mixed_algorithmic_bytes(case, nv=7):
