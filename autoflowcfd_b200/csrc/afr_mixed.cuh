@@ -7,7 +7,7 @@
 // geometry metrics, the primitive recovery from the conserved state, the
 // residual sums and RK update, the norm and the force coefficients.
 //
-// Three kernels per stage (same data flow as the reference's residual,
+// Four kernels per stage (same data flow as the reference's residual,
 // core/fr_residual/inviscid.py:139-345 and core/fr_residual/viscous_flux.py:113-302):
 //   k_mx_pre   per 8-cell tile: gradients of (u,v,w,T) (D_3d as a GEMM) and the
 //              extrapolation of all point fields to every face point of the
@@ -21,7 +21,8 @@
 //   k_mx_vol   per C-cell tile (persistent): c2f, viscous D_3d and the folded
 //              W = f2c*D_fine divergence as GEMMs -> volume terms (FP32);
 //   k_mx_update per few cells: lifting in ascending color order, outlier
-//              zeroing, SSP-RK3 combination, positivity, filter (FP64).
+//              zeroing, SSP-RK3 combination, positivity (FP64), filter (an
+//              FP64 product on the tensor path).
 //
 // Contraction inputs are deviations from the cell mean where the operator
 // reproduces constants (c2f, extrapolation, derivatives), so the split error is
