@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   // then R (volume residuals, then with the interface corrections), T
   // (transport k, w + padding for the outlier helper) and Ref
   __shared__ double X[CPB * S * 18];
+  __shared__ double sRd[CPB * S];         // det, then 1 / det
   __shared__ double work[CPB * OUT_WORK];
   double* sInv = X;
   double* sAdj = X + CPB * S * 9;
@@ -336,9 +337,13 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
       cp_async8(sInv + t, ib + t);
       cp_async8(sAdj + t, ab + t);
     }
+    for (int t = threadIdx.x; t < nc * S; t += blockDim.x) cp_async8(sRd + t, g.det + (size_t)e0 * S + t);
     cp_async_wait_all();
   }
   __syncthreads();
+  // one reciprocal of det per point (published by the next barrier): each use
+  // differs from a division by det by at most an ulp
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) sRd[t] = 1.0 / sRd[t];
   const double* fl = sP + 4;  // k, w, gamma_k, gamma_w of point p at fl[p * 9 + 0..3]
   // grad k, grad w in reference space (D3g rows s*3+m) as one FP64
   // tensor-core product: columns (cell, field)
@@ -387,7 +392,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
         [&](int k, int col) { return Ft[((col >> 2) * S * 3 + k) * 4 + (col & 3)]; },
         [&](int s, int col, double x) {
           const int b = col >> 2;
-          R[(b * S + s) * 4 + (col & 3)] = -x / g.det[(size_t)(e0 + b) * S + s];
+          R[(b * S + s) * 4 + (col & 3)] = -x * sRd[b * S + s];
         });
   }
   // one thread per point, all four fields; the slots are fetched four at a time
@@ -395,8 +400,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
     const int s = p % S;
     const int e = e0 + p / S;
-    // one reciprocal per point: each term differs from contrib / det by at most an ulp
-    const double rdj = 1.0 / g.det[(size_t)e * S + s];
+    const double rdj = sRd[p];
     double C[4] = {0.0, 0.0, 0.0, 0.0};
     const int sb = fc.tslot_ptr[e], se = fc.tslot_ptr[e + 1];
     for (int s0 = sb; s0 < se; s0 += 4) {
@@ -431,6 +435,16 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     for (int q = 0; q < 4; ++q) Ref[p * 4 + q] = C[q];  // staged: R is complete only after the barrier below
   }
   __syncthreads();
+  // the fluxes are consumed: their space receives the tile's point sources
+  // (Sk, Sw, beta, ...) and dt by asynchronous copies for the final update
+  double* sPt = Ft;
+  double* sDtS = Ft + CPB * S * 5;
+  {
+    const double* pb = a.pt + (size_t)e0 * S * 5;
+    for (int t = threadIdx.x; t < nc * S * 5; t += blockDim.x) cp_async8(sPt + t, pb + t);
+    for (int t = threadIdx.x; t < nc * S; t += blockDim.x) cp_async8(sDtS + t, a.dt + (size_t)e0 * S + t);
+    cp_async_commit();
+  }
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
     const double rho = sP[p * 9];
     const double* Cp = Ref + p * 4;
@@ -449,14 +463,15 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     Ref[p * 5 + 2] = 0.0; Ref[p * 5 + 3] = 0.0; Ref[p * 5 + 4] = 0.0;
   }
   __syncthreads();
+  cp_async_wait0();  // published by the barriers inside the outlier pass
   suppress_outliers_blocks<S>(T, Ref, 5, nc, work);
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
     const size_t p = (size_t)e0 * S + t;
     const double rho = sP[t * 9];
     const double tk = dfinite(T[t * 5 + 0]);
     const double tw = dfinite(T[t * 5 + 1]);
-    const double* pt = a.pt + p * 5;
-    const double dts = a.dt[p];
+    const double* pt = sPt + t * 5;
+    const double dts = sDtS[t];
     const double kf = fl[t * 9 + 0], wf = fl[t * 9 + 1];
     const double wo = fmax(wf, 1e-10);
     const double dkd = dfinite((pt[0] / fmax(rho, 1e-10)) / (1.0 + dts * (SST_BSTAR * wo)));
