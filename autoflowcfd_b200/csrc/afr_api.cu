@@ -41,6 +41,7 @@ struct afr_handle {
   double* norm_part = nullptr;
   double* norm_rho_part = nullptr;
   double* red = nullptr;      // reduction results
+  double* red_part = nullptr; // per-chunk partials of the two-level reductions
   double* pt = nullptr;
   double* cfp = nullptr;
   double* sp8 = nullptr;
@@ -142,6 +143,26 @@ __global__ void k_reduce_sum(const double* x, size_t n, double* out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = sh[0];
+}
+
+// First level of the deterministic reductions: CTA b sums (or takes the
+// minimum of) x[b*RED_CHUNK, (b+1)*RED_CHUNK) in a fixed order; the second
+// level runs k_reduce_sum / k_reduce_min over the partials in one CTA.
+constexpr int RED_CHUNK = 8192, RED_THREADS = 256;
+template <bool MIN>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_chunks(const double* __restrict__ x, size_t n,
+                                                               double* __restrict__ part) {
+  __shared__ double sh[RED_THREADS];
+  const size_t b0 = (size_t)blockIdx.x * RED_CHUNK, b1 = b0 + RED_CHUNK < n ? b0 + RED_CHUNK : n;
+  double acc = MIN ? INFINITY : 0.0;
+  for (size_t i = b0 + threadIdx.x; i < b1; i += RED_THREADS) acc = MIN ? fmin(acc, x[i]) : acc + x[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = RED_THREADS / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] = MIN ? fmin(sh[threadIdx.x], sh[threadIdx.x + o]) : sh[threadIdx.x] + sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 __global__ void k_reduce_min(const double* x, size_t n, double* out) {
@@ -508,7 +529,9 @@ int compute_dt(afr_handle* h, const double* U, const double* nut, double* dt, cu
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(h, e, "local dt");
   if (h->prm.global_dt_factor > 0.0) {
-    k_reduce_min<<<1, 1024, 0, st>>>(dt, n, h->red);
+    const unsigned nb = (unsigned)((n + RED_CHUNK - 1) / RED_CHUNK);
+    k_reduce_chunks<true><<<nb, RED_THREADS, 0, st>>>(dt, n, h->red_part);
+    k_reduce_min<<<1, 1024, 0, st>>>(h->red_part, nb, h->red);
     k_fill_scaled<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dt, n, h->red, h->prm.global_dt_factor);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "global dt");
@@ -1166,6 +1189,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   if ((rc = dalloc(h, &h->norm_part, N))) return bail(rc);
   if ((rc = dalloc(h, &h->norm_rho_part, N))) return bail(rc);
   if ((rc = dalloc(h, &h->red, 4))) return bail(rc);
+  if ((rc = dalloc(h, &h->red_part, (N * S + RED_CHUNK - 1) / RED_CHUNK + 1))) return bail(rc);
   if (prm->turb == AFR_TURB_SST) {
     if ((rc = dalloc(h, &h->pt, N * S * 5))) return bail(rc);
     if ((rc = dalloc(h, &h->cfp, F * P * 4))) return bail(rc);
@@ -1262,8 +1286,12 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
     return r;
   });
   if (e != cudaSuccess) return cuda_fail(h, e, "step");
-  k_reduce_sum<<<1, 1024, 0, st>>>(h->norm_part, (size_t)h->N, h->red);
-  nl += 1;
+  {
+    const unsigned nb = (unsigned)(((size_t)h->N + RED_CHUNK - 1) / RED_CHUNK);
+    k_reduce_chunks<false><<<nb, RED_THREADS, 0, st>>>(h->norm_part, (size_t)h->N, h->red_part);
+    k_reduce_sum<<<1, 1024, 0, st>>>(h->red_part, nb, h->red);
+  }
+  nl += 2;
   if (tm) tm->mark(st);
   if (launches) *launches = nl;
   if (norm_out) {
