@@ -122,6 +122,12 @@ __global__ void k_form_adj(const double* det, const double* inv, double* adj, si
   adj[t] = det[t / 9] * inv[t];  // compute_adj_j, core/fr_operators/volume_contract.py:47-80
 }
 
+// |volume|^(1/3) per cell, the length of the local time step (core/fr_solver/cfl.py)
+__global__ void k_cube_root_abs(const double* v, size_t n, double* out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = pow(fabs(v[t]), 1.0 / 3.0);
+}
+
 __global__ void k_metric_flux_scale(const double* adj, double* mfs, size_t npts) {
   const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npts) return;
@@ -945,7 +951,10 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     cudaFree(invf);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "geometry set-up"));
   }
-  h->g = Geom{h->N, h->n_prism, det, inv, adj, adjf, vol, mfs, wd};
+  double* hvol;
+  if ((rc = dalloc(h, &hvol, N))) return bail(rc);
+  k_cube_root_abs<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(vol, N, hvol);
+  h->g = Geom{h->N, h->n_prism, det, inv, adj, adjf, vol, mfs, wd, hvol};
 
   // ---- operators ----
   std::vector<double> Wkeep[2];

@@ -57,6 +57,7 @@ struct Geom {
   const double* volume;     // (N)
   const double* mfs;        // (N, S) sum_m |adj[m,:]|
   const double* wall_dist;  // (N, S) or null
+  const double* hvol;       // (N) |volume|^(1/3), the local-dt length (formed once at create)
 };
 
 // Face records.  A "slot" is one side of one face record whose own

@@ -507,7 +507,7 @@ __global__ void k_local_dt(Geom g, int S, int order, const double* __restrict__ 
   const double a = sqrt(fmax(1.4 * pr / fmax(rho, 1e-10), 1e-10));
   const double vm = sqrt(ux * ux + uy * uy + uz * uz);
   const double wave = fmax(vm + a, 1e-10);
-  const double h = pow(fabs(g.volume[e]), 1.0 / 3.0);
+  const double h = g.hvol[e];  // pow(|volume|, 1/3), formed at create
   const double CFL = 0.1;
   const double fa = 1.0 / (2 * order + 1);
   const double fv = 1.0 / ((2 * order + 1) * (2 * order + 1));
