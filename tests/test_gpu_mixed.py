@@ -88,3 +88,18 @@ def test_mixed_refuses_ill_conditioned_operators(golden):
     # 2^-24 of that exceeds the quantities being computed
     with pytest.raises(_lib.AfrError, match="row l1"):
         make(golden("tet_p3_tgv"), "mixed")
+
+
+def test_launch_shape_reports_the_persistent_grids(golden):
+    """afr_launch_shape: the pre-pass residency is computed from registers,
+    shared memory and threads (at least one CTA per SM, at most two by tensor
+    memory), the volume kernel holds one CTA per SM, and the plain form reports
+    -1 for the mixed-form shapes."""
+    case = golden("prism_p2_sst")
+    smx, s64 = make(case, "mixed"), make(case, "fp64")
+    ls = smx.launch_shape()
+    assert ls["n_sms"] > 0 and 1 <= ls["pre_per_sm"] <= ls["pre_max_per_sm"] <= 2
+    assert ls["vol_per_sm"] == 1 and ls["face_block"] in (64, 128, 256) and ls["update_variant"] in (0, 1, 2)
+    assert s64.launch_shape()["pre_per_sm"] == -1
+    smx.cleanup()
+    s64.cleanup()
