@@ -74,6 +74,14 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // fetch operands and c(m, n, value) stores results; block-wide work split by
 // warp, no barrier inside.  The sum order over k is the unit's, so results
 // can differ from a sequential FP64 sum in the last bits.
+// one m8n8k4 FP64 step: lane (g = lane/4, t = lane%4) supplies A[g][t] and
+// B[t][g] and holds D[g][2t], D[g][2t+1]
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a0, double b0) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a0), "d"(b0));
+}
+
 template <class FA, class FB, class FC>
 __device__ __forceinline__ void dmma_product(int M, int N, int K, FA a, FB b, FC c) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -86,9 +94,7 @@ __device__ __forceinline__ void dmma_product(int M, int N, int K, FA a, FB b, FC
       const int k = k0 + t;
       const double a0 = (m < M && k < K) ? a(m, k) : 0.0;
       const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
-      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                   : "+d"(c0), "+d"(c1)
-                   : "d"(a0), "d"(b0));
+      dmma884(c0, c1, a0, b0);
     }
     const int n = n0 + 2 * t;
     if (m < M) {

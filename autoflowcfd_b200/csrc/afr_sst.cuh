@@ -208,12 +208,6 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
 // in the reference.  Lanes 0..P-1 then form the corrections.
 constexpr int SST_FACE_WARPS = 4;
 
-__device__ __forceinline__ void dmma884(double& d0, double& d1, double a0, double b0) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a0), "d"(b0));
-}
-
 template <int S, int NP>
 __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
   constexpr int W = SST_FACE_WARPS, RW = 17;  // RW: po (8), pn of the first (4) and second (4) source, pad
