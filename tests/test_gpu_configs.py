@@ -1,0 +1,88 @@
+"""The small configuration at full size on the GPU: inviscid Euler, P1, an
+isentropic vortex (strength 5, free-stream Mach 0.5) on a triply periodic
+16 x 16 x 16-hex unit cube split into 24,576 tets, SSP-RK3 with the global
+time step 3 * min(dt_local) (CFL 0.3), through the C-ABI.
+
+- Plain form against the oracle on the same generated tables, two steps,
+  relative max-norm 1e-12.
+- Mixed form against the plain form over the full 100 steps: field relative
+  L2 1e-6 (the mixed form's target), and the vortex's kinetic energy."""
+import numpy as np
+import pytest
+
+from autoflowcfd_b200 import boxgeom, boxmesh
+from autoflowcfd_b200.solver import B200FRSolver
+
+pytestmark = pytest.mark.gpu
+
+GAMMA, RHO, P = 1.4, 1.225, 101325.0
+
+
+def vortex(xyz, L=1.0, beta=5.0):
+    """Isentropic vortex (published form; the reference's
+    tests/validation/_isentropic_vortex.py:42-71), centre at the box centre,
+    core radius 0.2 L, carried by u = 0.5 a along x."""
+    a = np.sqrt(GAMMA * P / RHO)
+    u0 = 0.5 * a
+    x, y = xyz[..., 0] - 0.5 * L, xyz[..., 1] - 0.5 * L
+    rc = 0.2 * L
+    r2 = (x / rc) ** 2 + (y / rc) ** 2
+    swirl = beta * a / (2 * np.pi) * np.exp(0.5 * (1 - r2))
+    theta = 1 - (GAMMA - 1) * beta**2 / (8 * GAMMA * np.pi**2) * np.exp(1 - r2)
+    rho = RHO * theta ** (1 / (GAMMA - 1))
+    p = P * theta ** (GAMMA / (GAMMA - 1))
+    u, v = u0 - swirl * y / rc, swirl * x / rc
+    U = np.stack([rho, rho * u, rho * v, np.zeros_like(rho), p / (GAMMA - 1) + 0.5 * rho * (u * u + v * v)], -1)
+    return U, u0
+
+
+@pytest.fixture(scope="module")
+def c1():
+    box = boxmesh.tet_box(16, 16, 16, (1.0, 1.0, 1.0), jitter=0.0, periodic=True)
+    case = boxgeom.build_case(box, 1, None, wall_distance=False, want_sps_coords=True)
+    U, u0 = vortex(case.pop("sps_coords"))
+    return case, U, u0
+
+
+def solver(case, U, u0, precision):
+    s = B200FRSolver(case, turb_model_name="NONE", mu_molecular=1.8e-5, rho_inf=RHO, vel_inf=u0, p_inf=P,
+                     inviscid_only=True, global_dt_factor=3.0, precision=precision)
+    s.set_state_from_cpu(U)
+    return s
+
+
+def test_c1_plain_form_matches_oracle(c1):
+    from oracle import fr_oracle as O
+
+    case, U, u0 = c1
+    assert int(case["n_cells"]) == 24576
+    dense = dict(case)
+    tab = dense.pop("src_mat_table")
+    for key in ("nb_src0_mat", "nb_src1_mat", "ow_src0_mat", "ow_src1_mat"):
+        dense[key] = tab[dense.pop(key + "_index")]
+    so = O.Solver(O.Mesh.from_case(dense), U.copy(), 1.8e-5, None, None, True, 3.0)
+    s = solver(case, U, u0, "fp64")
+    for _ in range(2):
+        so.step()
+        s.step()
+        got = s.U.cpu().numpy()
+        assert np.max(np.abs(got - so.U)) <= 1e-12 * np.max(np.abs(so.U))
+    s.cleanup()
+
+
+def test_c1_mixed_form_tracks_plain_over_100_steps(c1):
+    case, U, u0 = c1
+    s64, smx = solver(case, U, u0, "fp64"), solver(case, U, u0, "mixed")
+    for _ in range(100):
+        s64.step(want_norm=False)
+        smx.step(want_norm=False)
+    a, b = smx.U.cpu().numpy(), s64.U.cpu().numpy()
+    assert np.all(np.isfinite(a))
+    assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b)
+
+    def ke(W):
+        return float(np.sum(0.5 * (W[..., 1] ** 2 + W[..., 2] ** 2 + W[..., 3] ** 2) / W[..., 0]))
+
+    assert abs(ke(a) - ke(b)) <= 1e-6 * ke(b)
+    s64.cleanup()
+    smx.cleanup()
