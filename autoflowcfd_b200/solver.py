@@ -225,6 +225,14 @@ class B200FRSolver:
         check(LIB.afr_device_bytes(self._h, ctypes.byref(v)), self._h)
         return int(v.value)
 
+    def autotune(self) -> list:
+        """Choose the mixed form's launch shapes by timing residual evaluations
+        of the current state (afr_autotune); [pre CTAs per SM, face block,
+        update variant], or -1s for the plain form.  Results do not change."""
+        ch = (ctypes.c_int32 * 3)()
+        check(LIB.afr_autotune(self._h, _dev_ptr(self.U), _dev_ptr(self.nu_t), ch, _stream()), self._h)
+        return [int(v) for v in ch]
+
     def launch_shape(self) -> dict:
         """Launch shapes of the mixed-form kernels (see afr_launch_shape)."""
         out = (ctypes.c_int32 * 8)()
