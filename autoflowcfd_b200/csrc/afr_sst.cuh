@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     const double Sm = sqrt(2.0 * ss);
     const double gd = gp[3][0] * gp[4][0] + gp[3][1] * gp[4][1] + gp[3][2] * gp[4][2];
     // --- compute_source_terms ---
-    const double nu = MU_SOURCE / fmax(rho, 1e-10);
+    const double rrho = 1.0 / fmax(rho, 1e-10);  // one reciprocal: each use within an ulp of a division
+    const double nu = MU_SOURCE * rrho;
     const double k_s = fmin(kf, 1e40);
     const double w_s = fmax(fmin(wf, 1e40), 1e-10);
     const double CD = fmax(2.0 * rho * SST_SW2 / w_s * gd, 1e-10);
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     const double F2 = sst_F2(k_s, w_s, d, nu);
     const double beta = F1 * SST_B1 + (1.0 - F1) * SST_B2;
     double nut = SST_A1 * fmax(k_s, 1e-10) / fmax(SST_A1 * fmax(w_s, 1e-10), F2 * fmax(Sm, 1e-10));
-    nut = fmin(nut, SST_TVR * MU_SOURCE / fmax(rho, 1e-10));
+    nut = fmin(nut, SST_TVR * MU_SOURCE * rrho);
     if (!isfinite(nut)) nut = 0.0;
     double Pk = nut * rho * (Sm * Sm);
     Pk = fmin(Pk, 10.0 * SST_BSTAR * rho * k_s * w_s);
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     const double Sk = dfinite(Pk - Dk);
     const double Sw = dfinite(Pw - Dw + CDw);
     // --- transport diffusion coefficients (mu = molecular viscosity of the mean flow) ---
-    const double nu_m = a.mu / fmax(rho, 1e-10);
+    const double nu_m = a.mu * rrho;
     const double CD2 = fmax(2.0 * rho * SST_SW2 / fmax(wf, 1e-10) * gd, 1e-10);
     const double F1t = sst_F1(kf, wf, d, nu_m, rho, CD2);
     const double sk = F1t * SST_SK1 + (1.0 - F1t) * SST_SK2;
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
     // outputs staged in this point's own rows (read above by this thread only),
     // then stored as contiguous blocks
     const double gk = a.mu + sk * rnut, gw = a.mu + sw * rnut;
-    const double r1 = u[1] / rho, r2 = u[2] / rho, r3 = u[3] / rho;
+    const double r1 = u[1] * rrho, r2 = u[2] * rrho, r3 = u[3] * rrho;
     double* o = f + t * 5;
     o[0] = Sk;
     o[1] = Sw;
