@@ -78,6 +78,7 @@ SIGNATURES = {
     "afr_step_profile": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     "afr_rms_norm_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "afr_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P_I64, _P_I32, ctypes.c_int32, ctypes.c_void_p]),
     "afr_autotune": (ctypes.c_int, [ctypes.c_void_p] * 3 + [_P_I32, ctypes.c_void_p]),
     "afr_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _P_I32]),
     "afr_segment_norms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P_I64, ctypes.c_int32, _P_D,

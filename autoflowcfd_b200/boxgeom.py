@@ -16,7 +16,7 @@ enough for millions of cells:
 * face records (which records exist, owner / neighbour roles, primary flags,
   interpolation sources and their matrices) are replayed from a 3x3x3-hex
   template the reference itself flattened (``data/tmpl_<kind>_p<order>.npz``,
-  made by ``data/make_tables.py``): every cell copies the records of the
+  made by ``tests/golden/make_tables.py``): every cell copies the records of the
   template cell in the same topological position (low boundary / interior /
   high boundary per axis);
 * face colors come from the reference's greedy rule (C++ in libafr_b200.so).
@@ -191,10 +191,14 @@ def _rel_cells(box, H, rel):
 
 
 def build_case(box: BoxMesh, order: int, plane_cfg: Optional[dict] = None, wall_distance: bool = False,
-               want_sps_coords: bool = False) -> Dict[str, np.ndarray]:
+               want_sps_coords: bool = False, colorer=None) -> Dict[str, np.ndarray]:
     """Flattened FR case for ``box`` at polynomial order ``order``.
 
     Args:
+        colorer: ``f(owner, neighbor, is_boundary, n_cells) -> colors``; the
+            default is the library's C++ greedy coloring.  A caller that must
+            not load the library passes another implementation of the same
+            rule.
         plane_cfg: boundary configuration per plane name (PLANE_NAMES), dicts
             as the reference's BoundaryGhostStateProvider takes
             ({"type": "WALL", "is_no_slip": True}, {"type": "FARFIELD",
@@ -284,9 +288,9 @@ def build_case(box: BoxMesh, order: int, plane_cfg: Optional[dict] = None, wall_
     case["true_area_weight"] = np.outer(area, rel_w)
     case["face_node_ids"] = nid
     # ---- colors ----
-    from ._lib import greedy_face_coloring
-
-    case["colors"] = greedy_face_coloring(owner, case["neighbor_cell"], case["is_boundary"], N)
+    if colorer is None:
+        from ._lib import greedy_face_coloring as colorer
+    case["colors"] = colorer(owner, case["neighbor_cell"], case["is_boundary"], N)
     # ---- boundary conditions ----
     isb = case["is_boundary"].astype(bool)
     plane = np.full(F, -1, np.int64)

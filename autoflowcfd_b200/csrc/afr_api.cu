@@ -52,6 +52,12 @@ struct afr_handle {
   int n_cd_faces = 0;
   double* cd_part = nullptr;  // (n_cd_faces, 6)
   unsigned* status = nullptr;
+  // asynchronous status read of steps taken without a norm: the step copies
+  // the device word into pinned host memory and records status_ev; the next
+  // call on the handle reports a problem once that copy has completed
+  unsigned* status_host = nullptr;
+  cudaEvent_t status_ev = nullptr;
+  bool status_pending = false;
   // mixed-precision form (prec == AFR_PREC_MIXED)
   int prec = AFR_PREC_FP64;
   MxOps mo{};
@@ -507,15 +513,50 @@ cudaError_t dispatch(afr_handle* h, Fn&& fn) {
   return cudaErrorInvalidValue;
 }
 
+int status_code(afr_handle* h, unsigned s) {
+  if (s & DS_BAD_INDEX) return fail(h, AFR_EINDEX, "kernel saw an out-of-range table index");
+  if (s & DS_NONFINITE) return fail(h, AFR_ENONFINITE, "non-finite value in the state");
+  if (s & DS_TC_TIMEOUT) return fail(h, AFR_ECUDA, "a tensor-core completion wait timed out");
+  return AFR_OK;
+}
+
 int check_status(afr_handle* h, cudaStream_t st) {
   unsigned s = 0;
   cudaError_t e = cudaMemcpyAsync(&s, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(h, e, "status read");
-  if (s & DS_BAD_INDEX) return fail(h, AFR_EINDEX, "kernel saw an out-of-range table index");
-  if (s & DS_NONFINITE) return fail(h, AFR_ENONFINITE, "non-finite value in the state");
-  if (s & DS_TC_TIMEOUT) return fail(h, AFR_ECUDA, "a tensor-core completion wait timed out");
-  return AFR_OK;
+  h->status_pending = false;
+  return status_code(h, s);
+}
+
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Status of an earlier step taken without a norm, if its asynchronous copy has
+// completed; never waits.
+int pending_status(afr_handle* h, cudaStream_t st) {
+  if (!h->status_pending || capturing(st)) return AFR_OK;
+  const cudaError_t q = cudaEventQuery(h->status_ev);
+  if (q == cudaErrorNotReady) {
+    (void)cudaGetLastError();  // not an error: leave no trace for later launch checks
+    return AFR_OK;
+  }
+  if (q != cudaSuccess) return cuda_fail(h, q, "status event");
+  h->status_pending = false;
+  return status_code(h, *h->status_host);
+}
+
+// Queue the copy of the device status word to the pinned host word.  Outside
+// stream capture an event marks its completion for pending_status; inside a
+// capture the copy becomes part of the graph and afr_status reads the word.
+cudaError_t queue_status_copy(afr_handle* h, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(h->status_host, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess || capturing(st)) return e;
+  e = cudaEventRecord(h->status_ev, st);
+  if (e == cudaSuccess) h->status_pending = true;
+  return e;
 }
 
 StageArgs base_args(afr_handle* h) {
@@ -683,6 +724,8 @@ int afr_device_bytes(const afr_handle* h, uint64_t* out) {
 
 int afr_destroy(afr_handle* h) {
   if (!h) return AFR_EINVAL;
+  if (h->status_ev) cudaEventDestroy(h->status_ev);
+  if (h->status_host) cudaFreeHost(h->status_host);
   for (void* p : h->allocs) cudaFree(p);
   delete h;
   return AFR_OK;
@@ -919,6 +962,10 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
 
   if ((rc = dalloc(h, &h->status, 1))) return bail(rc);
   cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+  if (cudaHostAlloc((void**)&h->status_host, sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->status_ev, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(h, AFR_ENOMEM, "pinned status word"));
+  *h->status_host = 0;
 
   // ---- geometry ----
   double *det = nullptr, *inv = nullptr, *detf = nullptr, *invf = nullptr;
@@ -1261,6 +1308,8 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
   if (!h || !U) return AFR_EINVAL;
   const bool sst = h->prm.turb == AFR_TURB_SST;
   if (sst && (!k || !omega || !nu_t)) return fail(h, AFR_EINVAL, "SST step needs k, omega and nu_t");
+  int rc0 = pending_status(h, st);  // a problem of an earlier step taken without a norm
+  if (rc0) return rc0;
   int nl = 0;
   if (tm) tm->mark(st);
   int rc = compute_dt(h, U, sst ? nu_t : nullptr, h->dt, st);
@@ -1311,7 +1360,8 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
     *norm_out = std::sqrt(ss) / std::sqrt((double)h->N * h->S * h->nv);
     return check_status(h, st);
   }
-  return AFR_OK;
+  e = queue_status_copy(h, st);
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "status copy");
 }
 
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
@@ -1458,6 +1508,35 @@ int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int3
     out[i] = cnt > 0 ? std::sqrt(sums[i]) / std::sqrt(cnt) : 0.0;
   }
   return AFR_OK;
+}
+
+int afr_status(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t* seg_status, int32_t clear,
+               void* stream) {
+  if (!h || nseg < 0 || (nseg > 0 && (!cell_ptr || !seg_status))) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (capturing(st)) return fail(h, AFR_EINVAL, "afr_status synchronises: not inside a stream capture");
+  unsigned s = 0;
+  cudaError_t e = cudaMemcpyAsync(&s, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "status read");
+  if (nseg > 0) {
+    // a segment whose stage-0 norm partials of the last step are not all
+    // finite holds a non-finite value; partials are sums of squares, so their
+    // per-segment sum is finite exactly when every partial is
+    std::vector<double> sums(nseg);
+    int rc = afr_segment_norms(h, nseg, cell_ptr, 0, sums.data(), stream);
+    if (rc) return rc;
+    for (int i = 0; i < nseg; ++i) seg_status[i] = std::isfinite(sums[i]) ? AFR_OK : AFR_ENONFINITE;
+  }
+  const int code = status_code(h, s);
+  if (clear) {
+    e = cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(h, e, "status clear");
+    *h->status_host = 0;
+  }
+  h->status_pending = false;
+  return code;
 }
 
 int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* ms_out, int n_ms,

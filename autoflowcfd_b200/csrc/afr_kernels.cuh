@@ -648,6 +648,8 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     double acc_rho = 0.0;
     for (int s = 0; s < S; ++s) acc_rho += part[CPB * S + tid * S + s];
     a.norm_rho_part[e0 + tid] = acc_rho;
+    // a non-finite dU/dt anywhere in the cell makes its partial non-finite
+    if (!isfinite(acc) && a.status) atomicOr(a.status, (unsigned)DS_NONFINITE);
   }
 }
 

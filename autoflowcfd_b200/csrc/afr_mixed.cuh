@@ -1092,6 +1092,8 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
     double acc_rho = 0.0;
     for (int s = 0; s < S; ++s) acc_rho += part[CPB * S + tid * S + s];
     a.norm_rho_part[e0 + tid] = acc_rho;
+    // a non-finite dU/dt anywhere in the cell makes its partial non-finite
+    if (!isfinite(acc) && a.status) atomicOr(a.status, (unsigned)DS_NONFINITE);
   }
 }
 

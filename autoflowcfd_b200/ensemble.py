@@ -276,6 +276,24 @@ class B200Ensemble:
             res[g.members] = out
         return res
 
+    def status(self, clear: bool = True) -> np.ndarray:
+        """Per-case device status after the last step, in draw order: 0 (AFR_OK)
+        or AFR_ENONFINITE for a case whose state stopped being finite.  Cases
+        share no cells, so a failed case leaves the others' results unchanged;
+        ``clear`` resets each group's sticky status word so the healthy cases
+        keep running.  Index or tensor-core errors of a group raise."""
+        from .solver import _stream
+
+        res = np.zeros(len(self.specs), np.int32)
+        for g in self.groups:
+            seg = np.zeros(len(g.members), np.int32)
+            rc = LIB.afr_status(g.solver._h, len(g.members), g.cell_ptr.ctypes.data_as(_lib._P_I64),
+                                seg.ctypes.data_as(_lib._P_I32), 1 if clear else 0, _stream())
+            if rc not in (_lib.AFR_OK, _lib.AFR_ENONFINITE):
+                check(rc, g.solver._h)
+            res[g.members] = seg
+        return res
+
     def state(self, i: int) -> torch.Tensor:
         """Device view of case i's conserved state (n_cells, n_sps, 5)."""
         for g in self.groups:

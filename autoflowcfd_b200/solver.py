@@ -177,7 +177,12 @@ class B200FRSolver:
     def step(self, dt: float = 1e-3, want_norm: bool = True) -> float:
         """FRSolver.step / GPUFRSolver.step: one SSP-RK3 step with local time
         stepping (the ``dt`` argument is ignored, as in the reference's
-        steady SSP-RK mode, core/fr_solver/step.py:47-58)."""
+        steady SSP-RK mode, core/fr_solver/step.py:47-58).
+
+        With ``want_norm`` the call synchronises and raises AfrError when the
+        step produced a non-finite value.  Without it nothing synchronises; a
+        non-finite value is raised by the next step once the device has
+        finished this one (or by ``status()``)."""
         norm = ctypes.c_double(0.0)
         check(LIB.afr_step(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega), _dev_ptr(self.nu_t),
                            ctypes.byref(norm) if want_norm else None, _stream()), self._h)
@@ -185,6 +190,14 @@ class B200FRSolver:
             self.residual_history.append(norm.value)
             return norm.value
         return float("nan")
+
+    def status(self, clear: bool = False) -> int:
+        """Device status after the queued work (synchronises): 0 when every
+        step so far stayed finite, else raises AfrError (AFR_ENONFINITE ...).
+        ``clear`` resets the sticky device status after the error is raised."""
+        rc = LIB.afr_status(self._h, 0, None, None, 1 if clear else 0, _stream())
+        check(rc, self._h)
+        return rc
 
     def density_residual(self) -> float:
         """RMS of the density column of dU/dt at the last step (FP64), the

@@ -13,7 +13,8 @@ stages).  metric = DOF-updates/s = n_cells * 27 SPs * 5 variables * 3 stages
 per step / time.  ``value`` is the mixed-precision form (BF16 hi+lo split
 tensor-core contractions, FP32 fluxes, FP64 state) timed with device-resident
 inputs; the plain FP64 form runs in the same process from the same start
-state (``plain_fp64``), and ``accuracy`` compares the two final states and Cd.
+state (``plain_fp64``), and ``accuracy`` compares the two forms per field over
+steps 1-6 (before the SST growth) and Cd.
 ``e2e`` times the mixed step through the C-ABI with the state in pinned host
 memory, copied in and out every step.  The C2 state diverges after about 13
 steps under the reference's SST closure (in both forms, as in the reference's
@@ -64,11 +65,14 @@ def plane_cfg():
     return cfg
 
 
-def make_case(spec):
+def make_case(spec, colorer=None):
+    """Tables of the C2 generator's box; ``colorer`` replaces the library's
+    face coloring (the CPU arm passes the oracle's, so it loads no CUDA code)."""
     from autoflowcfd_b200 import boxgeom, boxmesh
 
     box = boxmesh.prism_box(*spec["shape"], spec["lengths"], jitter=spec["jitter"], seed=spec["seed"])
-    case = boxgeom.build_case(box, spec["order"], plane_cfg(), wall_distance=True, want_sps_coords=True)
+    case = boxgeom.build_case(box, spec["order"], plane_cfg(), wall_distance=True, want_sps_coords=True,
+                              colorer=colorer)
     return case
 
 
@@ -97,8 +101,8 @@ def initial_state(case, spec):
 
 
 # DRAM bytes per cell and launch of the mixed stage kernels, measured with ncu
-# on the 76,800-prism P2 SST case (profiles/mixed_stage_kernels_p2_sst_prism_76800.md);
-# a full-size launch moves these times the number of cells.
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 76,800-prism P2 SST
+# case; a full-size launch moves these times the number of cells.
 MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 8383.0, "k_mx_face": 7075.0, "k_mx_vol": 9912.0, "k_mx_update": 6126.0}
 
 
@@ -179,18 +183,34 @@ def clocks_summary(path, dev_index):
             "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(spec=SAMPLE, max_seconds=25.0):
-    """The reference algorithm on the host cores (the numpy oracle port), on a
-    bounded sample box of the same generator; DOF-updates/s."""
+def _blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        return max((int(i.get("num_threads", 1)) for i in threadpool_info() if i.get("user_api") == "blas"),
+                   default=1)
+    except Exception:
+        return None
+
+
+def _port_solver(spec):
+    """The numpy restatement of the reference's step (the oracle) on a sample
+    box of the C2 generator, with the oracle's own face coloring."""
     from oracle import fr_oracle as O
 
-    case = make_case(spec)
+    case = make_case(spec, colorer=O.greedy_face_coloring)
     U, k, om, nut, mu = initial_state(case, spec)
     tab = case.pop("src_mat_table")
     for key in ("nb_src0_mat", "nb_src1_mat", "ow_src0_mat", "ow_src1_mat"):
         case[key] = tab[case.pop(key + "_index")]
     m = O.Mesh.from_case(case)
-    s = O.Solver(m, U, mu, O.TurbState(k, om, nut), case["wall_distance"])
+    return O.Solver(m, U, mu, O.TurbState(k, om, nut), case["wall_distance"]), U.shape[:2]
+
+
+def cpu_baseline(spec=SAMPLE, max_seconds=25.0):
+    """The reference algorithm on the host cores (the numpy oracle port), on a
+    bounded sample box of the same generator; DOF-updates/s."""
+    s, (N, S) = _port_solver(spec)
     s.step()  # warm-up
     t0 = time.perf_counter()
     n = 0
@@ -200,40 +220,53 @@ def cpu_baseline(spec=SAMPLE, max_seconds=25.0):
         if time.perf_counter() - t0 > max_seconds / 2 or n >= 20:
             break
     dt = time.perf_counter() - t0
-    N, S = U.shape[:2]
-    return {"value": N * S * 5 * 3 * n / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+    return {"value": N * S * 5 * 3 * n / dt, "unit": UNIT, "cores": os.cpu_count(), "threads": _blas_threads(),
+            "kind": "port",
             "sample": f"{N} prisms P2 SST ({spec['shape'][0]}x{spec['shape'][1]}x{spec['shape'][2]} hex), "
-                      f"{n} steps, numpy oracle (BLAS threads = host cores)"}
+                      f"{n} steps, numpy restatement of the reference's FRSolver.step (the reference itself is "
+                      f"Python + Numba and is not installed where the GPU runs)"}
+
+
+def _repo_libraries_loaded():
+    """Shared objects of this repository mapped into the process."""
+    try:
+        maps = open("/proc/self/maps").read().splitlines()
+    except OSError:
+        return []
+    roots = (HERE, os.path.realpath(HERE))
+    paths = {ln.split()[-1] for ln in maps if len(ln.split()) >= 6}
+    return sorted(p for p in paths if ".so" in p and (p.startswith(roots) or "libafr_b200" in p))
 
 
 def run_reference(args, rank, world):
-    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "C2 P2 RANS-SST prisms, bounded sample of the same generator", "form": "CPU"}}
+    """CPU arm: the reference's algorithm (numpy restatement) on the host cores,
+    rank 0 only, on a bounded sample of the C2 generator; it loads none of this
+    repository's CUDA code (asserted)."""
     if rank != 0:
         return
     sample = SAMPLE
-    from oracle import fr_oracle as O
-
-    case = make_case(sample)
-    U, k, om, nut, mu = initial_state(case, sample)
-    tab = case.pop("src_mat_table")
-    for key in ("nb_src0_mat", "nb_src1_mat", "ow_src0_mat", "ow_src1_mat"):
-        case[key] = tab[case.pop(key + "_index")]
-    m = O.Mesh.from_case(case)
-    s = O.Solver(m, U, mu, O.TurbState(k, om, nut), case["wall_distance"])
+    s, (N, S) = _port_solver(sample)
     for _ in range(max(args.warmup, 1)):
         s.step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         s.step()
     dt = time.perf_counter() - t0
-    N, S = U.shape[:2]
+    loaded = _repo_libraries_loaded()
+    assert not loaded, f"the CPU arm loaded repository libraries: {loaded}"
     v = N * S * 5 * 3 * args.steps / dt
-    line.update(value=v, ms_per_step=1e3 * dt / args.steps,
-                cpu_baseline={"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                              "sample": f"{N} prisms P2 SST, {args.steps} steps, numpy oracle"},
-                e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "C2 P2 RANS-SST prisms, bounded sample of the same generator "
+                                   f"({sample['shape'][0]}x{sample['shape'][1]}x{sample['shape'][2]} hex -> {N} prisms)",
+                       "form": "CPU"},
+            "value": v, "ms_per_step": 1e3 * dt / args.steps,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "threads": _blas_threads(),
+                             "kind": "port",
+                             "sample": f"{N} prisms P2 SST, {args.steps} steps, numpy restatement of the "
+                                       "reference's FRSolver.step"},
+            "native_so_loaded": loaded,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -243,6 +276,12 @@ def run_reference(args, rank, world):
 # algorithm, so the timed steps run in segments that each restart from the
 # seeded start state; the restarts are outside the timed region.
 SEGMENT = 8
+# steps after which the two forms' fields are compared (the reference's SST
+# closure starts the growth of k at step 7 on this start state)
+WINDOW = (1, 2, 3, 4, 5, 6)
+# relative size of the seeded perturbation of the start state for the FP64
+# form's own sensitivity over the window (the accuracy block's baseline)
+PERTURB = 1e-9
 
 
 def max_over_ranks(times_ms, dist=None, device="cpu"):
@@ -319,7 +358,7 @@ def e2e_pipelined(s, starts, steps, stream, barrier):
     return {"e2e_ms": e0.elapsed_time(e1) / n, "h2d": h2d_bytes, "d2h": h2d_bytes}
 
 
-def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
+def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path, perturb=0.0):
     """Time one solver's steps (device-resident, restarted from the seeded
     state every SEGMENT steps), one breakdown step, and optionally the e2e
     loop; returns timings, breakdown and the fields after SEGMENT steps."""
@@ -358,12 +397,27 @@ def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
     if sampler:
         sampler.terminate()
     out = {"ms": ms, "finite": finite}
-    # fields after SEGMENT steps from the start state, for the cross-form comparison
+    # fields (device copies, ~2.2 GB each at full size) after the steps of the
+    # accuracy window, from the start state; the window ends before the SST
+    # growth of this start state (step 7)
     restart()
-    for _ in range(SEGMENT):
+    out["window"] = {}
+    for it in range(1, max(WINDOW) + 1):
         s.step(want_norm=False)
-    out["final"] = [t.clone() for t in fields]
+        if it in WINDOW:
+            out["window"][it] = [t.clone() for t in (s.U, s.k, s.omega)]
     out["cd"] = s.compute_aerodynamic_coefficients(1.0)
+    if perturb:
+        # the same window from a start state perturbed by `perturb` (relative,
+        # seeded): how far this workload itself carries a small difference
+        g = torch.Generator(device=s.U.device).manual_seed(7)
+        restart()
+        s.U.mul_(1.0 + perturb * torch.randn(s.U.shape, generator=g, device=s.U.device, dtype=s.U.dtype))
+        out["window_perturbed"] = {}
+        for it in range(1, max(WINDOW) + 1):
+            s.step(want_norm=False)
+            if it in WINDOW:
+                out["window_perturbed"][it] = [t.clone() for t in (s.U, s.k, s.omega)]
     restart()
     out["breakdown"] = profiling.step_breakdown(s)
     if want_e2e:
@@ -371,13 +425,20 @@ def run_form(s, steps, warmup, stream, barrier, want_e2e, clk_path):
     return out
 
 
-def field_errors(a, b):
-    """Relative errors of field a against reference b (global and per variable)."""
-    d = (a - b).double()
-    b = b.double()
-    out = {"l2_rel": float(d.norm() / b.norm()), "max_rel": float(d.abs().max() / b.abs().max())}
-    if a.dim() == 3:
-        out["l2_rel_per_var"] = [float(d[..., v].norm() / b[..., v].norm()) for v in range(5)]
+def per_field_errors(U, k, w, U_ref, k_ref, w_ref):
+    """Relative L2 and max error per field of one state against a reference:
+    rho, rho u, rho v, rho w, E (each momentum component relative to the
+    momentum vector's size) and k, omega."""
+    out = {}
+    mom = U_ref[..., 1:4]
+    for v, name in enumerate(("rho", "rho_u", "rho_v", "rho_w", "E")):
+        d = (U[..., v] - U_ref[..., v]).double()
+        ref = mom if 1 <= v <= 3 else U_ref[..., v]
+        out[name] = {"l2_rel": float(d.norm() / ref.double().norm()),
+                     "max_rel": float(d.abs().max() / ref.double().abs().max())}
+    for name, a, b in (("k", k, k_ref), ("omega", w, w_ref)):
+        d = (a - b).double()
+        out[name] = {"l2_rel": float(d.norm() / b.double().norm()), "max_rel": float(d.abs().max() / b.double().abs().max())}
     return out
 
 
@@ -532,8 +593,9 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    clk_path = os.path.join(HERE, "gpurun_out", f"clocks_rank{rank}.csv")
-    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    import tempfile
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"afr_bench_clocks_rank{rank}_{os.getpid()}.csv")
     forms = {"both": ["mixed", "fp64"], "mixed": ["mixed"], "fp64": ["fp64"]}[args.form]
     res = {}
     for i, form in enumerate(forms):
@@ -544,7 +606,7 @@ def main():
         if form == "mixed":
             s.autotune()  # launch shapes only; results are the same
         N, S = s.n_cells, s.n_sps
-        r = run_form(s, args.steps, args.warmup, stream, barrier, want_e2e=(i == 0),
+        r = run_form(s, args.steps, args.warmup, stream, barrier, want_e2e=(i == 0), perturb=PERTURB if form == "fp64" else 0.0,
                      clk_path=clk_path if (rank == 0 and i == 0) else None)
         r["device_bytes"] = s.device_bytes()
         if form == "mixed":
@@ -615,12 +677,22 @@ def main():
                               "speedup_of_mixed": float(ts[3]) / ms}
         mx = res["mixed"]
         cd64, cdmx = f64["cd"]["Cd"], mx["cd"]["Cd"]
+        per_step = {str(it): per_field_errors(*mx["window"][it], *f64["window"][it]) for it in WINDOW}
+        fields = list(per_step[str(WINDOW[-1])])
+        worst = {f: {m: max(per_step[str(it)][f][m] for it in WINDOW) for m in ("l2_rel", "max_rel")} for f in fields}
+        sens = {str(it): per_field_errors(*f64["window_perturbed"][it], *f64["window"][it]) for it in WINDOW}
         line["accuracy"] = {
-            "against": f"plain FP64 form, same start state, after {SEGMENT} steps",
-            "U": field_errors(mx["final"][0], f64["final"][0]),
-            "k": field_errors(mx["final"][1], f64["final"][1]),
-            "omega": field_errors(mx["final"][2], f64["final"][2]),
-            "Cd_fp64": cd64, "Cd_mixed": cdmx, "Cd_rel_err": abs(cdmx - cd64) / max(abs(cd64), 1e-300)}
+            "against": f"plain FP64 form, same start state, steps {list(WINDOW)} (before the SST growth)",
+            "per_field_worst_over_window": worst,
+            "per_step_l2": {it: {f: v["l2_rel"] for f, v in e.items()} for it, e in per_step.items()},
+            "per_step_max": {it: {f: v["max_rel"] for f, v in e.items()} for it, e in per_step.items()},
+            "fp64_sensitivity": {
+                "what": f"plain FP64 form from the start state times (1 + {PERTURB:g} N(0,1)) against the unperturbed run",
+                "per_step_l2": {it: {f: v["l2_rel"] for f, v in e.items()} for it, e in sens.items()},
+                "per_step_max": {it: {f: v["max_rel"] for f, v in e.items()} for it, e in sens.items()}},
+            "field_l2_target": 1e-6, "fields_over_target": [f for f in fields if worst[f]["l2_rel"] > 1e-6],
+            "Cd_fp64": cd64, "Cd_mixed": cdmx, "Cd_rel_err": abs(cdmx - cd64) / max(abs(cd64), 1e-300),
+            "Cd_after_steps": WINDOW[-1]}
     clk = clocks_summary(clk_path, local) if rank == 0 else None
     if clk:
         line["clocks"] = clk

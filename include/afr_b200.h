@@ -29,9 +29,11 @@
  * reference's own layouts: U is (n_cells, n_sps, n_vars) float64, fields are
  * (n_cells, n_sps) float64).  The library never frees caller memory.  Calls
  * on one handle are not thread safe.  `stream` is a cudaStream_t (0 = the
- * legacy default stream).  Kernels never trap: device-side problems are
- * reported through a status word read back by the call (AFR_ENONFINITE,
- * AFR_EINDEX).
+ * legacy default stream).  afr_create range-checks every table index
+ * (AFR_EINDEX) before any kernel runs.  Kernels never trap: non-finite values
+ * and tensor-core wait time-outs are reported through a device status word
+ * (AFR_ENONFINITE, AFR_ECUDA) that the calls read back (see afr_step and
+ * afr_status).
  */
 #ifndef AFR_B200_H
 #define AFR_B200_H
@@ -168,9 +170,28 @@ int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, doubl
                    double* nu_t, double* diag, void* stream);
 
 /* One SSP-RK3 step in place on U (and k, omega, nu_t with SST; pass NULL
- * otherwise).  *norm_out (host) receives the RMS of dU/dt at stage 0. */
+ * otherwise).  *norm_out (host) receives the RMS of dU/dt at stage 0; the call
+ * then synchronises the stream and returns the device status (AFR_ENONFINITE
+ * when any cell's dU/dt at stage 0 is not finite).  With norm_out == NULL the
+ * call does not synchronise: it queues a copy of the status word to pinned
+ * host memory, and the next afr_step on the handle returns the problem once
+ * that copy has completed (inside a stream capture the copy is part of the
+ * graph and afr_status reads the word).  The device status is sticky until
+ * afr_status clears it. */
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out,
              void* stream);
+
+/* Device status of the handle after the work queued on stream (synchronises;
+ * not inside a stream capture): AFR_OK, AFR_ENONFINITE, AFR_EINDEX or AFR_ECUDA
+ * (a tensor-core wait ran out).  With nseg > 0, seg_status[i] receives the
+ * status of cells [cell_ptr[i], cell_ptr[i+1]) -- AFR_ENONFINITE when any of
+ * their stage-0 dU/dt values of the last step is not finite -- so that
+ * independent cases concatenated into one handle fail one by one.  clear = 1
+ * resets the device status afterwards.  Replaces the per-case status of the
+ * batched driver (the reference has one case per solver and raises Python
+ * exceptions, core/fr_solver/step.py:217-221). */
+int afr_status(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t* seg_status, int32_t clear,
+               void* stream);
 
 /* afr_step with a CUDA event after every launch group; ms_out[i] receives the
  * device time of group i: local dt, [SST point, SST face, SST update],

@@ -310,6 +310,30 @@ def ghost_states(m: Mesh, Q, faces):
     return Qo, G
 
 
+def greedy_face_coloring(owner, neighbor, is_boundary, n_cells):
+    """greedy_face_coloring, core/utils/face_coloring.py:124-176: faces in order,
+    each takes the smallest color no earlier face sharing one of its cells
+    (the owner, and the neighbour of an interior face) already has."""
+    owner = np.asarray(owner, np.int64)
+    nb = np.where(np.asarray(is_boundary).astype(bool), -1, np.asarray(neighbor, np.int64))
+    cell_faces = [[] for _ in range(int(n_cells))]
+    for f in range(len(owner)):
+        cell_faces[owner[f]].append(f)
+        if nb[f] >= 0:
+            cell_faces[nb[f]].append(f)
+    colors = np.full(len(owner), -1, np.int32)
+    for f in range(len(owner)):
+        used = set()
+        for c in (owner[f], nb[f]):
+            if c >= 0:
+                used.update(int(colors[g]) for g in cell_faces[c] if g != f and colors[g] >= 0)
+        k = 0
+        while k in used:
+            k += 1
+        colors[f] = k
+    return colors
+
+
 def _color_faces(m: Mesh):
     col = m.c["colors"]
     return [np.flatnonzero(col == c) for c in range(int(col.max()) + 1)]

@@ -6,6 +6,9 @@ import pytest
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if REPO not in sys.path:
     sys.path.insert(0, REPO)
+GOLDEN_DIR = os.path.join(REPO, "tests", "golden")
+if GOLDEN_DIR not in sys.path:
+    sys.path.insert(0, GOLDEN_DIR)  # flows.py: start states shared with the fixture generator
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
 
@@ -18,7 +21,9 @@ def golden_path(name):
     return os.path.join(GOLDEN, name + ".npz")
 
 
-CASES = ["tet_p1_vortex", "prism_p2_sst", "prism_p1_ns", "tet_p3_tgv"]
+CASES = ["tet_p1_vortex", "prism_p2_sst", "prism_p1_ns", "tet_p3_tgv", "prism_p1_floors", "tet_p1_align"]
+# cases with a wall force integral in their fixture
+CD_CASES = ["prism_p2_sst", "prism_p1_ns", "prism_p1_floors"]
 
 
 def case_tol(name):

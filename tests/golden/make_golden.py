@@ -15,29 +15,42 @@ the reference's own outputs:
   (``core/fr_solver/step.py:15-221``) and their residual norms;
 * the wall force coefficients (``postprocess/fr_coefficients.py:27-152``).
 
+Besides these single-evaluation cases it writes *trajectory* fixtures:
+per-step summaries (residual norms, per-variable sums / L2 / extrema, k and
+nu_t maxima) and sampled states of longer runs of the reference's
+``FRSolver.step``, on meshes the tests regenerate bit-identically with
+``autoflowcfd_b200.boxgeom`` (so the fixtures stay small).
+
 The reference cannot be imported where the tests run on a GPU, so the outputs
 are committed as ``tests/golden/*.npz``.  Re-run with
-``NUMBA_CACHE_DIR=/tmp/nc python tests/golden/make_golden.py``.
+
+    AFR_REFERENCE=<reference checkout> NUMBA_CACHE_DIR=/tmp/nc \
+        python tests/golden/make_golden.py [case ...]
+
+(the reference checkout defaults to /root/reference).
 """
 
 import copy
 import os
 import sys
+import time
 import types
 from types import SimpleNamespace
 
 import numpy as np
 
-REF = "/root/reference"
+REF = os.environ.get("AFR_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
+sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.join(REF, "src"))
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/afr_numba_cache")
 
 from autoflowcfd_b200 import boxmesh  # noqa: E402
-
-GAMMA = 1.4
+from flows import (GAMMA, FLOOR_CELLS, c1_vortex, c3_tgv, channel_state, conserved,  # noqa: E402,F401
+                   plant_floor_states, tgv_state, vortex_state)
+from flows import P as flows_P, RHO as flows_RHO  # noqa: E402
 BC_CODES = {"WALL": 0, "FARFIELD": 1, "INLET": 2, "OUTLET": 3, "SYMMETRY": 4}
 
 
@@ -179,52 +192,15 @@ def op_tables(ops):
     )
 
 
-def conserved(rho, u, v, w, p):
-    E = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
-    return np.stack([rho, rho * u, rho * v, rho * w, E], axis=-1)
-
-
-def vortex_state(x, y, Lx, Ly, rc, rho_inf, p_inf, u_inf, beta=5.0):
-    """Isentropic vortex (``tests/validation/_isentropic_vortex.py:42-71``),
-    centre at the box centre, core radius rc."""
-    a_inf = np.sqrt(GAMMA * p_inf / rho_inf)
-    dx = x - 0.5 * Lx
-    dy = y - 0.5 * Ly
-    r2 = (dx / rc) ** 2 + (dy / rc) ** 2
-    swirl = (beta * a_inf / (2 * np.pi)) * np.exp(0.5 * (1 - r2))
-    theta = 1 - (GAMMA - 1) * beta**2 / (8 * GAMMA * np.pi**2) * np.exp(1 - r2)
-    rho = rho_inf * theta ** (1 / (GAMMA - 1))
-    p = p_inf * theta ** (GAMMA / (GAMMA - 1))
-    return conserved(rho, u_inf - swirl * dy / rc, swirl * dx / rc, np.zeros_like(x), p)
-
-
-def tgv_state(x, y, z, L, u0, rho0, p0):
-    """Taylor-Green vortex initial field (``tests/validation/test_tgv.py:96-112``)."""
-    k = 2 * np.pi / L
-    u = u0 * np.sin(k * x) * np.cos(k * y) * np.cos(k * z)
-    v = -u0 * np.cos(k * x) * np.sin(k * y) * np.cos(k * z)
-    w = np.zeros_like(u)
-    p = p0 + rho0 * u0**2 / 16 * (np.cos(2 * k * x) + np.cos(2 * k * y)) * (np.cos(2 * k * z) + 2)
-    rho = p / p0 * rho0
-    return conserved(rho, u, v, w, p)
-
-
-def channel_state(x, y, z, L, rho_inf, u_inf, p_inf, seed):
-    """Freestream with a smooth, seeded multi-mode perturbation (a few percent)."""
-    rng = np.random.default_rng(seed)
-    ph = rng.uniform(0, 2 * np.pi, size=8)
-    Lx, Ly, Lz = L
-    s = lambda i, a, b, c: np.sin(2 * np.pi * (a * x / Lx + b * y / Ly + c * z / Lz) + ph[i])  # noqa: E731
-    rho = rho_inf * (1 + 0.02 * s(0, 1, 1, 0) + 0.01 * s(1, 0, 2, 1))
-    u = u_inf * (1 + 0.05 * s(2, 2, 0, 1)) * np.tanh(6 * z / Lz + 0.3)
-    v = 0.04 * u_inf * s(3, 1, 1, 1)
-    w = 0.03 * u_inf * s(4, 0, 1, 2)
-    p = p_inf * (1 + 0.002 * s(5, 1, 0, 1))
-    return conserved(rho, u, v, w, p)
-
-
 def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_only=False,
-              global_dt_factor=None, n_steps=2, turb_init=None):
+              global_dt_factor=None, n_steps=2, turb_init=None, plant=None, tweak_flat=None):
+    """Run the reference on one small case and store its inputs and outputs.
+
+    ``plant(U) -> U`` edits the full start state (all n_vars columns) after
+    the turbulence columns are set; ``tweak_flat(flat)`` edits the reference's
+    cached ``FlatFaceGeometry`` in place before anything is evaluated, so every
+    consumer of the face tables (residual kernels, transport, the stored
+    tables) sees the same arrays."""
     import numba
     from autoflowcfd.core.fr_solver import FRSolver
     from autoflowcfd.core.time_integration import TimeIntegrationScheme
@@ -243,6 +219,10 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
     solver.order_continuation_enabled = False
     if not box.periodic:
         solver.boundary_ghost_provider = plane_provider(mesh, box, plane_cfg)
+    if tweak_flat is not None:
+        from autoflowcfd.core.fr_operators.face_kernels import get_flat_face_geometry
+
+        tweak_flat(get_flat_face_geometry(mesh, solver.ops))
     N, S = mesh.n_cells, mesh.n_sps_per_cell
     n_vars = solver.state.n_vars
     xyz = mesh.sps_coords.reshape(N, S, 3)
@@ -288,6 +268,8 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
         U[:, :, 5] = rho * k0
         U[:, :, 6] = rho * w0
         out["k0"], out["omega0"], out["nu_t0"] = k0, w0, nut0
+    if plant is not None:
+        U = plant(U)
     out["U0"] = U.copy()
 
     orig_dt = solver._compute_local_time_step
@@ -348,6 +330,23 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
         solver._compute_local_time_step = lambda: np.full((N, S), global_dt_factor * float(np.min(orig_dt())))
     if inviscid_only:
         solver.compute_viscous_residual = lambda: np.zeros_like(solver.state.U)
+    # count the points each clamp of enforce_positivity acts on during the steps
+    import autoflowcfd.core.time_integration.base as tib
+
+    trips = np.zeros(5, np.int64)
+    real_pos = tib.enforce_positivity
+
+    def positivity_spy(Uf, p_floor=1.0):
+        rho = np.maximum(Uf[:, 0], 1e-6)
+        vel = Uf[:, 1:4] / rho[:, None]
+        vm = np.sqrt(np.sum(vel**2, axis=1))
+        vel = np.where((vm > 1e4)[:, None], vel * (1e4 / np.maximum(vm, 1e-300))[:, None], vel)
+        pp = (GAMMA - 1.0) * (Uf[:, 4] - 0.5 * rho * np.sum(vel**2, axis=1))
+        trips[:] += [np.sum(Uf[:, 0] < 1e-6), np.sum(vm > 1e4), np.sum(pp < p_floor),
+                     np.sum(Uf[:, 5] < 0.0) if Uf.shape[1] > 5 else 0, np.sum(Uf[:, 6] < 1e-8) if Uf.shape[1] > 6 else 0]
+        return real_pos(Uf, p_floor)
+
+    tib.enforce_positivity = positivity_spy
     norms = []
     for s in range(n_steps):
         norms.append(solver.step(1e-3))
@@ -357,13 +356,112 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
             out[f"w_step{s + 1}"] = solver.turb_model.omega_field.copy()
             out[f"nut_step{s + 1}"] = solver.turb_model.nu_t.copy()
     out["norms"] = np.array(norms)
+    tib.enforce_positivity = real_pos
+    out["positivity_trips"] = trips  # points clamped: rho, |u|, p, rho*k, rho*omega
 
     if not box.periodic and not inviscid_only:
         coef = compute_aerodynamic_coefficients_fr(solver, reference_area=1.0)
         out["cd_cl"] = np.array([coef.Cd, coef.Cl, coef.Cs], float)
+    if tweak_flat is not None:
+        from autoflowcfd.core.fr_operators.face_kernels import get_flat_face_geometry
+
+        # the tweaked tables stayed the ones in use for the whole run
+        assert np.array_equal(get_flat_face_geometry(mesh, solver.ops).true_normal, out["true_normal"])
+    for k, v in out.items():
+        if isinstance(v, np.ndarray) and v.dtype.kind == "f":
+            assert np.all(np.isfinite(v)), f"{name}: non-finite reference output {k}"
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(f"{name}: N={N} S={S} faces={len(out['owner_cell'])} colors={out['colors'].max() + 1} "
           f"norms={norms}", flush=True)
+    return out
+
+
+def _summaries(U, k=None, nut=None):
+    """Per-variable sum, L2, max and min of a state (and k / nu_t maxima)."""
+    flat = U.reshape(-1, U.shape[-1])
+    out = dict(sum=flat.sum(0), l2=np.sqrt((flat * flat).sum(0)), max=flat.max(0), min=flat.min(0),
+               finite=np.int32(np.all(np.isfinite(U))))
+    if k is not None:
+        out.update(k_max=np.max(k), nut_max=np.max(nut), k_min=np.min(k))
+    return out
+
+
+def make_trajectory(name, box, order, turb, mu, free, plane_cfg, state_xyz, n_steps, *, inviscid_only=False,
+                    global_dt_factor=None, turb_xyz=None, sample_steps=(), stride=1, stop_nonfinite=True):
+    """Run the reference's FRSolver.step n_steps times from a start state and
+    store per-step summaries plus sampled states (every ``stride``-th cell).
+
+    ``state_xyz(xyz) -> U[..., :5]`` and ``turb_xyz(xyz) -> (k, omega, nu_t)``
+    are evaluated on the reference mesh's solution points, which the
+    box-mesh generator reproduces bit for bit, so a test rebuilds the same
+    start state from the same formulas."""
+    import numba
+    from autoflowcfd.core.fr_solver import FRSolver
+    from autoflowcfd.core.time_integration import TimeIntegrationScheme
+
+    numba.set_num_threads(min(8, os.cpu_count() or 1))
+    mesh_bc = None
+    if plane_cfg is not None:
+        mesh_bc = {n: ("WALL" if plane_cfg[n]["type"] == "WALL" and plane_cfg[n].get("is_no_slip", True)
+                       else "FARFIELD") for n in boxmesh.PLANE_NAMES}
+    mesh = ref_mesh(box, order, mesh_bc)
+    rho_inf, u_inf, p_inf = free
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name=turb, time_scheme=TimeIntegrationScheme.SSP_RK3,
+                      rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf, mu_molecular=mu,
+                      n_threads=min(8, os.cpu_count() or 1))
+    solver.order_continuation_enabled = False
+    if not box.periodic:
+        solver.boundary_ghost_provider = plane_provider(mesh, box, plane_cfg)
+    N, S = mesh.n_cells, mesh.n_sps_per_cell
+    xyz = mesh.sps_coords.reshape(N, S, 3)
+    U = np.zeros((N, S, solver.state.n_vars))
+    U[:, :, :5] = state_xyz(xyz)
+    out = dict(meta_name=np.array(name), order=np.int32(order), n_cells=np.int32(N), n_sps=np.int32(S),
+               turb=np.array(turb), mu=np.float64(mu), freestream=np.array(free, float),
+               inviscid_only=np.int32(inviscid_only), global_dt_factor=np.float64(global_dt_factor or 0.0),
+               box_kind=np.array(box.kind), box_shape=np.array(box.shape), box_lengths=np.array(box.lengths),
+               box_periodic=np.int32(box.periodic), stride=np.int32(stride))
+    if turb == "SST":
+        nodes = mesh._node_coords
+        solver.compute_wall_distance_field(nodes, np.flatnonzero(np.abs(nodes[:, 2]) < 1e-12))
+        k0, w0, nut0 = turb_xyz(xyz)
+        solver.turb_model.k_field = k0.copy()
+        solver.turb_model.omega_field = w0.copy()
+        solver.turb_model.nu_t = nut0.copy()
+        U[:, :, 5] = U[:, :, 0] * k0
+        U[:, :, 6] = U[:, :, 0] * w0
+    out["U0_sample"] = U[::stride].copy()
+    solver.state.U = U.copy()
+    solver.state._update_primitives()
+    if global_dt_factor:
+        orig_dt = solver._compute_local_time_step
+        solver._compute_local_time_step = lambda: np.full((N, S), global_dt_factor * float(np.min(orig_dt())))
+    if inviscid_only:
+        solver.compute_viscous_residual = lambda: np.zeros_like(solver.state.U)
+    rows = []
+    t0 = time.time()
+    for it in range(1, n_steps + 1):
+        with np.errstate(all="ignore"):
+            norm = solver.step(1e-3)
+        tm = solver.turb_model
+        row = _summaries(solver.state.U, None if tm is None else tm.k_field, None if tm is None else tm.nu_t)
+        row["norm"] = norm
+        rows.append(row)
+        if it in sample_steps:
+            out[f"U_s{it}"] = solver.state.U[::stride].copy()
+            if tm is not None:
+                out[f"k_s{it}"] = tm.k_field[::stride].copy()
+                out[f"w_s{it}"] = tm.omega_field[::stride].copy()
+                out[f"nut_s{it}"] = tm.nu_t[::stride].copy()
+        print(f"{name}: step {it} norm {norm:.6e} finite {row['finite']} "
+              + (f"k_max {row['k_max']:.4e} nut_max {row['nut_max']:.4e} " if tm is not None else "")
+              + f"({time.time() - t0:.0f} s)", flush=True)
+        if stop_nonfinite and not row["finite"]:
+            break
+    for key in rows[0]:
+        out["step_" + key] = np.array([r[key] for r in rows])
+    out["n_steps_run"] = np.int32(len(rows))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     return out
 
 
@@ -428,8 +526,101 @@ def main(which=None):
                   lambda x, y, z: tgv_state(x, y, z, L, u0, rho, p), inviscid_only=True, global_dt_factor=3.0,
                   n_steps=1)
 
+    def c_prism_p1_floors():
+        """Start states beyond every floor and clamp of the path (values far
+        from the thresholds): the AUSM+up rho >= 1e-6 / p >= 10 Pa floors
+        (core/fr_operators/kernels.py:41-44) and every clamp of
+        enforce_positivity (core/time_integration/positivity.py:13-45)."""
+        Ls = (2.0, 1.0, 1.0)
+        box = boxmesh.prism_box(4, 3, 2, Ls, jitter=0.1, seed=5)
+        rho, p = 1.225, 101325.0
+        u = 0.2 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e5
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        k_in = 1.5 * (0.01 * u) ** 2
+        w_in = rho * k_in / (10 * mu)
+
+        def turb_init(xyz):
+            N, S = xyz.shape[:2]
+            k = k_in * (1 + 0.2 * np.sin(2 * np.pi * xyz[..., 0] / Ls[0]))
+            w = w_in * (1 + 0.3 * np.cos(2 * np.pi * xyz[..., 1] / Ls[1]))
+            return k, w, k / w
+
+        make_case("prism_p1_floors", box, 1, "SST", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 17), turb_init=turb_init,
+                  plant=plant_floor_states)
+
+    def c_tet_p1_align():
+        """Face normals that disagree with the adjugate direction: on records
+        f % 7 == 3 every flux point's true normal is reversed (alignment -1),
+        on records f % 11 == 5 the even flux points' normals are turned by
+        90 degrees (alignment ~0); both take the reference's fallback to the
+        true normal (core/fr_residual/inviscid_kernel_colored.py:104-108 and
+        its neighbour-side twin at :186-190)."""
+        L = 1.0
+        box = boxmesh.tet_box(3, 3, 3, (L, L, L), jitter=0.0, periodic=True)
+        rho, p = 1.225, 101325.0
+        u = 0.5 * np.sqrt(GAMMA * p / rho)
+
+        def tweak(flat):
+            tn = flat.true_normal
+            F = tn.shape[0]
+            rev = np.arange(F) % 7 == 3
+            tn[rev] = -tn[rev]
+            rot = np.flatnonzero(np.arange(F) % 11 == 5)
+            for f in rot:
+                for i in range(0, tn.shape[1], 2):
+                    n = tn[f, i].copy()
+                    e = np.array([1.0, 0.0, 0.0]) if abs(n[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+                    t = np.cross(n, e)
+                    tn[f, i] = t / np.linalg.norm(t)
+
+        make_case("tet_p1_align", box, 1, "NONE", 1.8e-5, (rho, u, p), None,
+                  lambda x, y, z: vortex_state(x, y, L, L, 0.2 * L, rho, p, u),
+                  inviscid_only=True, global_dt_factor=3.0, tweak_flat=tweak)
+
+    def t_c1():
+        """The small configuration at full size: 16^3 hex -> 24,576 periodic
+        tets, P1, isentropic vortex, Euler, global dt 3 min(dt_local), 100 steps."""
+        box = boxmesh.tet_box(16, 16, 16, (1.0, 1.0, 1.0), jitter=0.0, periodic=True)
+        u = c1_vortex(np.zeros((1, 1, 3)))[1]
+        make_trajectory("traj_c1_vortex", box, 1, "NONE", 1.8e-5, (flows_RHO, u, flows_P), None,
+                        lambda xyz: c1_vortex(xyz)[0], 100, inviscid_only=True, global_dt_factor=3.0,
+                        sample_steps=(1, 100), stride=8)
+
+    def t_c2_sample():
+        """The C2 generator on its 8 x 6 x 6-hex sample (576 prisms, P2, SST,
+        the bench's start state), 20 steps: k and nu_t through the SST growth."""
+        import bench
+
+        spec = bench.SAMPLE
+        box = boxmesh.prism_box(*spec["shape"], spec["lengths"], jitter=spec["jitter"], seed=spec["seed"])
+        rho, u, p, mu, k0, w0 = bench.flow_conditions()
+
+        def state(xyz):
+            return bench.initial_state({"sps_coords": xyz}, spec)[0][..., :5]
+
+        def turb(xyz):
+            _, k, w, nut, _ = bench.initial_state({"sps_coords": xyz}, spec)
+            return k, w, nut
+
+        make_trajectory("traj_c2_sample", box, 2, "SST", mu, (rho, u, p), bench.plane_cfg(), state, 20,
+                        turb_xyz=turb, sample_steps=(1, 6, 12), stride=1)
+
+    def t_p3():
+        """The precision-stress configuration at the oracle's size: 8^3 hex ->
+        3,072 jittered periodic tets, P3, Taylor-Green at Mach 0.1, Euler,
+        global dt; run until the state is non-finite (at most 12 steps)."""
+        box = boxmesh.tet_box(8, 8, 8, (1.0, 1.0, 1.0), jitter=0.05, seed=7, periodic=True)
+        make_trajectory("traj_p3_tgv", box, 3, "NONE", 1.8e-5, (flows_RHO, 0.0, flows_P), None,
+                        lambda xyz: c3_tgv(xyz)[0], 12, inviscid_only=True, global_dt_factor=3.0,
+                        sample_steps=(1,), stride=16)
+
     cases = {"tet_p1_vortex": c_tet_p1, "prism_p2_sst": c_prism_p2_sst, "prism_p1_ns": c_prism_p1_ns,
-             "tet_p3_tgv": c_tet_p3}
+             "tet_p3_tgv": c_tet_p3, "prism_p1_floors": c_prism_p1_floors, "tet_p1_align": c_tet_p1_align,
+             "traj_c1_vortex": t_c1, "traj_c2_sample": t_c2_sample, "traj_p3_tgv": t_p3}
     for k, fn in cases.items():
         if which and k not in which:
             continue

@@ -1,8 +1,8 @@
 """Harvest the reference-space tables the box-mesh generator needs.
 
-Runs the reference (AutoFlowCFD, read from ``/root/reference``) once per
-(cell kind, order) on a 3x3x3-hex template box and stores, in
-``tmpl_<kind>_p<order>.npz`` next to this file:
+Runs the reference (AutoFlowCFD, a checkout named by ``AFR_REFERENCE``,
+default /root/reference) once per (cell kind, order) on a 3x3x3-hex template
+box and stores, in ``autoflowcfd_b200/data/tmpl_<kind>_p<order>.npz``:
 
 * the FR operators of ``generate_fr_operators`` (fr/operators.py:105-206) and
   the flattened-face extras (boundary extrapolation, g_left/g_right,
@@ -23,7 +23,8 @@ parametrise the same straight-sided patch from both sides).
 ``autoflowcfd_b200.boxgeom`` replays these records on boxes of any size and
 recomputes all geometry from the node coordinates.
 
-Run: ``NUMBA_CACHE_DIR=/tmp/nc python -m autoflowcfd_b200.data.make_tables``.
+This is the recipe for committed data, not part of the package.  Run:
+``AFR_REFERENCE=<checkout> NUMBA_CACHE_DIR=/tmp/nc python tests/golden/make_tables.py``.
 """
 
 import os
@@ -31,11 +32,12 @@ import sys
 
 import numpy as np
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+GOLDEN = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(GOLDEN))
+HERE = os.path.join(REPO, "autoflowcfd_b200", "data")  # where the templates are written
+REF = os.environ.get("AFR_REFERENCE", "/root/reference")
 sys.path.insert(0, REPO)
-sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+sys.path.insert(0, GOLDEN)
 sys.path.insert(0, os.path.join(REF, "src"))
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/afr_numba_cache")
 

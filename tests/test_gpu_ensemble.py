@@ -58,3 +58,53 @@ def test_graph_replay_and_autotune_keep_results():
         assert np.array_equal(tuned.state(i).cpu().numpy(), eager.state(i).cpu().numpy()), i
     eager.cleanup()
     tuned.cleanup()
+
+
+def test_nonfinite_case_is_isolated():
+    """A NaN injected on the host into one case's start state: that case alone
+    is reported non-finite (afr_status per case), every other case gets
+    bitwise its clean result, and the healthy cases keep running after the
+    status is cleared."""
+    cases = [E.build_case(s) for s in SPECS]
+    clean = E.B200Ensemble(SPECS, cases=cases)
+    bad = E.B200Ensemble(SPECS, cases=cases)
+    victim = 2
+    st = bad.state(victim)
+    st[st.shape[0] // 2, 3, 1] = float("nan")
+    for _ in range(2):
+        clean.step()
+        bad.step()
+    status = bad.status(clear=True)
+    assert status.tolist() == [4 if i == victim else 0 for i in range(len(SPECS))]  # AFR_ENONFINITE
+    assert clean.status().tolist() == [0] * len(SPECS)
+    for i in range(len(SPECS)):
+        if i != victim:
+            assert np.array_equal(bad.state(i).cpu().numpy(), clean.state(i).cpu().numpy()), i
+    norms = bad.norms()
+    assert not np.isfinite(norms[victim]) and np.all(np.isfinite(np.delete(norms, victim)))
+    clean.cleanup()
+    bad.cleanup()
+
+
+def test_step_without_norm_reports_nonfinite_at_the_next_step():
+    """afr_step with no norm does not synchronise; the status it leaves in
+    pinned host memory makes the next step raise once the device is done."""
+    from autoflowcfd_b200._lib import AFR_ENONFINITE, AfrError
+
+    spec = SPECS[1]
+    case = E.build_case(spec)
+    s = B200FRSolver(case, turb_model_name="NONE", mu_molecular=E.MU, rho_inf=E.RHO_INF, vel_inf=spec.velocity,
+                     p_inf=E.P_INF)
+    U = E.uniform_state(spec, int(case["n_cells"]), int(case["n_sps"]))
+    U[1, 2, 4] = np.inf
+    s.set_state_from_cpu(U)
+    s.step(want_norm=False)          # returns at once
+    torch.cuda.synchronize()
+    with pytest.raises(AfrError) as ei:
+        s.step(want_norm=False)
+    assert ei.value.status == AFR_ENONFINITE
+    with pytest.raises(AfrError):
+        s.status(clear=True)
+    s.set_state_from_cpu(E.uniform_state(spec, int(case["n_cells"]), int(case["n_sps"])))
+    assert np.isfinite(s.step())     # cleared status, finite state: healthy again
+    s.cleanup()

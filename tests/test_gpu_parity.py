@@ -143,3 +143,64 @@ def test_outlier_zeroing_matches_oracle(golden, name, var, amp):
     assert np.all(got[mask] == 0.0)
     assert rel(got, ref) < 1e-12
     s.cleanup()
+
+
+@pytest.mark.parametrize("name", ["prism_p1_floors", "tet_p1_align"])
+def test_edge_case_fixtures_per_field(golden, name):
+    """The fixtures whose start states and face normals reach the AUSM+up
+    floors, every positivity clamp and the alignment fallback: the plain form
+    matches the reference per field (each conserved variable and, with SST,
+    the carried rho*k / rho*omega columns and the k, omega, nu_t fields) at
+    1e-12, and the clamped values themselves exactly."""
+    from fields import per_field, scalar, worst
+
+    case = golden(name)
+    s = make_solver(case, global_dt_factor=0.0)
+    assert worst(per_field(s.compute_inviscid_residual(), case["R_inv"])) < 1e-12
+    assert worst(per_field(s.compute_viscous_residual(), case["R_visc"])) < 1e-12
+    s.cleanup()
+    s = make_solver(case)
+    for i in range(len(case["norms"])):
+        s.step()
+        U = s.U.cpu().numpy()
+        ref = case[f"U_step{i + 1}"]
+        assert worst(per_field(U, ref)) < 1e-12, i
+        if U.shape[-1] > 5:
+            assert np.array_equal(U[..., 5:] == 0.0, ref[..., 5:] == 0.0)  # rho*k >= 0 clamp
+            assert np.array_equal(U[..., 6] == 1e-8, ref[..., 6] == 1e-8)  # rho*omega >= 1e-8 clamp
+            assert scalar(U[..., 5], ref[..., 5])[1] < 1e-12 and scalar(U[..., 6], ref[..., 6])[1] < 1e-12
+            for a, key in ((s.k, "k"), (s.omega, "w"), (s.nu_t, "nut")):
+                assert scalar(a, case[f"{key}_step{i + 1}"])[1] < 1e-12, key
+    s.cleanup()
+
+
+@pytest.mark.parametrize("name", ["prism_p1_ns", "prism_p2_sst"])
+def test_gpufrsolver_signature_drop_in(golden, name):
+    """B200GPUFRSolver takes GPUFRSolver's constructor arguments (mesh, ops,
+    order, n_vars, device_id, ..., boundary_ghost_provider, turb_model) --
+    here reference-shaped stand-ins carrying the fixture's arrays -- and steps
+    like the reference (1e-12), with Cd/Cl."""
+    import refstandins
+    from autoflowcfd_b200.reference_io import B200GPUFRSolver
+
+    case = golden(name)
+    mesh, ops, flat = refstandins.mesh_ops_flat(case)
+    free = case["freestream"]
+    sst = str(case["turb"]) == "SST"
+    s = B200GPUFRSolver(mesh, ops, order=int(case["order"]), n_vars=7 if sst else 5, device_id=0,
+                        rho_inf=free[0], vel_inf=free[1], p_inf=free[2], mu_molecular=float(case["mu"]),
+                        boundary_ghost_provider=refstandins.provider(case), turb_model=str(case["turb"]),
+                        wall_distance=case["wall_distance"] if sst else None, flat=flat,
+                        cd_wall_face=case["cd_wall_face"])
+    s.set_state_from_cpu(case["U0"])
+    if sst:
+        s.set_turbulence(case["k0"], case["omega0"], case["nu_t0"])
+    for i in range(len(case["norms"])):
+        n = s.step()
+        assert rel(s.U, case[f"U_step{i + 1}"]) < 1e-12
+        assert abs(n - case["norms"][i]) <= 1e-12 * case["norms"][i]
+    c = s.compute_aerodynamic_coefficients(1.0)
+    assert np.allclose([c["Cd"], c["Cl"], c["Cs"]], case["cd_cl"], rtol=1e-10, atol=0)
+    out = s.solve(max_iter=2, tol=0.0)
+    assert out["iterations"] == 2 and len(out["residual_history"]) == len(case["norms"]) + 2
+    s.cleanup()

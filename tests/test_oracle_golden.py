@@ -8,7 +8,7 @@ import copy
 import numpy as np
 import pytest
 
-from conftest import CASES, case_tol, golden_path
+from conftest import CASES, CD_CASES, case_tol, golden_path
 from oracle import fr_oracle as O
 
 
@@ -57,7 +57,7 @@ def test_steps_match_reference(name):
             assert rel(s.turb.nut, case[f"nut_step{i + 1}"]) < 1e-12
 
 
-@pytest.mark.parametrize("name", ["prism_p2_sst", "prism_p1_ns"])
+@pytest.mark.parametrize("name", CD_CASES)
 def test_force_coefficients_match_reference(name):
     case, m, s = O.load_case(golden_path(name))
     for _ in range(len(case["norms"])):
@@ -71,3 +71,46 @@ def test_oracle_detects_planted_error():
     case, m, s = O.load_case(golden_path("prism_p1_ns"))
     m.c["g_left"] = m.c["g_left"] * (1 + 1e-9)
     assert rel(O.inviscid_residual(m, case["U0"]), case["R_inv"][..., :5]) > 1e-11
+
+
+def test_floor_and_clamp_branches_are_exercised(golden):
+    """The floors fixture was made from states beyond every clamp of the
+    reference's enforce_positivity (core/time_integration/positivity.py:13-45)
+    and the AUSM+up floors (core/fr_operators/kernels.py:41-44); the generator
+    counted the points each clamp acted on during the two steps."""
+    from flows import FLOOR_CELLS
+
+    g = golden("prism_p1_floors")
+    assert np.all(g["positivity_trips"] > 0), g["positivity_trips"]  # rho, |u|, p, rho*k, rho*omega
+    U0 = g["U0"]
+    vac = U0[FLOOR_CELLS["vacuum"]]
+    assert np.all(vac[:, 0] < 1e-6) and np.all(0.4 * vac[:, 4] < 10.0)  # below both AUSM floors
+    U1 = g["U_step1"]
+    assert np.all(U1[FLOOR_CELLS["neg_rho_k"], :, 5] == 0.0)
+    assert np.all(U1[FLOOR_CELLS["tiny_rho_w"], :, 6] == 1e-8)
+
+
+def test_alignment_fallback_is_exercised():
+    """In the alignment fixture some true normals point against (or across) the
+    adjugate direction, so the reference's alignment < 0.5 fallback
+    (core/fr_residual/inviscid_kernel_colored.py:104-108, neighbour side
+    :186-190) takes them on both sides of a record; the benign fixtures never
+    reach it."""
+
+    def fallback_points(name):
+        case, m, _ = O.load_case(golden_path(name))
+        adj = m.extras["adj"]
+        counts = []
+        for owner in (True, False):
+            isb = m.c["is_boundary"].astype(bool)
+            prim = m.c["owner_is_primary" if owner else "neighbor_is_primary"].astype(bool)
+            f = np.flatnonzero(prim if owner else prim & ~isb)
+            cell, ax, sd = O._side_geometry(m, f, owner)
+            arow = np.matmul(O.extrap_E(m, cell, ax, sd), adj[cell, :, ax, :])
+            d = arow / np.linalg.norm(arow, axis=-1, keepdims=True) * sd[:, None, None]
+            tn = m.c["true_normal"][f] * (1.0 if owner else -1.0)
+            counts.append(int(np.sum(np.sum(d * tn, axis=-1) < 0.5)))
+        return counts
+
+    assert min(fallback_points("tet_p1_align")) > 0
+    assert fallback_points("tet_p1_vortex") == [0, 0]
