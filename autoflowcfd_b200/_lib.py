@@ -56,6 +56,7 @@ class AfrParams(ctypes.Structure):
         ("n_vars", ctypes.c_int32), ("turb", ctypes.c_int32), ("inviscid_only", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("mu", ctypes.c_double), ("rho_inf", ctypes.c_double),
         ("vel_inf", ctypes.c_double), ("p_inf", ctypes.c_double), ("global_dt_factor", ctypes.c_double),
+        ("mixed_ignore_conditioning", ctypes.c_int32),
     ]
 
 
@@ -78,6 +79,7 @@ SIGNATURES = {
     "afr_step_profile": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     "afr_rms_norm_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "afr_residual_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "afr_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P_I64, _P_I32, ctypes.c_int32, ctypes.c_void_p]),
     "afr_autotune": (ctypes.c_int, [ctypes.c_void_p] * 3 + [_P_I32, ctypes.c_void_p]),
     "afr_launch_shape": (ctypes.c_int, [ctypes.c_void_p, _P_I32]),

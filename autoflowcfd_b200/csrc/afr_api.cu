@@ -762,7 +762,7 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
     l1 = std::max(l1, row_l1(m->c2f[t], Fn, S, S, 1));
     for (int mm = 0; mm < 3; ++mm) l1 = std::max(l1, row_l1(m->D_3d[t] + mm, S, S, 3 * S, 3));
     l1 = std::max(l1, row_l1(m->boundary_extrap + (size_t)t * 6 * P * S, 6 * P, S, S, 1));
-    if (l1 > MAX_ROW_L1)
+    if (l1 > MAX_ROW_L1 && !h->prm.mixed_ignore_conditioning)
       return fail(h, AFR_EUNSUPPORTED,
                   std::string("the mixed form needs operators with row l1 norms <= 1e6 (FP32 accumulation); the ") +
                       (t == 0 ? "prism" : "tet") + " operators of this order reach " + std::to_string(l1));
@@ -1508,6 +1508,21 @@ int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int3
     out[i] = cnt > 0 ? std::sqrt(sums[i]) / std::sqrt(cnt) : 0.0;
   }
   return AFR_OK;
+}
+
+int afr_residual_sums(afr_handle* h, double* out2, void* stream) {
+  if (!h || !out2) return AFR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned nb = (unsigned)(((size_t)h->N + RED_CHUNK - 1) / RED_CHUNK);
+  // the same fixed-order two-level sums as the step norm, into the handle's
+  // reduction scratch, then both results to the caller's device buffer
+  k_reduce_chunks<false><<<nb, RED_THREADS, 0, st>>>(h->norm_part, (size_t)h->N, h->red_part);
+  k_reduce_sum<<<1, 1024, 0, st>>>(h->red_part, nb, h->red + 2);
+  k_reduce_chunks<false><<<nb, RED_THREADS, 0, st>>>(h->norm_rho_part, (size_t)h->N, h->red_part);
+  k_reduce_sum<<<1, 1024, 0, st>>>(h->red_part, nb, h->red + 3);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out2, h->red + 2, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "residual sums");
 }
 
 int afr_status(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t* seg_status, int32_t clear,

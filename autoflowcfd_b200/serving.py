@@ -4,14 +4,20 @@ Requests (a box case to be solved to a residual drop) arrive over time.  On
 arrival a worker pool generates the request's mesh tables on the host while
 the GPU keeps running the admitted requests.  A request is admitted, first
 come first served, as soon as a slot is free and the free device memory
-(``cudaMemGetInfo``) covers its estimated footprint plus a reserve.  Each
+(``cudaMemGetInfo``) covers its estimated footprint plus a reserve; a request
+that cannot fit even on an idle device is rejected rather than tried.  Each
 admitted request keeps its state resident on the device and runs on its own
 CUDA stream as replays of a captured multi-step CUDA graph, so the work of all
-admitted requests overlaps on the GPU.  After every slice its density residual
-(the RMS of the density column of dU/dt, FP64) is read back; the request
-finishes when that residual has dropped by ``drop`` relative to its first step,
-at ``max_iter`` steps, or on a non-finite residual.  Its handle is then freed,
-which makes room for the next admissions.
+admitted requests overlaps on the GPU.  The graph of a slice ends by copying
+the slice's residual sums (``afr_residual_sums``: FP64, fixed order) into
+pinned host memory and the loop polls each request's completion event: a
+request whose slice is done is checked at once and, unless finished, its next
+slice is issued immediately -- no request waits for the others' slices.  A
+request finishes when its density residual (the RMS of the density column of
+dU/dt) has dropped by ``drop`` relative to its first step, at ``max_iter``
+steps, or on a non-finite residual.  Its handle is then freed, which makes
+room for the next admissions.  A request whose handle cannot be created (for
+example out of device memory) fails alone; the others keep running.
 
 Each request's arithmetic depends only on its own handle, so its result is the
 same alone and in the mix (bitwise: no cross-request reduction exists).
@@ -45,7 +51,7 @@ class SolveResult:
     admitted_s: float
     finished_s: float
     iterations: int
-    status: str                  # "converged", "max_iter" or "nonfinite"
+    status: str                  # "converged", "max_iter", "nonfinite", "rejected" or "error"
     residual_drop: float         # last / first density residual
     n_cells: int
     order: int
@@ -95,8 +101,21 @@ class _Active:
     graph: object
     admitted_s: float
     first: float
+    sums: object = None          # pinned host (2,) residual sums written by the slice graph
+    done: object = None          # event recorded after the last issued slice
     iters: int = 0
     n_cells: int = 0
+
+
+def admission(free_bytes: float, estimate: float, reserve_bytes: float, n_active: int, max_active: int) -> str:
+    """Admission decision for the queue head: "admit", "wait" (a slot or
+    memory frees up when a running request finishes) or "reject" (it would
+    not fit even on an idle device)."""
+    if n_active >= max_active:
+        return "wait"
+    if free_bytes - estimate >= reserve_bytes:
+        return "admit"
+    return "wait" if n_active > 0 else "reject"
 
 
 @dataclass
@@ -140,6 +159,16 @@ class ServingLoop:
         with torch.cuda.stream(stream):
             s = B200FRSolver(case, turb_model_name=self.turb, mu_molecular=E.MU, rho_inf=E.RHO_INF,
                              vel_inf=spec.velocity, p_inf=E.P_INF, precision=self.precision, device=self.device)
+        try:
+            return self._prepare(req, s, now, stream)
+        except Exception:
+            torch.cuda.synchronize(self.device)
+            s.cleanup()
+            raise
+
+    def _prepare(self, req: SolveRequest, s, now: float, stream) -> _Active:
+        spec = req.spec
+        with torch.cuda.stream(stream):
             N, S = s.n_cells, s.n_sps
             U = E.uniform_state(spec, N, S)
             if self.turb == "SST":
@@ -155,11 +184,30 @@ class ServingLoop:
             self.bytes_per_cell[spec.order] = 1.1 * (s.device_bytes() + s.U.numel() * 8) / N
             s.step(want_norm=False)              # iteration 1, eagerly
             first = s.density_residual()
+            dev = torch.zeros(2, dtype=torch.float64, device=self.device)
+            sums = torch.zeros(2, dtype=torch.float64).pin_memory()
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=stream):
                 for _ in range(self.steps_per_slice):
                     s.step(want_norm=False)
-        return _Active(req, s, stream, g, now, first, 1, N)
+                s.residual_sums(dev)
+                sums.copy_(dev, non_blocking=True)
+            s._slice_dev = dev                   # kept alive with the graph
+        return _Active(req, s, stream, g, now, first, sums, None, 1, N)
+
+    def _issue(self, a: _Active):
+        with torch.cuda.stream(a.stream):
+            a.graph.replay()
+            a.done = torch.cuda.Event()
+            a.done.record(a.stream)
+        a.iters += self.steps_per_slice
+
+    def _density(self, a: _Active) -> float:
+        return float(np.sqrt(float(a.sums[1]) / (a.n_cells * a.solver.n_sps)))
+
+    def _failed(self, req: SolveRequest, status: str, now: float) -> SolveResult:
+        return SolveResult(req.rid, req.arrival_s, now, now, 0, status, float("nan"), req.spec.n_cells,
+                           req.spec.order, float("nan"))
 
     def _finish(self, a: _Active, status: str, res: float, now: float) -> SolveResult:
         with torch.cuda.stream(a.stream):
@@ -183,6 +231,7 @@ class ServingLoop:
         done: List[SolveResult] = []
         pool = ThreadPoolExecutor(max_workers=self.gen_workers)
         self.peak_active = 0
+        self.errors: Dict[int, str] = {}
         t0 = time.perf_counter()
         try:
             while pending or queue or active:
@@ -194,30 +243,44 @@ class ServingLoop:
                         futures[r.rid] = pool.submit(lambda c: c, tables[r.rid])
                     else:
                         futures[r.rid] = pool.submit(self._build, r.spec)
-                while queue and len(active) < self.max_active:
+                while queue:
                     r = queue[0]
                     if not futures[r.rid].done():
                         break
                     free, _ = torch.cuda.mem_get_info()
-                    if active and free - self._estimate(r.spec) < self.reserve_gb * 1e9:
+                    decision = admission(free, self._estimate(r.spec), self.reserve_gb * 1e9, len(active),
+                                         self.max_active)
+                    if decision == "wait":
                         break
                     queue.popleft()
                     case = futures.pop(r.rid).result()
-                    active[r.rid] = self._start(r, case, time.perf_counter() - t0)
+                    now = time.perf_counter() - t0
+                    if decision == "reject":
+                        done.append(self._failed(r, "rejected", now))
+                        continue
+                    try:
+                        a = self._start(r, case, now)
+                    except Exception as exc:  # this request alone fails (e.g. out of device memory)
+                        self.errors[r.rid] = repr(exc)
+                        done.append(self._failed(r, "error", time.perf_counter() - t0))
+                        torch.cuda.empty_cache()
+                        continue
+                    finally:
+                        del case
+                    active[r.rid] = a
+                    self._issue(a)
                     self.peak_active = max(self.peak_active, len(active))
-                    del case
                 if not active:
                     time.sleep(0.002)
                     continue
-                # one slice for every admitted request, issued before any check so the slices overlap
-                for a in active.values():
-                    with torch.cuda.stream(a.stream):
-                        a.graph.replay()
-                    a.iters += self.steps_per_slice
+                # every request whose slice has completed: check it, then re-issue or finish it
+                progressed = False
                 for rid in list(active):
                     a = active[rid]
-                    with torch.cuda.stream(a.stream):
-                        res = a.solver.density_residual()
+                    if not a.done.query():
+                        continue
+                    progressed = True
+                    res = self._density(a)
                     status = None
                     if not np.isfinite(res):
                         status = "nonfinite"
@@ -229,9 +292,15 @@ class ServingLoop:
                         done.append(self._finish(a, status, res, time.perf_counter() - t0))
                         del active[rid]
                         torch.cuda.empty_cache()
+                    else:
+                        self._issue(a)
+                if not progressed:
+                    time.sleep(0.0005)
         finally:
             pool.shutdown(wait=True)
             for a in active.values():
+                if a.done is not None:
+                    a.done.synchronize()
                 a.graph = None
                 a.solver.cleanup()
         return done

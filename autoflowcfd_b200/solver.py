@@ -62,12 +62,15 @@ class B200FRSolver:
             contractions as BF16 hi+lo split tensor-core products with FP32
             accumulation, FP32 fluxes; FP64 state, metrics, norms and Cd/Cl).
         device: CUDA device.
+        mixed_ignore_conditioning: build the mixed form even for operators
+            whose row l1 norms exceed its FP32-accumulation bound (to measure
+            its error there; refused by default).
     """
 
     def __init__(self, case: Dict[str, np.ndarray], turb_model_name: str = "NONE", mu_molecular: float = 1.8e-5,
                  rho_inf: float = 1.225, vel_inf: float = 33.33, p_inf: float = 101325.0,
                  inviscid_only: bool = False, global_dt_factor: float = 0.0, precision: str = "fp64",
-                 device="cuda:0"):
+                 device="cuda:0", mixed_ignore_conditioning: bool = False):
         name = turb_model_name.upper()
         if name not in ("SST", "NONE"):
             raise ValueError(f"Unknown turbulence model: {turb_model_name}")
@@ -90,6 +93,7 @@ class B200FRSolver:
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
         prm.precision = _lib.AFR_PREC_MIXED if precision == "mixed" else _lib.AFR_PREC_FP64
+        prm.mixed_ignore_conditioning = 1 if mixed_ignore_conditioning else 0
         self._prm = prm
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
@@ -198,6 +202,15 @@ class B200FRSolver:
         rc = LIB.afr_status(self._h, 0, None, None, 1 if clear else 0, _stream())
         check(rc, self._h)
         return rc
+
+    def residual_sums(self, out: torch.Tensor) -> torch.Tensor:
+        """Queue (no synchronisation, no allocation; capturable) the sums of
+        squares of the last step's stage-0 dU/dt into the device tensor
+        ``out`` (2 doubles): all variables, and the density column."""
+        if not (out.is_cuda and out.dtype == torch.float64 and out.numel() >= 2 and out.is_contiguous()):
+            raise ValueError("out must be a contiguous float64 CUDA tensor of 2 elements")
+        check(LIB.afr_residual_sums(self._h, ctypes.c_void_p(out.data_ptr()), _stream()), self._h)
+        return out
 
     def density_residual(self) -> float:
         """RMS of the density column of dU/dt at the last step (FP64), the

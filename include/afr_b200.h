@@ -144,6 +144,10 @@ typedef struct afr_params {
   double mu;                /* molecular viscosity of the mean flow (FRSolver mu_molecular) */
   double rho_inf, vel_inf, p_inf;
   double global_dt_factor;  /* >0: dt = factor * min(dt_local) everywhere (time-accurate runs) */
+  /* 1: build the mixed form even for operators above the row-l1 bound (its
+   * results then carry errors of about 2^-24 * row l1 * |x|); for measuring
+   * that error only, the refusal (0) is the default */
+  int32_t mixed_ignore_conditioning;
 } afr_params;
 
 int afr_create(const afr_mesh_desc* mesh, const afr_params* params, void* stream, afr_handle** out);
@@ -260,6 +264,17 @@ int afr_launch_shape(const afr_handle* h, int32_t* out);
  * the stream. */
 int afr_segment_norms(afr_handle* h, int32_t nseg, const int64_t* cell_ptr, int32_t which, double* out,
                       void* stream);
+
+/* Sums of squares of the last afr_step's stage-0 dU/dt into the caller's
+ * device buffer out2: out2[0] over all variables, out2[1] over the density
+ * column, each summed in the fixed order of the step norm (the RMS norms are
+ * sqrt(out2[0] / (cells * n_sps * n_vars)) and sqrt(out2[1] / (cells *
+ * n_sps))).  Kernel launches and a device-to-device copy only: no
+ * synchronisation and no allocation, so a steady-solve driver can record it
+ * in the CUDA graph of a slice of steps and poll the result.  Extends
+ * FRState.get_residual_norm (core/fr_solver/state.py:99-108) to the
+ * density-residual stopping rule of a steady solve. */
+int afr_residual_sums(afr_handle* h, double* out2, void* stream);
 
 /* Tensor-core self-check: D[128 x n] = A[128 x k] * B[n x k]^T on the
  * calling device with tcgen05.mma, A and B row-major BF16 bit patterns and D

@@ -49,3 +49,38 @@ def test_latency_summary():
     res = loop().run(requests(), tables=tables())
     s = SV.latency_summary(res, wall_s=10.0)
     assert s["completed"] == 3 and s["p99_s"] >= s["p50_s"] > 0
+
+
+def test_failures_stay_with_their_request(monkeypatch):
+    """One request's state poisoned on the host (NaN), one request whose set-up
+    raises (standing in for an out-of-memory handle): each fails alone, with
+    its own status, and the healthy request finishes with bitwise its
+    result alone."""
+    healthy = requests()[1]
+    alone = loop().run([healthy], tables=tables())[0]
+    real = SV.ServingLoop._prepare
+
+    def prepare(self, req, s, now, stream):
+        if req.rid == 0:
+            raise RuntimeError("afr status 2 (out of device memory): injected")
+        a = real(self, req, s, now, stream)
+        if req.rid == 2:
+            a.solver.U[0, 0, 0] = float("nan")
+        return a
+
+    monkeypatch.setattr(SV.ServingLoop, "_prepare", prepare)
+    lp = loop()
+    res = {r.rid: r for r in lp.run(requests(), tables=tables())}
+    assert res[0].status == "error" and "injected" in lp.errors[0]
+    assert res[2].status == "nonfinite"
+    assert res[1].status == "max_iter" and np.array_equal(res[1].state, alone.state)
+
+
+def test_request_too_large_for_the_device_is_rejected():
+    """The admission budget faked up (estimated bytes per cell far above the
+    device's memory): with nothing running, the request is rejected instead of
+    attempted."""
+    lp = loop()
+    lp.bytes_per_cell = {1: 1e12, 2: 1e12}
+    res = lp.run(requests()[:1], tables=tables())
+    assert res[0].status == "rejected" and res[0].iterations == 0
