@@ -79,6 +79,10 @@ SIGNATURES = {
     "afr_step_profile": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                                                   ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     "afr_rms_norm_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
+    "afr_step_dual_time": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                                                  ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                                                  ctypes.c_void_p]),
+    "afr_step_imex": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "afr_residual_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "afr_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P_I64, _P_I32, ctypes.c_int32, ctypes.c_void_p]),
     "afr_autotune": (ctypes.c_int, [ctypes.c_void_p] * 3 + [_P_I32, ctypes.c_void_p]),

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/afr_b200.h"
+#include "afr_implicit.cuh"
 #include "afr_mixed.cuh"
 #include "afr_sst.cuh"
 
@@ -69,6 +70,13 @@ struct afr_handle {
   // launch shapes chosen by afr_autotune (defaults until then)
   int mx_face_block = 128;  // threads per face-kernel CTA: 64, 128 or 256
   int mx_upd_var = 1;       // update-kernel cells per CTA: 0 = half, 1 = base, 2 = double
+  // dual-time / IMEX buffers, allocated by the first call of either scheme
+  double* iRinv = nullptr;   // (N,S,nv) inviscid residual (dU/dt)
+  double* iRvisc = nullptr;  // (N,S,nv) viscous residual (dU/dt)
+  double* iRscr = nullptr;   // (N,S,nv) discarded inviscid residual of the IMEX iterations
+  double* iUn = nullptr;     // (N,S,nv) state at the start of the physical step
+  double* iX = nullptr;      // (N,S,nv) next iterate
+  double* idt = nullptr;     // (N,S) physical time step of the dual-time SST update
   std::vector<void*> allocs;
   size_t mat_elems[4] = {0, 0, 0, 0};  // doubles of each interpolation-matrix allocation (0: shares the first)
   uint64_t bytes = 0;
@@ -188,6 +196,11 @@ __global__ void k_reduce_min(const double* x, size_t n, double* out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_fill_value(double* x, size_t n, double v) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v;
 }
 
 __global__ void k_fill_scaled(double* x, size_t n, const double* v, double factor) {
@@ -786,7 +799,9 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
       const int mm = n / Sq, s = n % Sq;
       return (s < S && j < S) ? D3[(size_t)s * 3 * S + j * 3 + mm] : 0.0;
     });
-    auto i_E = kmajor_image(128, Sq, [&](int fp, int s) {
+    const int edup = mx_ext_dup(6 * P);  // copies of the face-point rows (see afr_mixed.cuh)
+    auto i_E = kmajor_image(128, Sq, [&](int r, int s) {
+      const int fp = r % (128 / edup);
       if (fp >= 6 * P || s >= S) return 0.0;
       const int a = fp / P, i = fp % P;
       return ex[(((size_t)t * 3 + a / 2) * 2 + a % 2) * P * S + (size_t)i * S + s];
@@ -820,7 +835,7 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   const int FW = h->order <= 2 ? 18 : 5;
   float *xf, *pfm, *jm;
   const size_t ns = h->slots.n;
-  if ((rc = dalloc(h, &xf, N * FW * 6 * P)) || (rc = dalloc(h, &pfm, N * S * 20)) || (rc = dalloc(h, &jm, ns * P * 10)))
+  if ((rc = dalloc(h, &xf, N * FW * 6 * P)) || (rc = dalloc(h, &pfm, N * S * 20)) || (rc = dalloc(h, &jm, ns * P * 10 + 4)))  // 16 bytes of slack: the update kernel copies 16-byte-rounded slot ranges
     return rc;
   float* rv;
   if ((rc = dalloc(h, &rv, N * S * 10))) return rc;
@@ -1366,6 +1381,209 @@ static int step_impl(afr_handle* h, double* U, double* k, double* omega, double*
 
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
   return step_impl(h, U, k, omega, nu_t, norm_out, (cudaStream_t)stream, nullptr, nullptr);
+}
+
+// ---- dual-time and IMEX integrators (core/time_integration/dual.py, imex.py) ----
+namespace {
+int imp_buffers(afr_handle* h) {
+  if (h->iRinv) return AFR_OK;
+  const size_t n = (size_t)h->N * h->S * h->nv;
+  int rc;
+  if ((rc = dalloc(h, &h->iRinv, n)) || (rc = dalloc(h, &h->iRvisc, n)) || (rc = dalloc(h, &h->iRscr, n)) ||
+      (rc = dalloc(h, &h->iUn, n)) || (rc = dalloc(h, &h->iX, n)) || (rc = dalloc(h, &h->idt, (size_t)h->N * h->S)))
+    return rc;
+  return AFR_OK;
+}
+
+// inviscid and viscous residuals (dU/dt, zero turbulence columns) of the state U
+int eval_both(afr_handle* h, const double* U, const double* nut, double* Rinv, double* Rvisc, cudaStream_t st) {
+  StageArgs a = base_args(h);
+  a.Ucur = U;
+  a.inviscid_only = h->prm.inviscid_only;
+  a.stage = -1;
+  a.nut = nut;
+  a.Rinv = Rinv;
+  a.Rvisc = Rvisc;
+  const bool visc = !h->prm.inviscid_only;
+  cudaError_t e = dispatch(h, [&](auto L) { return L.eval(h, a, U, nut, visc, st); });
+  if (e == cudaSuccess && h->prm.inviscid_only) e = cudaMemsetAsync(Rvisc, 0, (size_t)h->N * h->S * h->nv * 8, st);
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "residual evaluation");
+}
+
+// sqrt of the sum of squares selected by mode (see k_imp_sumsq), synchronising
+int imp_norm(afr_handle* h, const ImpArgs& a, int mode, cudaStream_t st, double* out) {
+  const size_t n = (size_t)a.npts * a.nv;
+  const unsigned nb = (unsigned)((n + IMP_CHUNK - 1) / IMP_CHUNK);
+  k_imp_sumsq<<<nb, IMP_THREADS, 0, st>>>(a, mode, h->red_part);
+  k_reduce_sum<<<1, 1024, 0, st>>>(h->red_part, nb, h->red + 1);
+  double ss = 0.0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ss, h->red + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "norm");
+  *out = std::sqrt(ss);
+  return AFR_OK;
+}
+
+int filter_cells(afr_handle* h, double* U, cudaStream_t st) {
+  switch (h->order) {
+    case 1: k_filter_cells<8><<<h->N, 64, 0, st>>>(h->g, h->ops, U, h->nv); break;
+    case 2: k_filter_cells<27><<<h->N, 160, 0, st>>>(h->g, h->ops, U, h->nv); break;
+    default: k_filter_cells<64><<<h->N, 320, 0, st>>>(h->g, h->ops, U, h->nv); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "filter");
+}
+
+int copy_state(afr_handle* h, double* dst, const double* src, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, (size_t)h->N * h->S * h->nv * 8, cudaMemcpyDeviceToDevice, st);
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "state copy");
+}
+
+// the step's preamble shared with SSP-RK3: local dt, SST once (with turb_dt),
+// the residual at U^n and the RMS norm of dU/dt
+int imp_preamble(afr_handle* h, double* U, double* k, double* omega, double* nu_t, const double* turb_dt,
+                 double* norm_out, cudaStream_t st) {
+  const bool sst = h->prm.turb == AFR_TURB_SST;
+  int rc = compute_dt(h, U, sst ? nu_t : nullptr, h->dt, st);
+  if (rc) return rc;
+  if (sst) {
+    cudaError_t e = dispatch(h, [&](auto L) {
+      SstArgs s{U, turb_dt ? turb_dt : h->dt, k, omega, nu_t, h->pt, h->sp8, h->cfp, h->wall_face, nullptr, h->nv,
+                h->prm.mu};
+      return L.sst(h, s, st, nullptr);
+    });
+    if (e != cudaSuccess) return cuda_fail(h, e, "sst update");
+  }
+  if ((rc = eval_both(h, U, sst ? nu_t : nullptr, h->iRinv, h->iRvisc, st))) return rc;
+  ImpArgs a{};
+  a.npts = (int64_t)h->N * h->S;
+  a.nv = h->nv;
+  a.Rinv = h->iRinv;
+  a.Rvisc = h->iRvisc;
+  double nrm = 0.0;
+  if ((rc = imp_norm(h, a, 3, st, &nrm))) return rc;
+  if (norm_out) *norm_out = nrm / std::sqrt((double)h->N * h->S * h->nv);
+  return AFR_OK;
+}
+}  // namespace
+
+int afr_step_dual_time(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* U_prev,
+                       int32_t has_prev, double dt_physical, int32_t max_inner_iter, double tol, double* norm_out,
+                       void* stream) {
+  if (!h || !U || !U_prev || !(dt_physical > 0.0) || max_inner_iter < 0) return AFR_EINVAL;
+  const bool sst = h->prm.turb == AFR_TURB_SST;
+  if (sst && (!k || !omega || !nu_t)) return fail(h, AFR_EINVAL, "SST step needs k, omega and nu_t");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (capturing(st)) return fail(h, AFR_EINVAL, "the dual-time step synchronises: not inside a stream capture");
+  int rc = pending_status(h, st);
+  if (rc || (rc = imp_buffers(h))) return rc;
+  const size_t npts = (size_t)h->N * h->S;
+  // the SST fields advance with the physical step (core/fr_solver/step.py:109)
+  k_fill_value<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(h->idt, npts, dt_physical);
+  if ((rc = imp_preamble(h, U, k, omega, nu_t, h->idt, norm_out, st))) return rc;
+  const double* nut = sst ? nu_t : nullptr;
+  if ((rc = copy_state(h, h->iUn, U, st))) return rc;  // U^n; U itself holds the pseudo iterate
+  ImpArgs a{};
+  a.npts = (int64_t)npts;
+  a.nv = h->nv;
+  a.Rinv = h->iRinv;
+  a.Rvisc = h->iRvisc;
+  a.Un = h->iUn;
+  a.Uprev = has_prev ? U_prev : nullptr;
+  a.dtphys = dt_physical;
+  a.dtl = h->dt;
+  const unsigned gb = (unsigned)((npts + 255) / 256);
+  double init = 0.0, prev = 0.0, cfl = 0.1;
+  a.Ucur = U;
+  if ((rc = imp_norm(h, a, 0, st, &init))) return rc;
+  for (int it = 0; it < max_inner_iter; ++it) {
+    a.Ucur = U;
+    if (it > 0 && (rc = eval_both(h, U, nut, h->iRinv, h->iRvisc, st))) return rc;
+    double cur = init;
+    if (it > 0 && (rc = imp_norm(h, a, 0, st, &cur))) return rc;
+    if (cur < init * 1e-6) break;
+    if (it >= 1 && cur < tol) break;
+    if (it > 0) {
+      const double ratio = cur / prev;
+      if (ratio < 0.5) cfl = std::min(cfl * 1.5, 10.0);
+      else if (ratio > 1.0) cfl = std::max(cfl * 0.5, 0.1);
+    }
+    prev = cur;
+    a.scale = cfl;
+    // SSP-RK3 of the dual residual from U (the stage-0 residual is the one above)
+    double* stg[3] = {h->Ua, h->Ub, h->iX};
+    for (int s = 0; s < 3; ++s) {
+      if (s > 0 && (rc = eval_both(h, stg[s - 1], nut, h->iRinv, h->iRvisc, st))) return rc;
+      a.U0 = U;
+      a.Ucur = s == 0 ? U : stg[s - 1];
+      a.stage = s;
+      a.Unext = stg[s];
+      k_dual_stage<<<gb, 256, 0, st>>>(a);
+      if ((rc = filter_cells(h, stg[s], st))) return rc;
+    }
+    // positivity and filter once more on the pseudo step's result (dual.py:137-139)
+    k_positivity<<<gb, 256, 0, st>>>(h->iX, (int64_t)npts, h->nv);
+    if ((rc = filter_cells(h, h->iX, st))) return rc;
+    ImpArgs d = a;
+    d.U0 = U;
+    d.Ucur = h->iX;
+    double upd = 0.0;
+    if ((rc = imp_norm(h, d, 1, st, &upd))) return rc;
+    if (upd < 1e-10) break;
+    if ((rc = copy_state(h, U, h->iX, st))) return rc;
+  }
+  if ((rc = copy_state(h, U_prev, h->iUn, st))) return rc;  // level n becomes the next step's n-1
+  return check_status(h, st);
+}
+
+int afr_step_imex(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream) {
+  if (!h || !U) return AFR_EINVAL;
+  const bool sst = h->prm.turb == AFR_TURB_SST;
+  if (sst && (!k || !omega || !nu_t)) return fail(h, AFR_EINVAL, "SST step needs k, omega and nu_t");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (capturing(st)) return fail(h, AFR_EINVAL, "the IMEX step synchronises: not inside a stream capture");
+  int rc = pending_status(h, st);
+  if (rc || (rc = imp_buffers(h))) return rc;
+  if ((rc = imp_preamble(h, U, k, omega, nu_t, nullptr, norm_out, st))) return rc;
+  const double* nut = sst ? nu_t : nullptr;
+  const size_t npts = (size_t)h->N * h->S;
+  const unsigned gb = (unsigned)((npts + 255) / 256);
+  // R_exp = -inviscid(U^n) stays in iRinv; iRvisc holds the viscous residual of the iterate
+  ImpArgs a{};
+  a.npts = (int64_t)npts;
+  a.nv = h->nv;
+  a.Rinv = h->iRinv;
+  a.Rvisc = h->iRvisc;
+  a.dtl = h->dt;
+  a.Ucur = U;
+  double init = 0.0, prev = 0.0, damping = 0.5;
+  if ((rc = imp_norm(h, a, 2, st, &init))) return rc;
+  for (int it = 0; it < 5; ++it) {
+    if (it > 0 && (rc = eval_both(h, U, nut, h->iRscr, h->iRvisc, st))) return rc;
+    double cur = init;
+    if (it > 0 && (rc = imp_norm(h, a, 2, st, &cur))) return rc;
+    if (it > 0) {
+      const double ratio = cur / prev;
+      if (ratio < 0.5) damping = std::min(damping * 1.2, 1.0);
+      else if (ratio > 1.0) damping = std::max(damping * 0.5, 0.1);
+    } else {
+      damping = 0.5;
+    }
+    prev = cur;
+    a.Ucur = U;
+    a.scale = damping;
+    a.Unext = h->iX;
+    k_imex_update<<<gb, 256, 0, st>>>(a);
+    ImpArgs d = a;
+    d.U0 = U;
+    d.Ucur = h->iX;
+    double upd = 0.0;
+    if ((rc = imp_norm(h, d, 1, st, &upd))) return rc;
+    if (upd < 1e-8 || cur < init * 1e-6) break;
+    if ((rc = copy_state(h, U, h->iX, st))) return rc;
+  }
+  return check_status(h, st);
 }
 
 // ---- launch-shape autotuner (mixed form) ----

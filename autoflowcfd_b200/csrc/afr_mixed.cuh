@@ -48,6 +48,11 @@ constexpr int MX_PRE_CELLS = 8;
 __host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int pow2_cols(int x) { return x <= 32 ? 32 : (x <= 64 ? 64 : (x <= 128 ? 128 : 256)); }
+// Copies of the face-point rows in the 128-row extrapolation image: with 6*NP
+// face points <= 32 (P1) every 32-lane quarter of tensor memory holds a copy,
+// <= 64 (P2) two halves do; each copy's readout serves its share of the tile's
+// cells, so every warp of the CTA takes part in the readout.
+__host__ __device__ constexpr int mx_ext_dup(int nfp) { return nfp <= 32 ? 4 : (nfp <= 64 ? 2 : 1); }
 
 // Operator images, K-major canonical, BF16 bit patterns.  "cat" images stack
 // the hi rows over the lo rows (2N rows, one image); the others are [hi | lo].
@@ -56,7 +61,7 @@ struct MxOps {
   const uint16_t* W[2];    // B cat: rows s < Sq, K = 3*Fq, k = m*Fq + i
   const uint16_t* D3[2];   // B cat: rows s < Sq, K = 3*Sq, k = m*Sq + j
   const uint16_t* D3g[2];  // B: rows m*Sq + s, K = Sq (j)
-  const uint16_t* E[2];    // A: rows fp = (ax*2+side)*NP + i (128 rows), K = Sq
+  const uint16_t* E[2];    // A: rows j*(128/DUP) + fp, fp = (ax*2+side)*NP + i, copies j < DUP = mx_ext_dup(6*NP); K = Sq
   const double* MD;        // (N, S, 3) metric divergence of the folded W
   const float4* adjf;      // (N, FN, 3) FP32 fine-point adjugate rows (4th entry zero)
   const float4* adjs;      // (N, S, 3) FP32 solution-point adjugate rows
@@ -252,7 +257,7 @@ struct MxPreSmem {
 };
 
 template <int S, int NP>
-__global__ void __launch_bounds__(MX_THREADS, 1)
+__global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per SM (tensor memory allows two)
     k_mx_pre(Geom g, MxOps mo, MxBuf mb, const double* __restrict__ U, int nv, const double* __restrict__ nut,
              int visc, int cell_base, int cell_end, unsigned* status) {
   using L = MxPreSmem<S, NP>;
@@ -345,7 +350,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       const int col = k < 5 ? k : (k < 8 ? k - 4 : 5);
       double acc = 0.0;
       for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 6 + col];
-      sM[c * 9 + k] = acc / S;
+      sM[c * 9 + k] = acc * (1.0 / S);
     }
     __syncthreads();
     for (int t = tid; t < C * S; t += MX_THREADS) {
@@ -441,18 +446,23 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     if (abort_flag) break;
     tc::fence_after();
     {
-      const int q4 = warp & 3, fp = q4 * 32 + lane;
-      if (q4 * 32 < NFP) {
+      // copy j of the face-point rows (lanes j*128/DUP ...) serves cells
+      // [j*C/DUP, (j+1)*C/DUP); the quarters of one copy split its face points
+      constexpr int DUP = mx_ext_dup(NFP), QPC = 4 / DUP, CPC = C / DUP;
+      const int q4 = warp & 3, j = q4 / QPC, fp = (q4 % QPC) * 32 + lane;
+      if ((q4 % QPC) * 32 < NFP) {
         for (int f = warp >> 2; f < nfw; f += MX_THREADS / 128) {
-          float v8[8];
-          tc::tmem_ld8(tmem + ((uint32_t)(q4 * 32) << 16) + f * 8, v8);
+          float vc[CPC];  // this copy's cells only (fixed register indices)
+          tc::tmem_ldn<CPC>(tmem + ((uint32_t)(q4 * 32) << 16) + f * 8 + j * CPC, vc);
           if (fp < NFP) {
 #pragma unroll
-            for (int c = 0; c < C; ++c)
+            for (int cc = 0; cc < CPC; ++cc) {
+              const int c = j * CPC + cc;
               if (c < nc) {
-                const float val = f < 5 ? float(sM[c * 9 + f] + (double)v8[c]) : v8[c];
+                const float val = f < 5 ? float(sM[c * 9 + f] + (double)vc[cc]) : vc[cc];
                 mb.XF[((size_t)(e0 + c) * FW + f) * NFP + fp] = val;
               }
+            }
           }
         }
       }
@@ -718,7 +728,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
       const int c = t / 5, v = t % 5;
       double acc = 0.0;
       for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 5 + v];
-      sQb[t] = acc / S;
+      sQb[t] = acc * (1.0 / S);
     }
     __syncthreads();
     for (int c = tid; c < C; c += NT) {
@@ -900,47 +910,159 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
 // update kernel: CPB cells per CTA.  Lifting of the face jumps in ascending
 // color order (staged in shared memory), outlier zeroing, then the SSP-RK3
 // combination, positivity and filter in FP64 (or the residual-only outputs).
+//
+// The tile's inputs are contiguous blocks (the cells e0 .. e0+nc of the state,
+// step-start state, volume terms, reciprocal det and dt, and the slots of
+// those cells' jumps); each arrives in shared memory by one bulk asynchronous
+// copy (cp.async.bulk, completion counted in bytes on an mbarrier).  A block
+// whose address or size is not a multiple of 16 bytes (odd first cell of a
+// range, odd last tile) is copied by 8-byte asynchronous copies instead.
+// Shared-memory rows keep the global layout: state rows of n_vars doubles (an
+// odd stride, so threads reading consecutive points use distinct banks).
 // ---------------------------------------------------------------------------
 constexpr int MX_UPD_MAXSLOT = 6;  // slots per cell staged in shared memory (more: read from global)
+
+__host__ __device__ constexpr int align16(int b) { return (b + 15) / 16 * 16; }
 
 template <int S, int NP, int CPB>
 struct MxUpdSmem {
   static constexpr int THREADS = 256;
-  static constexpr int oRi = 0;                        // CPB*S*5 doubles
-  static constexpr int oRv = oRi + CPB * S * 5;
-  static constexpr int oU = oRv + CPB * S * 5;         // CPB*S*US
-  static constexpr int oU0 = oU + CPB * S * US;        // CPB*S*US step-start state
-  static constexpr int oW = oU0 + CPB * S * US;        // outliers: CPB*2*OUT_WORK
-  static constexpr int oP = oW + CPB * 2 * OUT_WORK;   // 2*CPB*S: squared dU/dt, squared density column
-  static constexpr int oG = oP + 2 * CPB * S;        // g_left, g_right (2*4)
-  static constexpr int oRd = oG + 8;                  // CPB*S reciprocal det
-  static constexpr int oDt = oRd + CPB * S;           // CPB*S local dt
-  static constexpr int nD = (oDt + CPB * S + 1) / 2 * 2;  // doubles (even: the jumps start 16-byte aligned)
-  static constexpr int nJ = CPB * MX_UPD_MAXSLOT * NP * 10;  // floats: staged jumps
-  static constexpr int nR = CPB * S * 10;                    // floats: the tile's volume terms
-  // ints: slot flags of the staged slots, per-cell slot pointers, distribution maps
+  static constexpr int NVMAX = 7;
+  // byte offsets; bulk-copy destinations 16-byte aligned
+  static constexpr int bU = 0;                                        // CPB*S*nv doubles
+  static constexpr int bU0 = align16(bU + CPB * S * NVMAX * 8);       // step-start state
+  static constexpr int bRV = align16(bU0 + CPB * S * NVMAX * 8);      // CPB*S*10 floats
+  static constexpr int bRd = align16(bRV + CPB * S * 10 * 4);         // CPB*S doubles
+  static constexpr int bDt = align16(bRd + CPB * S * 8);              // CPB*S doubles
+  static constexpr int bJ = align16(bDt + CPB * S * 8);               // jumps, 16-byte lead
+  static constexpr int bRi = align16(bJ + CPB * MX_UPD_MAXSLOT * NP * 10 * 4 + 16);  // CPB*S*5 doubles
+  static constexpr int bRv = bRi + CPB * S * 5 * 8;                   // CPB*S*5 doubles
+  static constexpr int bW = bRv + CPB * S * 5 * 8;                    // outliers: CPB*2*OUT_WORK doubles
+  static constexpr int bP = bW + CPB * 2 * OUT_WORK * 8;              // 2*CPB*S doubles
+  static constexpr int bG = bP + 2 * CPB * S * 8;                     // g_left, g_right (8 doubles)
+  static constexpr int bI = bG + 8 * 8;                               // ints
   static constexpr int nI = CPB * MX_UPD_MAXSLOT + CPB + 1 + 6 * S;
-  static constexpr int total = nD * 8 + nJ * 4 + nR * 4 + nI * 4;
+  static constexpr int total = bI + nI * 4;
 };
+
+namespace mxd {
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   tc::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool bulk_ok(const void* src, size_t bytes) {
+  return ((reinterpret_cast<uintptr_t>(src) | bytes) & 15u) == 0 && bytes > 0;
+}
+// 8-byte asynchronous copies of a block whose bulk copy is not possible
+__device__ __forceinline__ void copy8(void* dst, const void* src, size_t bytes) {
+  for (size_t t = threadIdx.x; t < bytes / 8; t += blockDim.x)
+    cp_async8(static_cast<char*>(dst) + 8 * t, static_cast<const char*>(src) + 8 * t);
+}
+}  // namespace mxd
+
+// Outlier zeroing of the mixed update kernel (same rule as
+// suppress_outliers_cells, core/fr_operators/troubled_cell.py:346-408): the
+// column statistics -- mean |U|, min and max |R|, NaN, and the count against
+// the lower bound of the median -- by four threads per column (aligned lane
+// groups, combined with shuffles) instead of one.  Reference rows have stride
+// ldU.  work >= OUT_WORK doubles per block (block b < nc: sRi of cell b,
+// nc + b: sRv of cell b).
+template <int S>
+__device__ void mx_suppress_outliers(double* sRi, double* sRv, const double* sU, int ldU, int nc, bool visc,
+                                     double* work) {
+  constexpr int NEED = S - ((S & 1) ? S / 2 : S / 2 - 1);  // elements at or above the (lower) middle rank
+  const int nb = nc * (visc ? 2 : 1);
+  const int ncol = nb * 5;
+  const int n4 = (ncol * 4 + (int)blockDim.x - 1) / (int)blockDim.x * (int)blockDim.x;
+  for (int base = 0; base < n4; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const bool on = t < ncol * 4;
+    const int col = on ? (t >> 2) : 0, sub = t & 3;
+    const int bb = col / 5, v = col % 5;
+    const double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
+    const double* Ur = sU + (bb % nc) * S * ldU;
+    double acc = 0.0, lo = INFINITY, hi = 0.0;
+    int nan = 0;
+    if (on)
+      for (int s = sub; s < S; s += 4) {
+        acc += fabs(Ur[s * ldU + v]);
+        const double x = fabs(R[s * 5 + v]);
+        lo = fmin(lo, x);
+        hi = fmax(hi, x);
+        nan |= isnan(x) ? 1 : 0;
+      }
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      nan |= __shfl_xor_sync(0xffffffffu, nan, o);
+    }
+    const double mean = acc / S;
+    bool skip = !nan && hi <= 1e4 * fmax(fmax(lo, 1e-9 * mean), 1e-300);
+    double bound = lo;
+    bool count = !nan && !skip;
+    double p = hi * 1e-4;
+    if (count) {
+      // next double up (p is finite and >= 0 here: its bit pattern plus one)
+      for (int it = 0; it < 4 && 1e4 * p < hi; ++it) p = __longlong_as_double(__double_as_longlong(p) + 1);
+      count = 1e4 * p >= hi;
+    }
+    int cnt = 0;
+    if (on && count)
+      for (int s = sub; s < S; s += 4) cnt += fabs(R[s * 5 + v]) >= p;
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (count && cnt >= NEED) {
+      skip = true;
+      bound = p;
+    }
+    if (on && sub == 0) {
+      double* w = work + bb * OUT_WORK;
+      w[5 + v] = mean;
+      w[v] = bound;
+      w[20 + v] = skip ? 0.0 : 1.0;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
+    double* w = work + bb * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_rank<S>(bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5, s, v, w);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
+    const int bb = t / (S * 5), r = t % (S * 5), v = r % 5;
+    const double* w = work + bb * OUT_WORK;
+    if (w[20 + v] != 0.0) outlier_zero(bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5, r, v, w, S & 1);
+  }
+  __syncthreads();
+}
 
 template <int S, int NP, int CPB>
 __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
     k_mx_update(Geom g, Ops ops, Faces fc, StageArgs a, const float* __restrict__ RV, const float* __restrict__ Jm,
                 const double* __restrict__ rdet) {
   using L = MxUpdSmem<S, NP, CPB>;
-  extern __shared__ double smu[];
-  double* sRi = smu + L::oRi;
-  double* sRv = smu + L::oRv;
-  double* sU = smu + L::oU;
-  double* work = smu + L::oW;
-  double* sU0 = smu + L::oU0;
-  double* part = smu + L::oP;
-  double* sGw = smu + L::oG;  // [0..3] g_left, [4..7] g_right
-  double* sRd = smu + L::oRd;
-  double* sDt = smu + L::oDt;
-  float* sJ = reinterpret_cast<float*>(smu + L::nD);
-  float* sRVf = sJ + L::nJ;
-  int* sFl = reinterpret_cast<int*>(sRVf + L::nR);
+  extern __shared__ __align__(128) uint8_t smb[];
+  __shared__ uint64_t bar;
+  double* sU = reinterpret_cast<double*>(smb + L::bU);
+  double* sU0 = reinterpret_cast<double*>(smb + L::bU0);
+  float* sRVf = reinterpret_cast<float*>(smb + L::bRV);
+  double* sRd = reinterpret_cast<double*>(smb + L::bRd);
+  double* sDt = reinterpret_cast<double*>(smb + L::bDt);
+  double* sRi = reinterpret_cast<double*>(smb + L::bRi);
+  double* sRv = reinterpret_cast<double*>(smb + L::bRv);
+  double* work = reinterpret_cast<double*>(smb + L::bW);
+  double* part = reinterpret_cast<double*>(smb + L::bP);
+  double* sGw = reinterpret_cast<double*>(smb + L::bG);  // [0..3] g_left, [4..7] g_right
+  int* sFl = reinterpret_cast<int*>(smb + L::bI);
   int* sPtr = sFl + CPB * MX_UPD_MAXSLOT;
   int* sDfp = sPtr + CPB + 1;
   int* sDco = sDfp + 3 * S;
@@ -951,70 +1073,95 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   const bool visc = !a.inviscid_only;
   const int tid = threadIdx.x;
   constexpr int N1D = S == 8 ? 2 : (S == 27 ? 3 : 4);
-  for (int t = tid; t < 3 * S; t += blockDim.x) {
-    sDfp[t] = ops.dist_fp[t];
-    sDco[t] = ops.dist_co[t];
-  }
-  if (tid < N1D) {
-    sGw[tid] = ops.g_left[tid];
-    sGw[4 + tid] = ops.g_right[tid];
-  }
-  if (tid <= nc) sPtr[tid] = fc.slot_ptr[e0 + tid];
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
   const bool staged = (k_end - k_beg) <= CPB * MX_UPD_MAXSLOT;
-  // The tile's inputs are contiguous blocks: asynchronous 8-byte copies, all
-  // in flight at once (state rows t -> point t/nv, variable t%nv through an
-  // exact float reciprocal; volume terms and jumps as float pairs)
+  // jump block: bytes [jb0, jb1) of Jm rounded out to 16-byte boundaries (the
+  // allocation carries 16 bytes of slack); the tile's first jump sits jlead
+  // bytes into the staged copy
+  const size_t jb0 = (size_t)k_beg * NP * 40, jb1 = (size_t)k_end * NP * 40;
+  const size_t ja0 = jb0 & ~size_t(15), ja1 = (jb1 + 15) & ~size_t(15);
+  const float* sJ = reinterpret_cast<const float*>(smb + L::bJ + (jb0 - ja0));
   {
-    const float rnv = 1.0f / float(nv);
+    const size_t ub = (size_t)nc * S * nv * 8, pb = (size_t)nc * S * 8, rb = (size_t)nc * S * 40;
     const double* uc = a.Ucur + (size_t)e0 * S * nv;
     const double* u0 = a.U0 + (size_t)e0 * S * nv;
-    for (int t = tid; t < nc * S * nv; t += blockDim.x) {
-      const int p = __float2int_rz((float(t) + 0.5f) * rnv), v = t - p * nv;
-      mxd::cp_async8(sU + p * US + v, uc + t);
-      if (a.stage >= 0) mxd::cp_async8(sU0 + p * US + v, u0 + t);
-    }
     const float* rv = RV + (size_t)e0 * S * 10;
-    for (int t = tid; t < nc * S * 5; t += blockDim.x) mxd::cp_async8(sRVf + 2 * t, rv + 2 * t);
-    for (int t = tid; t < nc * S; t += blockDim.x) {
-      mxd::cp_async8(sRd + t, rdet + (size_t)e0 * S + t);
-      if (a.stage >= 0) mxd::cp_async8(sDt + t, a.dt + (size_t)e0 * S + t);
+    const double* rd = rdet + (size_t)e0 * S;
+    const double* dt = a.stage >= 0 ? a.dt + (size_t)e0 * S : nullptr;
+    const char* jsrc = reinterpret_cast<const char*>(Jm) + ja0;
+    const bool bu = mxd::bulk_ok(uc, ub), bu0 = a.stage >= 0 && mxd::bulk_ok(u0, ub), brv = mxd::bulk_ok(rv, rb),
+               brd = mxd::bulk_ok(rd, pb), bdt = a.stage >= 0 && mxd::bulk_ok(dt, pb),
+               bj = staged && k_end > k_beg;  // rounded out: always aligned
+    if (tid == 0) {
+      tc::mbar_init(&bar, 1);
+      tc::fence_mbar_init();
     }
-    if (staged) {
-      const float* jb = Jm + (size_t)k_beg * NP * 10;
-      for (int t = tid; t < (k_end - k_beg) * NP * 5; t += blockDim.x) mxd::cp_async8(sJ + 2 * t, jb + 2 * t);
+    __syncthreads();
+    if (tid == 0) {
+      const uint32_t tx = (bu ? ub : 0) + (bu0 ? ub : 0) + (brv ? rb : 0) + (brd ? pb : 0) + (bdt ? pb : 0) +
+                          (bj ? ja1 - ja0 : 0);
+      mxd::mbar_expect_tx(&bar, tx);
+      if (bu) mxd::bulk_g2s(sU, uc, (uint32_t)ub, &bar);
+      if (bu0) mxd::bulk_g2s(sU0, u0, (uint32_t)ub, &bar);
+      if (brv) mxd::bulk_g2s(sRVf, rv, (uint32_t)rb, &bar);
+      if (brd) mxd::bulk_g2s(sRd, rd, (uint32_t)pb, &bar);
+      if (bdt) mxd::bulk_g2s(sDt, dt, (uint32_t)pb, &bar);
+      if (bj) mxd::bulk_g2s(smb + L::bJ, jsrc, (uint32_t)(ja1 - ja0), &bar);
+    }
+    if (!bu) mxd::copy8(sU, uc, ub);
+    if (a.stage >= 0 && !bu0) mxd::copy8(sU0, u0, ub);
+    if (!brv) mxd::copy8(sRVf, rv, rb);
+    if (!brd) mxd::copy8(sRd, rd, pb);
+    if (a.stage >= 0 && !bdt) mxd::copy8(sDt, dt, pb);
+    for (int t = tid; t < 3 * S; t += blockDim.x) {
+      sDfp[t] = ops.dist_fp[t];
+      sDco[t] = ops.dist_co[t];
+    }
+    if (tid < N1D) {
+      sGw[tid] = ops.g_left[tid];
+      sGw[4 + tid] = ops.g_right[tid];
+    }
+    if (tid <= nc) sPtr[tid] = fc.slot_ptr[e0 + tid];
+    if (staged)
       for (int t = tid; t < k_end - k_beg; t += blockDim.x) sFl[t] = a.slot_flags[k_beg + t];
-    }
     mxd::cp_async_wait_all();
+    uint32_t ph = 0;
+    if (!mxd::wait_commit(&bar, ph, a.status)) {
+      // the status reports the time-out; wait once more (bounded) so that no
+      // copy is still writing this CTA's shared memory when it moves on
+      uint32_t ph0 = 0;
+      tc::mbar_wait(&bar, ph0);
+    }
   }
   __syncthreads();
-  // lift the jumps of each cell's slots, ascending color order
-  // one thread per point: each slot's metadata decoded once for all variables
-  for (int p = tid; p < nc * S; p += blockDim.x) {
+  // lift the jumps of each cell's slots, ascending color order; two threads
+  // per point, one for the inviscid and one for the viscous jumps
+  for (int t = tid; t < 2 * nc * S; t += blockDim.x) {
+    const int p = t >> 1, half = t & 1;
+    if (half && !visc) {
+      sRv[p * 5 + 0] = sRv[p * 5 + 1] = sRv[p * 5 + 2] = sRv[p * 5 + 3] = sRv[p * 5 + 4] = 0.0;
+      continue;
+    }
     const int b = p / S, s = p - b * S;
-    const double rdj = sRd[p];  // reciprocal formed at create
-    double ci[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, cv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double cx[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (int k = sPtr[b]; k < sPtr[b + 1]; ++k) {
       const int fl = staged ? sFl[k - k_beg] : a.slot_flags[k];
       const int ax = (fl >> 2) & 3;
       const int fp = sDfp[ax * S + s];
       const double gw = sGw[((fl & 16) ? 4 : 0) + sDco[ax * S + s]];
-      const float* Jk = staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10;
+      const float* Jk = (staged ? sJ + ((k - k_beg) * NP + fp) * 10 : Jm + ((size_t)k * NP + fp) * 10) + 5 * half;
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        ci[v] -= gw * double(Jk[v]);
-        if (visc) cv[v] += gw * double(Jk[5 + v]);
-      }
+      for (int v = 0; v < 5; ++v) cx[v] += gw * double(Jk[v]);
     }
-    const float* rp = sRVf + p * 10;
+    const double rdj = sRd[p];
+    const float* rp = sRVf + p * 10 + 5 * half;
+    double* out = half ? sRv : sRi;
+    const double sg = half ? 1.0 : -1.0;  // inviscid corrections enter with -g', viscous with +g'
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      sRi[p * 5 + v] = double(rp[v]) + ci[v] * rdj;
-      sRv[p * 5 + v] = visc ? double(rp[5 + v]) + cv[v] * rdj : 0.0;
-    }
+    for (int v = 0; v < 5; ++v) out[p * 5 + v] = double(rp[v]) + sg * cx[v] * rdj;
   }
   __syncthreads();
-  suppress_outliers_cells<S>(sRi, sRv, sU, nc, visc, work);
+  mx_suppress_outliers<S>(sRi, sRv, sU, nv, nc, visc, work);
 
   if (a.stage < 0) {
     for (int p = tid; p < nc * S; p += blockDim.x)
@@ -1036,8 +1183,8 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
     for (int v = 0; v < 8; ++v)
       if (v < nv) sq_sum += Lr[v] * Lr[v];
     const double dts = sDt[p];
-    const double* u0 = sU0 + p * US;
-    double* uc = sU + p * US;
+    const double* u0 = sU0 + p * nv;
+    double* uc = sU + p * nv;
     if (a.stage == 0) {
 #pragma unroll
       for (int v = 0; v < 8; ++v) un[v] = v < nv ? u0[v] + dts * Lr[v] : 0.0;
@@ -1079,10 +1226,10 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   const double* Fm = ops.filt[ct];
   dmma_product(
       S, 5 * nc, S, [&](int s, int j) { return __ldg(Fm + s * S + j); },
-      [&](int j, int col) { return sU[((col / 5) * S + j) * US + col % 5]; },
+      [&](int j, int col) { return sU[((col / 5) * S + j) * nv + col % 5]; },
       [&](int s, int col, double x) { sOut[((col / 5) * S + s) * nv + col % 5] = x; });
   for (int p = tid; p < nc * S; p += blockDim.x)
-    for (int v = 5; v < nv; ++v) sOut[p * nv + v] = sU[p * US + v];
+    for (int v = 5; v < nv; ++v) sOut[p * nv + v] = sU[p * nv + v];
   __syncthreads();
   for (int t = tid; t < nc * S * nv; t += blockDim.x) a.Unext[(size_t)e0 * S * nv + t] = sOut[t];
   if (a.stage == 0 && tid < nc) {

@@ -210,8 +210,9 @@ class B200GPUFRSolver(_solver_base()):
     The numerics are those of the reference's CPU path (``FRSolver.step``),
     the parity target: local time steps with the CPU path's own CFL rule
     (core/fr_solver/cfl.py:96-134), so ``cfl`` is accepted for the signature
-    and must be positive; ``time_scheme`` must be "ssp_rk3".  The state starts
-    as the uniform free stream along x, as ``GPUFRSolver`` does.
+    and must be positive; ``time_scheme`` is "ssp_rk3", "dual_time" or
+    "imex_euler" (other schemes raise AFR_EUNSUPPORTED).  The state starts as
+    the uniform free stream along x, as ``GPUFRSolver`` does.
 
     Extra keyword arguments: ``wall_distance`` (required with SST),
     ``precision`` ("fp64" or "mixed"), ``inviscid_only`` and
@@ -223,10 +224,9 @@ class B200GPUFRSolver(_solver_base()):
                  time_scheme: str = "ssp_rk3", cfl: float = 1.0, rho_inf: float = 1.225, vel_inf: float = 33.33,
                  p_inf: float = 101325.0, mu_molecular: float = 1.8e-5, boundary_ghost_provider=None,
                  turb_model: str = "NONE", *, wall_distance=None, precision: str = "fp64",
-                 inviscid_only: bool = False, global_dt_factor: float = 0.0, flat=None, cd_wall_face=None):
+                 inviscid_only: bool = False, global_dt_factor: float = 0.0, flat=None, cd_wall_face=None,
+                 dual_time_inner_iter: int = 20):
         turb = str(turb_model).upper()
-        if str(time_scheme).lower() != "ssp_rk3":
-            raise _unsupported(f"time scheme {time_scheme!r}: the device step is SSP-RK3")
         if not cfl > 0:
             raise ValueError("cfl must be positive")
         if int(order) != int(mesh.order):
@@ -241,8 +241,9 @@ class B200GPUFRSolver(_solver_base()):
                            cd_wall_face=cd_wall_face)
         super().__init__(case, turb_model_name=turb, mu_molecular=mu_molecular, rho_inf=rho_inf, vel_inf=vel_inf,
                          p_inf=p_inf, inviscid_only=inviscid_only, global_dt_factor=global_dt_factor,
-                         precision=precision, device=f"cuda:{int(device_id)}")
+                         precision=precision, device=f"cuda:{int(device_id)}", time_scheme=time_scheme,
+                         dual_time_inner_iter=dual_time_inner_iter)
         self.mesh, self.ops = mesh, ops
         self.device_id = int(device_id)
         self.boundary_ghost_provider = boundary_ghost_provider
-        self.time_scheme, self.cfl = "ssp_rk3", float(cfl)
+        self.cfl = float(cfl)

@@ -65,12 +65,20 @@ class B200FRSolver:
         mixed_ignore_conditioning: build the mixed form even for operators
             whose row l1 norms exceed its FP32-accumulation bound (to measure
             its error there; refused by default).
+        time_scheme: "ssp_rk3" (steady local time stepping), "dual_time"
+            (BDF1/BDF2 physical steps by pseudo-time iteration) or
+            "imex_euler" (explicit inviscid, implicit viscous), as the
+            reference's TimeIntegrationScheme values
+            (core/time_integration/base.py).
+        dual_time_inner_iter: pseudo-time iterations per physical step
+            (FRSolver ``dual_time_inner_iter``).
     """
 
     def __init__(self, case: Dict[str, np.ndarray], turb_model_name: str = "NONE", mu_molecular: float = 1.8e-5,
                  rho_inf: float = 1.225, vel_inf: float = 33.33, p_inf: float = 101325.0,
                  inviscid_only: bool = False, global_dt_factor: float = 0.0, precision: str = "fp64",
-                 device="cuda:0", mixed_ignore_conditioning: bool = False):
+                 device="cuda:0", mixed_ignore_conditioning: bool = False, time_scheme: str = "ssp_rk3",
+                 dual_time_inner_iter: int = 20):
         name = turb_model_name.upper()
         if name not in ("SST", "NONE"):
             raise ValueError(f"Unknown turbulence model: {turb_model_name}")
@@ -89,6 +97,11 @@ class B200FRSolver:
         prm.inviscid_only = 1 if inviscid_only else 0
         prm.mu, prm.rho_inf, prm.vel_inf, prm.p_inf = self.mu_molecular, rho_inf, vel_inf, p_inf
         prm.global_dt_factor = float(global_dt_factor)
+        scheme = str(getattr(time_scheme, "value", time_scheme)).lower()
+        if scheme not in ("ssp_rk3", "dual_time", "imex_euler"):
+            raise _lib.AfrError(_lib.AFR_EUNSUPPORTED, f"time scheme {time_scheme!r} is not built on the device")
+        self.time_scheme = scheme
+        self.dual_time_inner_iter = int(dual_time_inner_iter)
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -109,6 +122,8 @@ class B200FRSolver:
             self.nu_t = torch.zeros((N, S), dtype=torch.float64, device=self.device)
         self.initialize_uniform(rho_inf, vel_inf, 0.0, 0.0, p_inf)
         self.residual_history = []
+        self._U_prev = None        # dual time: state at the previous physical level
+        self._has_prev = False
 
     # ------------------------------------------------------------------ state
     def initialize_uniform(self, rho=1.0, u=0.0, v=0.0, w=0.0, p=1.0, k=1e-6, omega=1e-2):
@@ -179,21 +194,37 @@ class B200FRSolver:
 
     # ------------------------------------------------------------------- step
     def step(self, dt: float = 1e-3, want_norm: bool = True) -> float:
-        """FRSolver.step / GPUFRSolver.step: one SSP-RK3 step with local time
-        stepping (the ``dt`` argument is ignored, as in the reference's
-        steady SSP-RK mode, core/fr_solver/step.py:47-58).
+        """FRSolver.step / GPUFRSolver.step (core/fr_solver/step.py:15-221).
 
-        With ``want_norm`` the call synchronises and raises AfrError when the
-        step produced a non-finite value.  Without it nothing synchronises; a
-        non-finite value is raised by the next step once the device has
-        finished this one (or by ``status()``)."""
+        ssp_rk3: one SSP-RK3 step with local time stepping; ``dt`` is ignored,
+        as in the reference's steady mode (step.py:47-58).  With ``want_norm``
+        the call synchronises and raises AfrError when the step produced a
+        non-finite value.  Without it nothing synchronises; a non-finite value
+        is raised by the next step once the device has finished this one (or
+        by ``status()``).
+
+        dual_time: one physical step of size ``dt`` (BDF1 on the first step,
+        BDF2 after); imex_euler: one IMEX Euler step with the local time step.
+        Both synchronise."""
         norm = ctypes.c_double(0.0)
-        check(LIB.afr_step(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega), _dev_ptr(self.nu_t),
-                           ctypes.byref(norm) if want_norm else None, _stream()), self._h)
-        if want_norm:
-            self.residual_history.append(norm.value)
-            return norm.value
-        return float("nan")
+        if self.time_scheme == "dual_time":
+            if self._U_prev is None:
+                self._U_prev = torch.empty_like(self.U)
+            check(LIB.afr_step_dual_time(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega),
+                                         _dev_ptr(self.nu_t), _dev_ptr(self._U_prev), 1 if self._has_prev else 0,
+                                         float(dt), self.dual_time_inner_iter, 1e-4, ctypes.byref(norm), _stream()),
+                  self._h)
+            self._has_prev = True
+        elif self.time_scheme == "imex_euler":
+            check(LIB.afr_step_imex(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega),
+                                    _dev_ptr(self.nu_t), ctypes.byref(norm), _stream()), self._h)
+        else:
+            check(LIB.afr_step(self._h, _dev_ptr(self.U), _dev_ptr(self.k), _dev_ptr(self.omega),
+                               _dev_ptr(self.nu_t), ctypes.byref(norm) if want_norm else None, _stream()), self._h)
+            if not want_norm:
+                return float("nan")
+        self.residual_history.append(norm.value)
+        return norm.value
 
     def status(self, clear: bool = False) -> int:
         """Device status after the queued work (synchronises): 0 when every
@@ -245,6 +276,19 @@ class B200FRSolver:
         check(LIB.afr_cd_cl(self._h, _dev_ptr(self.U), _dev_ptr(self.nu_t), float(reference_area), out, _stream()),
               self._h)
         return {"Cd": out[0], "Cl": out[1], "Cs": out[2]}
+
+    def save_checkpoint(self, path: str, iteration: int, metadata: Optional[dict] = None) -> str:
+        """Write the device state (U, SST fields, dual-time level n-1, residual
+        history) in the reference's checkpoint layout (autoflowcfd_b200.checkpoint)."""
+        from . import checkpoint
+
+        return checkpoint.save_checkpoint(self, path, iteration, metadata=metadata)
+
+    def resume_from_checkpoint(self, path: str) -> int:
+        """Restore the device state from a checkpoint of the same case; returns its iteration."""
+        from . import checkpoint
+
+        return checkpoint.resume(self, path)
 
     def device_bytes(self) -> int:
         v = ctypes.c_uint64(0)

@@ -185,6 +185,31 @@ int afr_sst_update(afr_handle* h, const double* U, const double* dt_local, doubl
 int afr_step(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out,
              void* stream);
 
+/* One physical step of the dual-time scheme (DUAL_TIME,
+ * core/fr_solver/step.py:167-185 and core/time_integration/dual.py:19-158):
+ * the SST fields advance once with the physical step dt_physical; the mean
+ * flow solves the BDF-implicit equation (BDF1 when has_prev == 0, BDF2 with
+ * the previous level U_prev otherwise) by up to max_inner_iter pseudo-time
+ * SSP-RK3 iterations with the local time step and the reference's adaptive
+ * CFL factor (0.1 .. 10), stopping when the dual residual dropped 1e-6
+ * relative, fell below tol (from the second iteration), or an update moved
+ * the state by less than 1e-10 (L2).  Positivity and the modal filter follow
+ * every stage and the pseudo step.  U (device) is advanced in place; U_prev
+ * (device, same shape, caller-owned) receives the state at the start of the
+ * step for the next call.  *norm_out (host, may be NULL) receives the RMS of
+ * the spatial dU/dt at the start of the step.  Synchronises (the iteration's
+ * control flow reads norms); not for stream capture. */
+int afr_step_dual_time(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* U_prev,
+                       int32_t has_prev, double dt_physical, int32_t max_inner_iter, double tol, double* norm_out,
+                       void* stream);
+
+/* One step of the IMEX Euler scheme (IMEX_EULER, core/fr_solver/step.py:186-193
+ * and core/time_integration/imex.py:17-97): the inviscid residual at the start
+ * of the step is explicit, the viscous residual implicit, solved by up to five
+ * damped Picard iterations (damping 0.5, adapted between 0.1 and 1) with the
+ * local time step and positivity; SST as in afr_step.  Synchronises. */
+int afr_step_imex(afr_handle* h, double* U, double* k, double* omega, double* nu_t, double* norm_out, void* stream);
+
 /* Device status of the handle after the work queued on stream (synchronises;
  * not inside a stream capture): AFR_OK, AFR_ENONFINITE, AFR_EINDEX or AFR_ECUDA
  * (a tensor-core wait ran out).  With nseg > 0, seg_status[i] receives the

@@ -794,6 +794,10 @@ class Solver:
     wall_distance: Optional[np.ndarray] = None
     inviscid_only: bool = False
     global_dt_factor: float = 0.0
+    time_scheme: str = "ssp_rk3"
+    dt_step: float = 1e-3            # physical step of the dual-time scheme
+    dual_time_inner_iter: int = 20
+    U_prev: Optional[np.ndarray] = None  # dual time: state at the previous physical level
 
     def mu_t(self, Q):
         """get_turbulent_viscosity_field, core/fr_solver/turbulence.py:355-366."""
@@ -811,8 +815,114 @@ class Solver:
             full[:, :, :5] += viscous_residual(self.m, U, self.mu, self.mu_t(Q))
         return -full
 
+    def _parts(self, U):
+        """(inviscid, viscous) residuals dU/dt of U, zero turbulence columns."""
+        Q = state_primitives(U)
+        Ri = np.zeros_like(U)
+        Rv = np.zeros_like(U)
+        Ri[:, :, :5] = inviscid_residual(self.m, U)
+        if not self.inviscid_only:
+            Rv[:, :, :5] = viscous_residual(self.m, U, self.mu, self.mu_t(Q))
+        return Ri, Rv
+
+    def _ssp_rk3(self, U0, rfun, dtc, residual0):
+        """TimeIntegrator._ssp_rk_stage_step with the RK3 table and the filter,
+        core/time_integration/base.py:250-335; rfun(U) -> R (dU/dt = -R)."""
+        m = self.m
+        N, S, nv = self.U.shape
+        L0 = -residual0
+        U1 = U0 + dtc * L0
+        enforce_positivity(U1)
+        U1 = modal_filter(m, U1.reshape(N, S, nv)).reshape(N * S, nv)
+        L1 = -rfun(U1)
+        U2 = 0.75 * U0 + 0.25 * U1 + 0.25 * dtc * L1
+        enforce_positivity(U2)
+        U2 = modal_filter(m, U2.reshape(N, S, nv)).reshape(N * S, nv)
+        L2 = -rfun(U2)
+        U3 = 1.0 / 3.0 * U0 + 0.0 * U1 + 2.0 / 3.0 * U2 + 2.0 / 3.0 * dtc * L2
+        enforce_positivity(U3)
+        return modal_filter(m, U3.reshape(N, S, nv)).reshape(N * S, nv)
+
+    def _dual_time(self, U_flat, dt_local, dt_phys):
+        """step_dual_time, core/time_integration/dual.py:19-158."""
+        N, S, nv = self.U.shape
+        U_n = U_flat
+        U_tau = U_n.copy()
+        prev = self.U_prev
+
+        def spatial(Uf):
+            return self.residual(Uf.reshape(N, S, nv)).reshape(N * S, nv)
+
+        if prev is None:
+            def dual(Uf):
+                return spatial(Uf) + (Uf - U_n) / dt_phys
+        else:
+            def dual(Uf):
+                return spatial(Uf) + (3.0 * Uf - 4.0 * U_n + prev) / (2.0 * dt_phys)
+
+        init = np.linalg.norm(dual(U_tau))
+        cfl = 0.1
+        prev_norm = None
+        for k in range(self.dual_time_inner_iter):
+            R = dual(U_tau)
+            cur = np.linalg.norm(R)
+            if cur < init * 1e-6:
+                break
+            if k >= 1 and cur < 1e-4:
+                break
+            if k > 0:
+                ratio = cur / prev_norm
+                if ratio < 0.5:
+                    cfl = min(cfl * 1.5, 10.0)
+                elif ratio > 1.0:
+                    cfl = max(cfl * 0.5, 0.1)
+            prev_norm = cur
+            dtc = (dt_local * cfl)[:, None]
+            U_next = self._ssp_rk3(U_tau, dual, dtc, R)
+            enforce_positivity(U_next)
+            U_next = modal_filter(self.m, U_next.reshape(N, S, nv)).reshape(N * S, nv)
+            if np.linalg.norm(U_next - U_tau) < 1e-10:
+                break
+            U_tau = U_next
+        return U_tau
+
+    def _imex(self, U_flat, dt_local):
+        """step_imex, core/time_integration/imex.py:17-97."""
+        N, S, nv = self.U.shape
+        Ri, _ = self._parts(U_flat.reshape(N, S, nv))
+        R_exp = -Ri.reshape(N * S, nv)
+
+        def r_imp(Uf):
+            return -self._parts(Uf.reshape(N, S, nv))[1].reshape(N * S, nv)
+
+        U_new = U_flat.copy()
+        dt_vec = dt_local[:, None]
+        init = np.linalg.norm(R_exp + r_imp(U_flat))
+        damping, prev_norm = 0.5, None
+        for it in range(5):
+            total = R_exp + r_imp(U_new)
+            cur = np.linalg.norm(total)
+            if it > 0:
+                ratio = cur / prev_norm
+                if ratio < 0.5:
+                    damping = min(damping * 1.2, 1.0)
+                elif ratio > 1.0:
+                    damping = max(damping * 0.5, 0.1)
+            else:
+                damping = 0.5
+            prev_norm = cur
+            U_next = U_new - dt_vec * total * damping
+            enforce_positivity(U_next)
+            if np.linalg.norm(U_next - U_new) < 1e-8 or cur < init * 1e-6:
+                break
+            U_new = U_next
+        return U_new
+
     def step(self):
-        """FRSolver.step, core/fr_solver/step.py:15-221 (SSP-RK3 branch)."""
+        """FRSolver.step, core/fr_solver/step.py:15-221 (SSP-RK3, DUAL_TIME and
+        IMEX_EULER branches)."""
+        if self.time_scheme != "ssp_rk3":
+            return self._step_scheme()
         m = self.m
         N, S, nv = self.U.shape
         Q = state_primitives(self.U)
@@ -839,6 +949,26 @@ class Solver:
         enforce_positivity(U3)
         U3 = modal_filter(m, U3.reshape(N, S, nv)).reshape(N * S, nv)
         self.U = U3.reshape(N, S, nv)
+        return float(np.linalg.norm(dUdt) / np.sqrt(dUdt.size))
+
+    def _step_scheme(self):
+        m = self.m
+        N, S, nv = self.U.shape
+        Q = state_primitives(self.U)
+        dt = local_dt(m, Q, self.mu, self.mu_t(Q))
+        if self.global_dt_factor:
+            dt = np.full((N, S), self.global_dt_factor * float(np.min(dt)))
+        if self.turb is not None:
+            turb_dt = np.full((N, S), self.dt_step) if self.time_scheme == "dual_time" else dt
+            sst_source_and_update(m, self.U, Q, self.turb, turb_dt, self.mu, self.wall_distance)
+        U_flat = self.U.reshape(N * S, nv).copy()
+        dUdt = -self.residual(self.U).reshape(N * S, nv)
+        if self.time_scheme == "dual_time":
+            U_new = self._dual_time(U_flat, dt.reshape(N * S), self.dt_step)
+            self.U_prev = U_flat.copy()
+        else:
+            U_new = self._imex(U_flat, dt.reshape(N * S))
+        self.U = U_new.reshape(N, S, nv)
         return float(np.linalg.norm(dUdt) / np.sqrt(dUdt.size))
 
 
@@ -885,4 +1015,8 @@ def load_case(path):
         wd = case["wall_distance"]
     s = Solver(m, case["U0"].copy(), float(case["mu"]), turb, wd, bool(case["inviscid_only"]),
                float(case["global_dt_factor"]))
+    if "time_scheme" in case:
+        s.time_scheme = str(case["time_scheme"])
+        s.dt_step = float(case["dt_step"])
+        s.dual_time_inner_iter = int(case["dual_time_inner_iter"])
     return case, m, s

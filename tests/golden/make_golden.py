@@ -193,7 +193,8 @@ def op_tables(ops):
 
 
 def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_only=False,
-              global_dt_factor=None, n_steps=2, turb_init=None, plant=None, tweak_flat=None):
+              global_dt_factor=None, n_steps=2, turb_init=None, plant=None, tweak_flat=None,
+              time_scheme="ssp_rk3", dt_step=1e-3):
     """Run the reference on one small case and store its inputs and outputs.
 
     ``plant(U) -> U`` edits the full start state (all n_vars columns) after
@@ -213,7 +214,7 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
                        else "FARFIELD") for n in boxmesh.PLANE_NAMES}
     mesh = ref_mesh(box, order, mesh_bc)
     rho_inf, u_inf, p_inf = free
-    solver = FRSolver(mesh=mesh, order=order, turb_model_name=turb, time_scheme=TimeIntegrationScheme.SSP_RK3,
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name=turb, time_scheme=TimeIntegrationScheme(time_scheme),
                       rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf, mu_molecular=mu,
                       n_threads=min(8, os.cpu_count() or 1))
     solver.order_continuation_enabled = False
@@ -234,7 +235,9 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
                turb=np.array(turb), mu=np.float64(mu), freestream=np.array(free, float),
                inviscid_only=np.int32(inviscid_only), periodic=np.int32(box.periodic),
                global_dt_factor=np.float64(global_dt_factor or 0.0),
-               box_shape=np.array(box.shape), box_lengths=np.array(box.lengths), box_kind=np.array(box.kind))
+               box_shape=np.array(box.shape), box_lengths=np.array(box.lengths), box_kind=np.array(box.kind),
+               time_scheme=np.array(time_scheme), dt_step=np.float64(dt_step),
+               dual_time_inner_iter=np.int32(solver.time_integrator.dual_time_steps))
     out["det_jacs"] = mesh.jacobians["det_jacs"].reshape(N, S)
     out["inv_jacs"] = mesh.jacobians["inv_jacs"].reshape(N, S, 3, 3)
     Fn = mesh.n_sps_per_cell_fine
@@ -349,7 +352,7 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
     tib.enforce_positivity = positivity_spy
     norms = []
     for s in range(n_steps):
-        norms.append(solver.step(1e-3))
+        norms.append(solver.step(dt_step))
         out[f"U_step{s + 1}"] = solver.state.U.copy()
         if solver.turb_model is not None:
             out[f"k_step{s + 1}"] = solver.turb_model.k_field.copy()
@@ -618,9 +621,54 @@ def main(which=None):
                         lambda xyz: c3_tgv(xyz)[0], 12, inviscid_only=True, global_dt_factor=3.0,
                         sample_steps=(1,), stride=16)
 
+    def c_prism_p1_ns_scheme(scheme, dt_step):
+        Ls = (2.0, 1.0, 1.0)
+        box = boxmesh.prism_box(4, 3, 2, Ls, jitter=0.1, seed=5, bump=(0.05, 1.0, 0.5, 0.3))
+        rho, p = 1.225, 101325.0
+        u = 0.2 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e5
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        cfg["x_min"] = {"type": "INLET", "Q_inlet": Qf}
+        cfg["x_max"] = {"type": "OUTLET", "p_outlet": p}
+        cfg["y_min"] = {"type": "SYMMETRY"}
+        cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
+        make_case(f"prism_p1_ns_{scheme}", box, 1, "NONE", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 5), time_scheme=scheme, dt_step=dt_step,
+                  n_steps=3)
+
+    def c_prism_p2_sst_scheme(scheme, dt_step):
+        Ls = (4.0, 2.0, 1.5)
+        box = boxmesh.prism_box(4, 3, 3, Ls, jitter=0.1, seed=7)
+        rho, p = 1.225, 101325.0
+        u = 0.1 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e6
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        k_in = 1.5 * (0.01 * u) ** 2
+        w_in = rho * k_in / (10 * mu)
+
+        def turb_init(xyz):
+            rng = np.random.default_rng(3)
+            N, S = xyz.shape[:2]
+            pert = 1 + 0.2 * np.sin(2 * np.pi * xyz[..., 0] / Ls[0] + 0.3) * np.cos(np.pi * xyz[..., 2] / Ls[2])
+            k = k_in * pert
+            w = w_in * (1 + 0.3 * np.cos(2 * np.pi * xyz[..., 1] / Ls[1]))
+            nut = 10 * mu / rho * (1 + 0.5 * rng.uniform(size=(N, S)))
+            return k, w, nut
+
+        make_case(f"prism_p2_sst_{scheme}", box, 2, "SST", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 11), turb_init=turb_init,
+                  time_scheme=scheme, dt_step=dt_step, n_steps=2)
+
     cases = {"tet_p1_vortex": c_tet_p1, "prism_p2_sst": c_prism_p2_sst, "prism_p1_ns": c_prism_p1_ns,
              "tet_p3_tgv": c_tet_p3, "prism_p1_floors": c_prism_p1_floors, "tet_p1_align": c_tet_p1_align,
-             "traj_c1_vortex": t_c1, "traj_c2_sample": t_c2_sample, "traj_p3_tgv": t_p3}
+             "traj_c1_vortex": t_c1, "traj_c2_sample": t_c2_sample, "traj_p3_tgv": t_p3,
+             "prism_p1_ns_dual_time": lambda: c_prism_p1_ns_scheme("dual_time", 2e-5),
+             "prism_p1_ns_imex_euler": lambda: c_prism_p1_ns_scheme("imex_euler", 1e-3),
+             "prism_p2_sst_dual_time": lambda: c_prism_p2_sst_scheme("dual_time", 2e-5)}
     for k, fn in cases.items():
         if which and k not in which:
             continue
