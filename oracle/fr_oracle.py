@@ -342,9 +342,46 @@ def _color_faces(m: Mesh):
 # ---------------------------------------------------------------------------
 # residuals
 # ---------------------------------------------------------------------------
+def inviscid_residual_p0(m: Mesh, U):
+    """compute_inviscid_residual_fv_p0, core/fr_residual/inviscid_p0.py:18-85 with
+    the kernel core/fr_residual/inviscid_p0_kernel.py:25-108: finite volume at
+    order 0 -- per face record, AUSM+up between the owner's and the
+    neighbour's (or ghost) state along the unit normal, times the face area,
+    taken out of the owner and added to the neighbour (divided by the cell
+    volumes); no primary-flag filtering.  Faces are added in record order."""
+    N = m.N
+    Q = conserved_to_primitive(U[..., :5])[:, 0, :]
+    isb = m.c["is_boundary"].astype(bool)
+    own, nbr = m.c["owner_cell"], m.c["neighbor_cell"]
+    n = m.c["true_normal"][:, 0, :]
+    area = m.c["true_area_weight"][:, 0]
+    vol = m.c["cell_volumes"]
+    Qn = Q[np.where(isb, own, nbr)]
+    bf = np.flatnonzero(isb)
+    if len(bf):
+        # _precompute_ghost_states (inviscid_p0.py:112-143) stores the ghost
+        # state per owner CELL, overwritten face by face in record order: every
+        # boundary face of a cell uses the ghost state of that cell's last
+        # boundary face
+        G = ghost_states(m, Q[:, None, :], bf)[1][:, 0, :]
+        Gcell = np.zeros((N, 5))
+        Gcell[own[bf]] = G  # later faces overwrite earlier ones (numpy assigns in index order)
+        Qn[bf] = Gcell[own[bf]]
+    F = ausm_up(Q[own], Qn, n) * area[:, None]
+    R = np.zeros((N, 5))
+    for f in range(len(own)):
+        R[own[f]] -= F[f] * (1.0 / vol[own[f]])
+        if not isb[f]:
+            R[nbr[f]] += F[f] * (1.0 / vol[nbr[f]])
+    return R[:, None, :]
+
+
 def inviscid_residual(m: Mesh, U):
     """compute_inviscid_residual_fr, core/fr_residual/inviscid.py:139-345,
-    with the colored interface kernel core/fr_residual/inviscid_kernel_colored.py:43-236."""
+    with the colored interface kernel core/fr_residual/inviscid_kernel_colored.py:43-236
+    (order 0: the finite-volume path, inviscid.py:164-170)."""
+    if m.S == 1:
+        return inviscid_residual_p0(m, U)
     N, S = m.N, m.S
     Q = conserved_to_primitive(U[..., :5])
     det = m.c["det_jacs"]

@@ -8,7 +8,7 @@ import copy
 import numpy as np
 import pytest
 
-from conftest import CASES, CD_CASES, SCHEME_CASES, case_tol, golden_path
+from conftest import CASES, CD_CASES, P0_CASES, SCHEME_CASES, case_tol, golden_path
 from oracle import fr_oracle as O
 
 
@@ -16,7 +16,7 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + P0_CASES)
 def test_residuals_match_reference(name):
     case, m, s = O.load_case(golden_path(name))
     U = case["U0"]
@@ -43,7 +43,7 @@ def test_sst_source_transport_update_match_reference():
         assert rel(a, case[k]) < 1e-12, k
 
 
-@pytest.mark.parametrize("name", CASES + SCHEME_CASES)
+@pytest.mark.parametrize("name", CASES + SCHEME_CASES + P0_CASES)
 def test_steps_match_reference(name):
     case, m, s = O.load_case(golden_path(name))
     for i in range(len(case["norms"])):
