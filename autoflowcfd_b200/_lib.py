@@ -48,6 +48,7 @@ class AfrMeshDesc(ctypes.Structure):
         ("n_src_mats", ctypes.c_int32), ("src_mat_table", _P_D),
         ("nb_src0_mat_index", _P_I32), ("nb_src1_mat_index", _P_I32),
         ("ow_src0_mat_index", _P_I32), ("ow_src1_mat_index", _P_I32),
+        ("fv_cell_volumes", _P_D), ("metric_flux_scale", _P_D),
     ]
 
 
@@ -92,6 +93,8 @@ SIGNATURES = {
     "afr_tc_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]),
     "afr_greedy_face_coloring": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, _P_I64, _P_I64, _P_U8, _P_I32]),
+    "afr_prolong": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _P_D,
+                                   ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 
@@ -176,9 +179,13 @@ class MeshTables:
                     c[k + t] = np.ascontiguousarray(case[k + t], dtype=np.float64)
         if case.get("wall_distance") is not None:
             c["wall_distance"] = np.ascontiguousarray(case["wall_distance"], dtype=np.float64)
-        if case.get("cd_wall_face") is not None and case.get("true_area_weight") is not None:
-            c["cd_wall_face"] = np.ascontiguousarray(case["cd_wall_face"], dtype=np.uint8)
+        for k in ("fv_cell_volumes", "metric_flux_scale"):
+            if case.get(k) is not None:
+                c[k] = np.ascontiguousarray(case[k], dtype=np.float64)
+        if case.get("true_area_weight") is not None:
             c["true_area_weight"] = np.ascontiguousarray(case["true_area_weight"], dtype=np.float64)
+            if case.get("cd_wall_face") is not None:
+                c["cd_wall_face"] = np.ascontiguousarray(case["cd_wall_face"], dtype=np.uint8)
         self.c = c
         N = int(case["n_cells"])
         d = AfrMeshDesc()
@@ -215,4 +222,9 @@ class MeshTables:
         d.wall_distance = _ptr(c.get("wall_distance"), ctypes.c_double)
         d.cd_wall_face = _ptr(c.get("cd_wall_face"), ctypes.c_uint8)
         d.true_area_weight = _ptr(c.get("true_area_weight"), ctypes.c_double)
+        N_S = N * int(case["n_sps"])
+        for k, n in (("fv_cell_volumes", N), ("metric_flux_scale", N_S)):
+            if k in c and c[k].size != n:
+                raise ValueError(f"{k} has {c[k].size} values, expected {n}")
+            setattr(d, k, _ptr(c.get(k), ctypes.c_double))
         self.desc = d

@@ -19,6 +19,7 @@
 #include "../../include/afr_b200.h"
 #include "afr_implicit.cuh"
 #include "afr_mixed.cuh"
+#include "afr_p0.cuh"
 #include "afr_sst.cuh"
 
 using namespace afr;
@@ -59,6 +60,8 @@ struct afr_handle {
   unsigned* status_host = nullptr;
   cudaEvent_t status_ev = nullptr;
   bool status_pending = false;
+  // order 0 (finite volume): face tables and per-face flux scratch
+  P0Tab p0{};
   // mixed-precision form (prec == AFR_PREC_MIXED)
   int prec = AFR_PREC_FP64;
   MxOps mo{};
@@ -77,6 +80,7 @@ struct afr_handle {
   double* iUn = nullptr;     // (N,S,nv) state at the start of the physical step
   double* iX = nullptr;      // (N,S,nv) next iterate
   double* idt = nullptr;     // (N,S) physical time step of the dual-time SST update
+  double* wprol = nullptr;   // (64 x 64) interpolation matrix of afr_prolong, allocated by its first call
   std::vector<void*> allocs;
   size_t mat_elems[4] = {0, 0, 0, 0};  // doubles of each interpolation-matrix allocation (0: shares the first)
   uint64_t bytes = 0;
@@ -473,6 +477,39 @@ struct Launch {
   }
 };
 
+// Order 0: the finite-volume face kernel and the per-cell gather-and-update
+// kernel stand in for the three kernels of a stage.  Gradients (the force
+// integral's pre-pass) use the generic one-point kernels.
+struct LaunchP0 {
+  static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
+    k_pre<1><<<h->N, 32, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
+    return cudaGetLastError();
+  }
+  static cudaError_t eval(afr_handle* h, StageArgs a, const double* U, const double* nut, bool grads,
+                          cudaStream_t st, StepTimer* tm = nullptr, int* nl = nullptr) {
+    (void)grads;
+    if (tm) tm->mark(st);  // no pre-pass: an empty interval
+    k_p0_face<<<(h->F + 127) / 128, 128, 0, st>>>(h->g, h->fc, h->bc, h->p0, U, h->nv, nut, h->prm.mu,
+                                                  a.inviscid_only ? 0 : 1);
+    if (tm) tm->mark(st);
+    a.N = h->N;
+    k_p0_cell<<<(h->N + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->p0, a);
+    if (tm) tm->mark(st);
+    if (nl) *nl += 2;
+    return cudaGetLastError();
+  }
+  static cudaError_t sst(afr_handle*, const SstArgs&, cudaStream_t, StepTimer* = nullptr) {
+    return cudaErrorNotSupported;  // refused at create
+  }
+  static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
+    if (h->n_cd_faces == 0) return cudaSuccess;
+    k_force<1, 1><<<(h->n_cd_faces + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->cd_faces, h->n_cd_faces, U,
+                                                               h->nv, h->PF, nut, h->area_w, h->prm.mu, h->cd_part);
+    return cudaGetLastError();
+  }
+  static cudaError_t mx_grids(afr_handle*) { return cudaErrorNotSupported; }  // refused at create
+};
+
 // ---- host-side BF16 hi+lo operator images for the mixed form ----
 uint16_t bf16_bits(float f) {
   uint32_t u;
@@ -519,6 +556,7 @@ std::vector<uint16_t> kmajor_image_cat(int N, int K, Get get) {
 template <class Fn>
 cudaError_t dispatch(afr_handle* h, Fn&& fn) {
   switch (h->order) {
+    case 0: return fn(LaunchP0());
     case 1: return fn(Launch<8, 27, 4, 2>());
     case 2: return fn(Launch<27, 64, 9, 3>());
     case 3: return fn(Launch<64, 64, 16, 4>());
@@ -914,6 +952,47 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   return AFR_OK;
 }
 
+// Order-0 tables: per-cell face references in ascending record order, the
+// per-cell ghost face (the cell's last boundary face: the reference's ghost
+// table holds one state per owner cell, overwritten face by face), the
+// penalty code of owner-primary boundary faces and the face areas.
+static int p0_setup(afr_handle* h, const afr_mesh_desc* m, cudaStream_t st) {
+  const size_t N = h->N, F = h->F;
+  if (F >= ((size_t)1 << 30)) return fail(h, AFR_EUNSUPPORTED, "more than 2^30 faces");
+  std::vector<int32_t> ptr(N + 1, 0), last(N, -1), gface(F, -1), pen(F, 0);
+  for (size_t f = 0; f < F; ++f) {
+    const bool bnd = m->is_boundary[f] != 0;
+    ptr[m->owner_cell[f] + 1]++;
+    if (!bnd) ptr[m->neighbor_cell[f] + 1]++;
+    if (bnd) last[m->owner_cell[f]] = (int32_t)f;
+  }
+  for (size_t c = 0; c < N; ++c) ptr[c + 1] += ptr[c];
+  std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1), ref(ptr[N]);
+  std::vector<double> area(F);
+  for (size_t f = 0; f < F; ++f) {
+    const bool bnd = m->is_boundary[f] != 0;
+    ref[pos[m->owner_cell[f]]++] = (int32_t)(f << 1);
+    if (!bnd) ref[pos[m->neighbor_cell[f]]++] = (int32_t)((f << 1) | 1);
+    if (bnd) {
+      gface[f] = last[m->owner_cell[f]];
+      if (m->owner_is_primary[f])
+        pen[f] = 1 | ((int32_t)m->owner_axis[f] << 1) | (m->owner_side[f] > 0.0 ? 8 : 0);
+    }
+    area[f] = m->true_area_weight[f * (size_t)h->P];
+  }
+  int32_t *dptr, *dref, *dg, *dpen;
+  double *dA, *flux, *fvv;
+  int rc;
+  if ((rc = upload(h, &dptr, ptr.data(), N + 1, st)) || (rc = upload(h, &dref, ref.data(), ref.size(), st)) ||
+      (rc = upload(h, &dg, gface.data(), F, st)) || (rc = upload(h, &dpen, pen.data(), F, st)) ||
+      (rc = upload(h, &dA, area.data(), F, st)) || (rc = dalloc(h, &flux, F * 8)) ||
+      (rc = upload(h, &fvv, m->fv_cell_volumes ? m->fv_cell_volumes : m->cell_volumes, N, st)))
+    return rc;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail(h, AFR_ECUDA, "order-0 tables");
+  h->p0 = P0Tab{dptr, dref, dg, dpen, dA, fvv, flux};
+  return AFR_OK;
+}
+
 int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_handle** out) {
   if (!m || !prm || !out) return AFR_EINVAL;
   *out = nullptr;
@@ -934,9 +1013,15 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   h->prm = *prm;
   h->nv = prm->n_vars;
   const int n1d = h->order + 1;
-  if (h->order < 1 || h->order > 3) return bail(fail(h, AFR_EUNSUPPORTED, "order must be 1, 2 or 3"));
+  if (h->order < 0 || h->order > 3) return bail(fail(h, AFR_EUNSUPPORTED, "order must be 0, 1, 2 or 3"));
   if (prm->precision != AFR_PREC_FP64 && prm->precision != AFR_PREC_MIXED)
     return bail(fail(h, AFR_EINVAL, "precision must be AFR_PREC_FP64 or AFR_PREC_MIXED"));
+  if (h->order == 0 && prm->precision != AFR_PREC_FP64)
+    return bail(fail(h, AFR_EUNSUPPORTED, "order 0 (finite volume) runs in the FP64 form only"));
+  if (h->order == 0 && prm->turb == AFR_TURB_SST)
+    return bail(fail(h, AFR_EUNSUPPORTED, "order 0 (finite volume) supports laminar and inviscid flow"));
+  if (h->order == 0 && !m->true_area_weight)
+    return bail(fail(h, AFR_EINVAL, "order 0 needs true_area_weight (the face areas)"));
   const int fine_1d = std::min(2 * h->order, 3) + 1;
   if (h->S != n1d * n1d * n1d || h->P != n1d * n1d || h->Fn != fine_1d * fine_1d * fine_1d)
     return bail(fail(h, AFR_EINVAL, "n_sps/n_fp/n_fine inconsistent with order"));
@@ -1007,7 +1092,10 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     const size_t nf = N * Fn * 9, nc = N * S * 9;
     k_form_adj<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(detf, invf, adjf, N * Fn);
     k_form_adj<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(det, inv, adj, N * S);
-    k_metric_flux_scale<<<(unsigned)((N * S + 255) / 256), 256, 0, st>>>(adj, mfs, N * S);
+    if (m->metric_flux_scale)
+      cudaMemcpyAsync(mfs, m->metric_flux_scale, N * S * sizeof(double), cudaMemcpyHostToDevice, st);
+    else
+      k_metric_flux_scale<<<(unsigned)((N * S + 255) / 256), 256, 0, st>>>(adj, mfs, N * S);
     cudaError_t e = cudaStreamSynchronize(st);
     cudaFree(detf);
     cudaFree(invf);
@@ -1023,7 +1111,14 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   for (int t = 0; t < 2; ++t) {
     const bool present = t == 0 ? h->n_prism > 0 : h->N > h->n_prism;
     if (!present) continue;
-    if (!m->D_3d[t] || !m->c2f[t] || !m->D_fine[t] || !m->f2c[t] || !m->filter[t])
+    // order 0 has no over-integration operators: identity transfers and a
+    // zero derivative (the finite-volume kernels do not read them)
+    static const double one[1] = {1.0}, zero3[3] = {0.0, 0.0, 0.0};
+    const bool p0 = h->order == 0;
+    const double* c2f_h = m->c2f[t] ? m->c2f[t] : (p0 ? one : nullptr);
+    const double* dfn_h = m->D_fine[t] ? m->D_fine[t] : (p0 ? zero3 : nullptr);
+    const double* f2c_h = m->f2c[t] ? m->f2c[t] : (p0 ? one : nullptr);
+    if (!m->D_3d[t] || !c2f_h || !dfn_h || !f2c_h || !m->filter[t])
       return bail(fail(h, AFR_EINVAL, "missing operator for a present cell type"));
     double *d3, *d3g, *c2f, *dfn, *f2c, *flt;
     if ((rc = upload(h, &d3, m->D_3d[t], S * S * 3, st))) return bail(rc);
@@ -1033,16 +1128,16 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
         for (size_t j = 0; j < S; ++j) g2[(s * 3 + mm) * S + j] = m->D_3d[t][s * 3 * S + j * 3 + mm];
     if ((rc = upload(h, &d3g, g2.data(), g2.size(), st))) return bail(rc);
     cudaStreamSynchronize(st);
-    if ((rc = upload(h, &c2f, m->c2f[t], Fn * S, st))) return bail(rc);
-    if ((rc = upload(h, &dfn, m->D_fine[t], Fn * Fn * 3, st))) return bail(rc);
-    if ((rc = upload(h, &f2c, m->f2c[t], S * Fn, st))) return bail(rc);
+    if ((rc = upload(h, &c2f, c2f_h, Fn * S, st))) return bail(rc);
+    if ((rc = upload(h, &dfn, dfn_h, Fn * Fn * 3, st))) return bail(rc);
+    if ((rc = upload(h, &f2c, f2c_h, S * Fn, st))) return bail(rc);
     if ((rc = upload(h, &flt, m->filter[t], S * S, st))) return bail(rc);
     // W = f2c * D_fine (S x 3Fn), summed in ascending fine-point order
     std::vector<double> Wh(S * 3 * Fn, 0.0);
     for (size_t r = 0; r < S; ++r)
       for (size_t k = 0; k < 3 * Fn; ++k) {
         double acc = 0.0;
-        for (size_t i = 0; i < Fn; ++i) acc += m->f2c[t][r * Fn + i] * m->D_fine[t][i * 3 * Fn + k];
+        for (size_t i = 0; i < Fn; ++i) acc += f2c_h[r * Fn + i] * dfn_h[i * 3 * Fn + k];
         Wh[r * 3 * Fn + k] = acc;
       }
     double* wdev;
@@ -1221,8 +1316,8 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
       return bail(rc);
     cudaStreamSynchronize(st);
     h->slots = SlotTable{(int32_t)ns, d_f, d_c, d_fl, d_0, d_1, d_i1};
-    // FP64 jumps: the plain stage only
-    if (prm->precision != AFR_PREC_MIXED && (rc = dalloc(h, &h->J, ns * P * 10))) return bail(rc);
+    // FP64 jumps: the plain stage of orders 1-3 only
+    if (prm->precision != AFR_PREC_MIXED && h->order > 0 && (rc = dalloc(h, &h->J, ns * P * 10))) return bail(rc);
   }
   // ---- boundary condition table ----
   {
@@ -1267,6 +1362,7 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = dalloc(h, &h->sp8, N * S * 8))) return bail(rc);
   }
   if (prm->precision == AFR_PREC_MIXED && (rc = mixed_setup(h, m, Wkeep, st))) return bail(rc);
+  if (h->order == 0 && (rc = p0_setup(h, m, st))) return bail(rc);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "afr_create"));
   *out = h;
@@ -1427,6 +1523,7 @@ int imp_norm(afr_handle* h, const ImpArgs& a, int mode, cudaStream_t st, double*
 
 int filter_cells(afr_handle* h, double* U, cudaStream_t st) {
   switch (h->order) {
+    case 0: k_filter_cells<1><<<h->N, 32, 0, st>>>(h->g, h->ops, U, h->nv); break;
     case 1: k_filter_cells<8><<<h->N, 64, 0, st>>>(h->g, h->ops, U, h->nv); break;
     case 2: k_filter_cells<27><<<h->N, 160, 0, st>>>(h->g, h->ops, U, h->nv); break;
     default: k_filter_cells<64><<<h->N, 320, 0, st>>>(h->g, h->ops, U, h->nv); break;
@@ -1615,6 +1712,22 @@ float time_eval(afr_handle* h, const double* U, const double* nut, double* Rinv,
   return best;
 }
 
+// new[c, a, v] = sum_b W[a, b] * old[c, b, v], b ascending; one thread per output
+__global__ void k_prolong(const double* __restrict__ old, int so, const double* __restrict__ W, int sn, int nc,
+                          int64_t N, double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * sn * nc) return;
+  const int v = (int)(i % nc);
+  const int64_t r = i / nc;
+  const int a = (int)(r % sn);
+  const int64_t c = r / sn;
+  const double* u = old + c * so * nc + v;
+  const double* w = W + (size_t)a * so;
+  double acc = 0.0;
+  for (int b = 0; b < so; ++b) acc += w[b] * u[(size_t)b * nc];
+  out[i] = acc;
+}
+
 __global__ void k_segment_sums(const double* __restrict__ part, const int64_t* __restrict__ ptr, double* out) {
   __shared__ double sh[256];
   double acc = 0.0;
@@ -1792,6 +1905,30 @@ int afr_step_profile(afr_handle* h, double* U, double* k, double* omega, double*
     }
   for (int i = 0; i < 24; ++i) cudaEventDestroy(tm.ev[i]);
   return rc;
+}
+
+int afr_prolong(afr_handle* h, const double* old_field, int32_t n_sps_old, int32_t n_cols, const double* W,
+                double* new_field, void* stream) {
+  if (!h || !old_field || !W || !new_field) return AFR_EINVAL;
+  if (n_sps_old < 1 || n_sps_old > 64 || n_cols < 1 || n_cols > 8)
+    return fail(h, AFR_EINVAL, "prolong: n_sps_old must be 1..64 and n_cols 1..8");
+  const size_t n_old = (size_t)h->N * n_sps_old * n_cols, n_new = (size_t)h->N * h->S * n_cols;
+  const uintptr_t o = reinterpret_cast<uintptr_t>(old_field), nw = reinterpret_cast<uintptr_t>(new_field);
+  if (o < nw + n_new * sizeof(double) && nw < o + n_old * sizeof(double))
+    return fail(h, AFR_EINVAL, "prolong: old and new fields overlap");
+  int rc;
+  if (!h->wprol && (rc = dalloc(h, &h->wprol, 64 * 64))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(h->wprol, W, (size_t)h->S * n_sps_old * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "prolong matrix");
+  if (n_new > 0)
+    k_prolong<<<(unsigned)((n_new + 255) / 256), 256, 0, st>>>(old_field, n_sps_old, h->wprol, h->S, n_cols,
+                                                                (int64_t)h->N, new_field);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(h, e, "prolong");
+  // W may be pageable memory the caller frees on return: finish the copy
+  e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? AFR_OK : cuda_fail(h, e, "prolong");
 }
 
 int afr_cd_cl(afr_handle* h, const double* U, const double* nu_t, double reference_area, double* out3, void* stream) {

@@ -174,13 +174,15 @@ def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, fla
 
         flat = get_flat_face_geometry(mesh, ops)
     N, S = int(mesh.n_cells), int(mesh.n_sps_per_cell)
-    Fn = int(mesh.n_sps_per_cell_fine)
+    # order 0 has no over-integration points: the one solution point stands in
+    fine = mesh.jacobians_fine if getattr(mesh, "jacobians_fine", None) is not None else mesh.jacobians
+    Fn = int(mesh.n_sps_per_cell_fine) if getattr(mesh, "jacobians_fine", None) is not None else S
     out = dict(order=np.int32(mesh.order), n_cells=np.int32(N), n_prism=np.int32(mesh.n_prism_cells),
                n_sps=np.int32(S), n_fine=np.int32(Fn))
     out["det_jacs"] = np.asarray(mesh.jacobians["det_jacs"], float).reshape(N, S)
     out["inv_jacs"] = np.asarray(mesh.jacobians["inv_jacs"], float).reshape(N, S, 3, 3)
-    out["det_jacs_fine"] = np.asarray(mesh.jacobians_fine["det_jacs"], float).reshape(N, Fn)
-    out["inv_jacs_fine"] = np.asarray(mesh.jacobians_fine["inv_jacs"], float).reshape(N, Fn, 3, 3)
+    out["det_jacs_fine"] = np.asarray(fine["det_jacs"], float).reshape(N, Fn)
+    out["inv_jacs_fine"] = np.asarray(fine["inv_jacs"], float).reshape(N, Fn, 3, 3)
     out["cell_volumes"] = np.asarray(mesh.get_all_cell_volumes(), float)
     out.update(op_tables(ops))
     out.update(flat_tables(flat))

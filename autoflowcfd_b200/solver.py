@@ -36,6 +36,15 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def _metric_flux_scale(case) -> np.ndarray:
+    """(N, S) sum_m |adj(J)[m,:]| of a case's solution points
+    (_get_metric_flux_scale, core/fr_solver/solver_geometry.py:18-32)."""
+    N, S = int(case["n_cells"]), int(case["n_sps"])
+    adj = np.asarray(case["det_jacs"], float).reshape(N, S)[..., None, None] * \
+        np.asarray(case["inv_jacs"], float).reshape(N, S, 3, 3)
+    return np.sum(np.linalg.norm(adj, axis=-1), axis=-1)
+
+
 @dataclass
 class SolverResult:
     """core/fr_solver/state.py:12-17."""
@@ -72,25 +81,30 @@ class B200FRSolver:
             (core/time_integration/base.py).
         dual_time_inner_iter: pseudo-time iterations per physical step
             (FRSolver ``dual_time_inner_iter``).
+        case_for_order: ``order -> case`` giving the same mesh's tables at a
+            lower order; with it ``solve`` runs the reference's order
+            continuation for order >= 2 (FRSolver.solve,
+            core/fr_solver/solver.py:270-323), P0 -> P1 -> ... -> order.
     """
 
     def __init__(self, case: Dict[str, np.ndarray], turb_model_name: str = "NONE", mu_molecular: float = 1.8e-5,
                  rho_inf: float = 1.225, vel_inf: float = 33.33, p_inf: float = 101325.0,
                  inviscid_only: bool = False, global_dt_factor: float = 0.0, precision: str = "fp64",
                  device="cuda:0", mixed_ignore_conditioning: bool = False, time_scheme: str = "ssp_rk3",
-                 dual_time_inner_iter: int = 20):
+                 dual_time_inner_iter: int = 20, case_for_order=None):
         name = turb_model_name.upper()
         if name not in ("SST", "NONE"):
             raise ValueError(f"Unknown turbulence model: {turb_model_name}")
         self.device = torch.device(device)
         self.turb_model_name = name
         self.n_cells = int(case["n_cells"])
-        self.n_sps = int(case["n_sps"])
         self.order = int(case["order"])
+        self.current_order = self.order
+        self.case_for_order = case_for_order
+        self.order_continuation_enabled = case_for_order is not None
         self.n_vars = 7 if name == "SST" else 5
         self.mu_molecular = float(mu_molecular)
         self.freestream = {"rho_inf": rho_inf, "vel_inf": vel_inf, "p_inf": p_inf}
-        self._tables = _lib.MeshTables(case)
         prm = _lib.AfrParams()
         prm.n_vars = self.n_vars
         prm.turb = _lib.AFR_TURB_SST if name == "SST" else _lib.AFR_TURB_NONE
@@ -108,22 +122,92 @@ class B200FRSolver:
         prm.precision = _lib.AFR_PREC_MIXED if precision == "mixed" else _lib.AFR_PREC_FP64
         prm.mixed_ignore_conditioning = 1 if mixed_ignore_conditioning else 0
         self._prm = prm
-        h = ctypes.c_void_p()
-        with torch.cuda.device(self.device):
-            check(LIB.afr_create(ctypes.byref(self._tables.desc), ctypes.byref(prm), _stream(), ctypes.byref(h)))
-        self._h = h
-        N, S = self.n_cells, self.n_sps
-        self.U = torch.zeros((N, S, self.n_vars), dtype=torch.float64, device=self.device)
-        self.k = self.omega = self.nu_t = None
-        if name == "SST":
-            # SSTModelFR initial fields, core/turbulence/sst.py:46-49
-            self.k = torch.full((N, S), 1e-6, dtype=torch.float64, device=self.device)
-            self.omega = torch.ones((N, S), dtype=torch.float64, device=self.device)
-            self.nu_t = torch.zeros((N, S), dtype=torch.float64, device=self.device)
+        self._h = None
+        # the mesh's cell volumes at its load order (the order-0 finite-volume
+        # divisor of an order continuation) and the metric flux scale the
+        # continuation's later phases reuse
+        self._fv_volumes = np.asarray(case["fv_cell_volumes"] if case.get("fv_cell_volumes") is not None
+                                      else case["cell_volumes"], float)
+        self._mfs_cache = None
+        self._open(case)
         self.initialize_uniform(rho_inf, vel_inf, 0.0, 0.0, p_inf)
         self.residual_history = []
+
+    def _open(self, case: Dict[str, np.ndarray]):
+        """Create the device handle of ``case`` (tables copied to HBM) and
+        fresh state fields of its size; releases the previous handle."""
+        tables = _lib.MeshTables(case)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(LIB.afr_create(ctypes.byref(tables.desc), ctypes.byref(self._prm), _stream(), ctypes.byref(h)))
+        self.cleanup()
+        self._tables, self._h = tables, h
+        self.current_order = int(case["order"])
+        self.n_sps = N_S = int(case["n_sps"])
+        N = self.n_cells
+        self.U = torch.zeros((N, N_S, self.n_vars), dtype=torch.float64, device=self.device)
+        self.k = self.omega = self.nu_t = None
+        if self.turb_model_name == "SST":
+            # SSTModelFR initial fields, core/turbulence/sst.py:46-49
+            self.k = torch.full((N, N_S), 1e-6, dtype=torch.float64, device=self.device)
+            self.omega = torch.ones((N, N_S), dtype=torch.float64, device=self.device)
+            self.nu_t = torch.zeros((N, N_S), dtype=torch.float64, device=self.device)
         self._U_prev = None        # dual time: state at the previous physical level
         self._has_prev = False
+
+    # ------------------------------------------------------ order continuation
+    def _case_at(self, order: int) -> Dict[str, np.ndarray]:
+        if self.case_for_order is None:
+            raise ValueError("order continuation needs case_for_order (the mesh's tables at lower orders)")
+        case = self.case_for_order(order)
+        if int(case["order"]) != order or int(case["n_cells"]) != self.n_cells:
+            raise ValueError(f"case_for_order({order}) returned order {int(case['order'])} with "
+                             f"{int(case['n_cells'])} cells (expected {self.n_cells})")
+        return case
+
+    def _phase_case(self, order: int) -> Dict[str, np.ndarray]:
+        """The tables of one continuation phase with the two quantities the
+        reference carries over from earlier phases: the load-order cell
+        volumes (its P0 finite-volume divisor, inviscid_p0.py:44-51) and the
+        metric flux scale cached by the first phase, broadcast over the
+        points (solver_geometry.py:18-32, cfl.py:136-146)."""
+        case = dict(self._case_at(order))
+        if case.get("fv_cell_volumes") is None:
+            case["fv_cell_volumes"] = self._fv_volumes
+        if self._mfs_cache is None:
+            self._mfs_cache = _metric_flux_scale(case)
+        else:
+            S = int(case["n_sps"])
+            c = self._mfs_cache
+            case["metric_flux_scale"] = np.ascontiguousarray(
+                np.broadcast_to(c, (self.n_cells, S)) if c.shape[1] in (1, S) else np.tile(c, (1, -(-S // c.shape[1])))[:, :S])
+        return case
+
+    def _restart_at_p0(self):
+        """run_order_continuation's restart (core/utils/order_continuation.py:236-288):
+        the uniform free stream on a P0 handle (SST fields at their initial values)."""
+        self._mfs_cache = None
+        self._open(self._phase_case(0))
+        f = self.freestream
+        self.initialize_uniform(f["rho_inf"], f["vel_inf"], 0.0, 0.0, f["p_inf"])
+
+    def _change_order(self, new_order: int, W: np.ndarray):
+        """Prolong U (and k, omega, nu_t) with W (new_n_sps x old_n_sps) onto a
+        handle of ``new_order``; the dual-time history is dropped
+        (interpolate_to_new_order_checked, core/utils/order_continuation.py:180-205)."""
+        old = {"U": self.U, "k": self.k, "omega": self.omega, "nu_t": self.nu_t}
+        s_old = self.n_sps
+        self._open(self._phase_case(new_order))
+        Wc = np.ascontiguousarray(W, dtype=np.float64)
+        if Wc.shape != (self.n_sps, s_old):
+            raise ValueError(f"prolongation matrix {Wc.shape} != ({self.n_sps}, {s_old})")
+        for name, src in old.items():
+            dst = getattr(self, name)
+            if src is None or dst is None:
+                continue
+            cols = src.shape[2] if src.dim() == 3 else 1
+            check(LIB.afr_prolong(self._h, _dev_ptr(src.contiguous()), s_old, cols,
+                                  Wc.ctypes.data_as(_lib._P_D), _dev_ptr(dst), _stream()), self._h)
 
     # ------------------------------------------------------------------ state
     def initialize_uniform(self, rho=1.0, u=0.0, v=0.0, w=0.0, p=1.0, k=1e-6, omega=1e-2):
@@ -252,9 +336,19 @@ class B200FRSolver:
                                     _stream()), self._h)
         return float(out[0])
 
-    def solve(self, max_iter: int = 1000, dt: float = 1e-3, tol: float = 1e-6, output_interval: int = 0) -> dict:
+    def solve(self, max_iter: int = 1000, dt: float = 1e-3, tol: float = 1e-6, output_interval: int = 0,
+              checkpoint_callback=None) -> dict:
         """GPUFRSolver.solve (core/gpu/gpu_solver.py:403-453): stops on tol or a
-        non-finite norm."""
+        non-finite norm.  With ``case_for_order`` and order >= 2 it runs the
+        order continuation of FRSolver.solve instead (its SolverResult fields,
+        plus the residual history)."""
+        if self.order_continuation_enabled and self.order >= 2:
+            from .continuation import run_order_continuation
+
+            log = print if output_interval else None
+            r = run_order_continuation(self, max_iter, dt, tol, checkpoint_callback, log)
+            return {"converged": r.converged, "iterations": r.iterations, "final_residual": r.final_residual,
+                    "residual_history": list(self.residual_history)}
         res = float("inf")
         it = 0
         converged = False

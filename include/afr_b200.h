@@ -21,6 +21,8 @@
  *   afr_step                FRSolver.step, core/fr_solver/step.py:15-221
  *                           (GPU form: GPUFRSolver.step, core/gpu/gpu_solver.py:295-401)
  *   afr_cd_cl               compute_aerodynamic_coefficients_fr, postprocess/fr_coefficients.py:27-152
+ *   afr_prolong             interpolate_to_new_order (order continuation),
+ *                           core/utils/order_continuation.py:62-124
  *   afr_destroy             GPUFRSolver.cleanup, core/gpu/gpu_solver_io.py:20-35
  *
  * Conventions: every call returns an int status (AFR_OK = 0).  Arrays passed
@@ -74,7 +76,11 @@ enum { AFR_BC_WALL = 0, AFR_BC_FARFIELD = 1, AFR_BC_INLET = 2, AFR_BC_OUTLET = 3
 typedef struct afr_handle afr_handle;
 
 /* Mesh, operators and face tables, as flattened by the reference
- * (core/fr_operators/face_kernels.py:124-187).  All host pointers. */
+ * (core/fr_operators/face_kernels.py:124-187).  All host pointers.
+ * order 0 is the reference's finite-volume path (one point per cell,
+ * core/fr_residual/inviscid_p0.py:18-85): n_sps = n_fine = n_fp = 1, the FP64
+ * form, laminar or inviscid; c2f, D_fine and f2c may be NULL there (the
+ * reference has none) and true_area_weight is required (the face areas). */
 typedef struct afr_mesh_desc {
   int32_t n_cells, n_prism, order, n_sps, n_fine, n_fp, n_faces;
   int32_t n_nb_src1, n_ow_src1; /* rows of the compact second-source tables */
@@ -122,7 +128,7 @@ typedef struct afr_mesh_desc {
   const double* bc_p_out;       /* (n_bc) */
   /* force integration (optional) */
   const uint8_t* cd_wall_face;      /* (F) or NULL */
-  const double* true_area_weight;   /* (F,P) or NULL */
+  const double* true_area_weight;   /* (F,P); NULL allowed above order 0 without forces */
   /* optional indexed form of the interpolation matrices: when src_mat_table
    * is non-NULL the four *_mat arrays above are ignored and record f's
    * matrix is src_mat_table[*_mat_index[f]]; the library keeps the table on
@@ -134,6 +140,20 @@ typedef struct afr_mesh_desc {
   const int32_t* nb_src1_mat_index; /* (n_nb_src1) */
   const int32_t* ow_src0_mat_index; /* (F) */
   const int32_t* ow_src1_mat_index; /* (n_ow_src1) */
+  /* optional fields of a solver whose order changed (order continuation,
+   * core/utils/order_continuation.py:207-425), NULL otherwise:
+   * fv_cell_volumes   (N) divisor of the order-0 finite-volume residual: the
+   *                   mesh's cell_volumes attribute, computed once at the
+   *                   order the mesh was loaded at (inviscid_p0.py:44-51),
+   *                   while cell_volumes above is the current order's
+   *                   (high_order_mesh.py:335-354, the local-dt length);
+   * metric_flux_scale (N,S) geometric local-dt scale sum_m |adj(J)[m,:]|:
+   *                   the reference caches it at its first evaluation and
+   *                   reuses it, broadcast over the points, while the cell
+   *                   count is unchanged (solver_geometry.py:18-32); NULL
+   *                   forms it from this order's Jacobians */
+  const double* fv_cell_volumes;
+  const double* metric_flux_scale;
 } afr_mesh_desc;
 
 typedef struct afr_params {
@@ -308,6 +328,19 @@ int afr_residual_sums(afr_handle* h, double* out2, void* stream);
  * mixed-precision kernels on one CTA and synchronises the stream.  No
  * counterpart in the reference (diagnostic for the mixed-precision form). */
 int afr_tc_check(int n, int k, const void* A, const void* B, float* D, void* stream);
+
+/* Order continuation: prolong a field of the same mesh held at a lower order
+ * (n_sps_old points per cell) to this handle's order,
+ *   new[c, a, v] = sum_b W[a, b] * old[c, b, v]   (b ascending),
+ * the np.einsum("ab,cbv->cav") of interpolate_to_new_order
+ * (core/utils/order_continuation.py:62-124).  W is a HOST (n_sps x
+ * n_sps_old) row-major matrix (the reference's trilinear interpolation
+ * matrix between the two Gauss-Legendre tensor grids, formed by the caller);
+ * old is (n_cells, n_sps_old, n_cols) and new (n_cells, n_sps, n_cols) on the
+ * device, n_cols 1..8, not overlapping.  The first call allocates a small
+ * matrix buffer on the handle; W is copied before the call returns. */
+int afr_prolong(afr_handle* h, const double* old_field, int32_t n_sps_old, int32_t n_cols, const double* W,
+                double* new_field, void* stream);
 
 /* Bytes of device memory the handle owns (tables + scratch). */
 int afr_device_bytes(const afr_handle* h, uint64_t* out);

@@ -355,7 +355,9 @@ def inviscid_residual_p0(m: Mesh, U):
     own, nbr = m.c["owner_cell"], m.c["neighbor_cell"]
     n = m.c["true_normal"][:, 0, :]
     area = m.c["true_area_weight"][:, 0]
-    vol = m.c["cell_volumes"]
+    # mesh.cell_volumes: computed at the order the mesh was loaded at (the
+    # target order during an order continuation), not the current order's
+    vol = m.c["fv_cell_volumes"] if "fv_cell_volumes" in m.c else m.c["cell_volumes"]
     Qn = Q[np.where(isb, own, nbr)]
     bf = np.flatnonzero(isb)
     if len(bf):
@@ -556,10 +558,14 @@ def local_dt(m: Mesh, Q, mu, mu_t):
     dt_adv = CFL * fa * hx / wave
     mu_eff = mu + mu_t if mu_t is not None else np.full_like(rho, mu)
     dt_visc = 0.25 * CFL * fv * rho * hx**2 / np.maximum(mu_eff, 1e-30)
-    adj = m.extras["adj"]
-    mfs = np.sum(np.linalg.norm(adj, axis=-1), axis=-1)
+    mfs = metric_flux_scale(m) if "mfs" not in m.extras else m.extras["mfs"]
     dt_geo = CFL * np.abs(m.c["det_jacs"]) / np.maximum(mfs * wave, 1e-300)
     return np.minimum(np.minimum(dt_adv, dt_visc), dt_geo)
+
+
+def metric_flux_scale(m: Mesh):
+    """_get_metric_flux_scale, core/fr_solver/solver_geometry.py:18-32: sum_m |adj(J)[m,:]|."""
+    return np.sum(np.linalg.norm(m.extras["adj"], axis=-1), axis=-1)
 
 
 def modal_filter(m: Mesh, U):
@@ -1038,6 +1044,94 @@ def cd_cl(m: Mesh, U, mu, nut, freestream, reference_area=1.0):
     q = 0.5 * rho_inf * vel_inf**2
     den = max(q * reference_area, 1e-300)
     return np.array([F[0] / den, F[2] / den, F[1] / den])
+
+
+# ---------------------------------------------------------------------------
+# order continuation
+# ---------------------------------------------------------------------------
+def interp_matrix_3d(old_1d, new_1d):
+    """_build_linear_interp_matrix_3d, core/utils/order_continuation.py:14-60:
+    column k is scipy's RegularGridInterpolator(method="linear",
+    fill_value=None) of the k-th unit vector on the old tensor grid, at the
+    new grid's points (meshgrid "ij", first coordinate slowest)."""
+    from scipy.interpolate import RegularGridInterpolator
+
+    n_old, n_new = len(old_1d), len(new_1d)
+    X, Y, Z = np.meshgrid(new_1d, new_1d, new_1d, indexing="ij")
+    pts = np.column_stack([X.ravel(), Y.ravel(), Z.ravel()])
+    W = np.zeros((n_new**3, n_old**3))
+    for k in range(n_old**3):
+        e = np.zeros(n_old**3)
+        e[k] = 1.0
+        f = RegularGridInterpolator((old_1d, old_1d, old_1d), e.reshape(n_old, n_old, n_old), method="linear",
+                                    bounds_error=False, fill_value=None)
+        W[:, k] = f(pts)
+    return W
+
+
+def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max_iter, dt, tol):
+    """run_order_continuation, core/utils/order_continuation.py:207-425, on
+    the oracle's solver: restart from the uniform free stream at P0
+    (FRState.initialize_uniform, core/fr_solver/state.py:50-74), phases
+    P0..order of max_iter // (order + 1) steps, phase tolerance
+    tol * 10**(order - p), an early move on after >= 20 steps once the
+    residual dropped 100x, the state prolonged between phases by
+    np.einsum("ab,cbv->cav", W, U) (interpolate_to_new_order, :62-124).
+
+    Returns (step_order, step_residual, states, result): ``states`` maps
+    "U_start_p<p>" / "U_end_p<p>" to the phase's first and last states."""
+    rho, u, p = freestream
+    c0 = case_for_order(0)
+    N = int(c0["n_cells"])
+    e = p / ((GAMMA - 1.0) * rho) + 0.5 * (u**2 + 0.0**2 + 0.0**2)
+    U = np.zeros((N, 1, 5))
+    U[:, :, 0], U[:, :, 1], U[:, :, 2], U[:, :, 3], U[:, :, 4] = rho, rho * u, rho * 0.0, rho * 0.0, rho * e
+    orders = list(range(0, order + 1))
+    step_order, step_res, states = [], [], {}
+    total, final = 0, 1e10
+    cur = 0
+    # the solver caches the metric flux scale at its first local time step
+    # (the P0 phase) and reuses it, broadcast over the points, while the cell
+    # count is unchanged (solver_geometry.py:18-32, cfl.py:136-146)
+    mfs_cache = None
+    for tp in orders:
+        if tp > 0:
+            W = interp_matrix_3d(np.polynomial.legendre.leggauss(cur + 1)[0], np.polynomial.legendre.leggauss(tp + 1)[0])
+            U = np.einsum("ab,cbv->cav", W, U)
+            cur = tp
+        mesh = Mesh.from_case(case_for_order(tp))
+        if mfs_cache is None:
+            mfs_cache = metric_flux_scale(mesh)
+        mesh.extras["mfs"] = np.broadcast_to(mfs_cache, (mesh.N, mesh.S)) if mfs_cache.shape[1] in (1, mesh.S) \
+            else np.tile(mfs_cache, (1, -(-mesh.S // mfs_cache.shape[1])))[:, :mesh.S]
+        s = Solver(mesh, U, mu, None, None, inviscid_only, 0.0)
+        states[f"U_start_p{tp}"] = s.U.copy()
+        phase_max, phase_tol = max_iter // len(orders), tol * (10 ** (order - tp))
+        init, converged = None, False
+        for i in range(phase_max):
+            res = s.step()
+            final = res
+            total += 1
+            step_order.append(tp)
+            step_res.append(res)
+            if init is None:
+                init = res
+            if res < phase_tol:
+                converged = True
+                break
+            if tp < order and i >= 20 and init > 0 and init / max(res, 1e-30) >= 1e2:
+                break
+        U = s.U
+        states[f"U_end_p{tp}"] = U.copy()
+        if tp == order and converged:
+            return step_order, step_res, states, (True, total, final)
+    return step_order, step_res, states, (False, total, final)
+
+
+def case_from_prefix(case, prefix):
+    """The tables a continuation fixture stores for one phase (keys
+    ``<prefix><name>``), as a case of their own."""
+    return {k[len(prefix):]: case[k] for k in case if k.startswith(prefix)}
 
 
 def load_case(path):

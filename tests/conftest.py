@@ -27,7 +27,7 @@ P0_CASES = ["prism_p0_ns", "tet_p0_vortex"]
 # steps of the dual-time (BDF1 then BDF2) and IMEX Euler schemes
 SCHEME_CASES = ["prism_p1_ns_dual_time", "prism_p1_ns_imex_euler", "prism_p2_sst_dual_time"]
 # cases with a wall force integral in their fixture
-CD_CASES = ["prism_p2_sst", "prism_p1_ns", "prism_p1_floors"]
+CD_CASES = ["prism_p2_sst", "prism_p1_ns", "prism_p1_floors", "prism_p0_ns"]
 
 
 def case_tol(name):

@@ -192,6 +192,42 @@ def op_tables(ops):
     )
 
 
+def mesh_tables(mesh, solver, mesh_bc):
+    """The mesh, operator, face and boundary tables of the solver's current
+    order, as the device path consumes them."""
+    N, S = mesh.n_cells, mesh.n_sps_per_cell
+    out = dict(order=np.int32(mesh.order), n_cells=np.int32(N), n_prism=np.int32(mesh.n_prism_cells),
+               n_sps=np.int32(S), n_fine=np.int32(mesh.n_sps_per_cell_fine))
+    out["det_jacs"] = mesh.jacobians["det_jacs"].reshape(N, S)
+    out["inv_jacs"] = mesh.jacobians["inv_jacs"].reshape(N, S, 3, 3)
+    Fn = mesh.n_sps_per_cell_fine
+    if mesh.jacobians_fine is None:  # order 0: no over-integration points (the inviscid flux is finite volume)
+        Fn = S
+        out["n_fine"] = np.int32(S)
+        out["det_jacs_fine"] = out["det_jacs"].copy()
+        out["inv_jacs_fine"] = out["inv_jacs"].copy()
+    else:
+        out["det_jacs_fine"] = mesh.jacobians_fine["det_jacs"].reshape(N, Fn)
+        out["inv_jacs_fine"] = mesh.jacobians_fine["inv_jacs"].reshape(N, Fn, 3, 3)
+    out["cell_volumes"] = mesh.get_all_cell_volumes()
+    # the P0 finite-volume divisor: volumes computed at the mesh's load order
+    out["fv_cell_volumes"] = np.asarray(mesh.cell_volumes, float)
+    out["sps_coords"] = mesh.sps_coords.reshape(N, S, 3)
+    out["nodes"] = mesh._node_coords
+    out["conn"] = (mesh._fixed_prism_conn if mesh.n_prism_cells else mesh._fixed_tet_conn).astype(np.int64)
+    out.update(op_tables(solver.ops))
+    out.update(flat_tables(mesh, solver.ops))
+    out.update(bc_tables(solver.boundary_ghost_provider, mesh.face_connectivity.n_faces))
+    out["true_area_weight"] = np.asarray(mesh.face_flux_points.true_area_weight, float)
+    if mesh_bc is not None:
+        from autoflowcfd.grid.connectivity.face_connectivity import tag_boundary_groups
+
+        gcode, name_to_code = tag_boundary_groups(mesh.face_connectivity, mesh.boundary_groups)
+        wall_codes = [c for n, c in name_to_code.items() if mesh.boundary_bc_types.get(n) == "WALL"]
+        out["cd_wall_face"] = np.isin(gcode, wall_codes).astype(np.uint8)
+    return out
+
+
 def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_only=False,
               global_dt_factor=None, n_steps=2, turb_init=None, plant=None, tweak_flat=None,
               time_scheme="ssp_rk3", dt_step=1e-3):
@@ -238,31 +274,8 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
                box_shape=np.array(box.shape), box_lengths=np.array(box.lengths), box_kind=np.array(box.kind),
                time_scheme=np.array(time_scheme), dt_step=np.float64(dt_step),
                dual_time_inner_iter=np.int32(solver.time_integrator.dual_time_steps))
-    out["det_jacs"] = mesh.jacobians["det_jacs"].reshape(N, S)
-    out["inv_jacs"] = mesh.jacobians["inv_jacs"].reshape(N, S, 3, 3)
-    Fn = mesh.n_sps_per_cell_fine
-    if mesh.jacobians_fine is None:  # order 0: no over-integration points (the inviscid flux is finite volume)
-        Fn = S
-        out["n_fine"] = np.int32(S)
-        out["det_jacs_fine"] = out["det_jacs"].copy()
-        out["inv_jacs_fine"] = out["inv_jacs"].copy()
-    else:
-        out["det_jacs_fine"] = mesh.jacobians_fine["det_jacs"].reshape(N, Fn)
-        out["inv_jacs_fine"] = mesh.jacobians_fine["inv_jacs"].reshape(N, Fn, 3, 3)
-    out["cell_volumes"] = mesh.get_all_cell_volumes()
-    out["sps_coords"] = xyz
-    out["nodes"] = mesh._node_coords
-    out["conn"] = (mesh._fixed_prism_conn if mesh.n_prism_cells else mesh._fixed_tet_conn).astype(np.int64)
-    out.update(op_tables(solver.ops))
-    out.update(flat_tables(mesh, solver.ops))
-    out.update(bc_tables(solver.boundary_ghost_provider, mesh.face_connectivity.n_faces))
-    out["true_area_weight"] = np.asarray(mesh.face_flux_points.true_area_weight, float)
-    if mesh_bc is not None:
-        from autoflowcfd.grid.connectivity.face_connectivity import tag_boundary_groups
-
-        gcode, name_to_code = tag_boundary_groups(mesh.face_connectivity, mesh.boundary_groups)
-        wall_codes = [c for n, c in name_to_code.items() if mesh.boundary_bc_types.get(n) == "WALL"]
-        out["cd_wall_face"] = np.isin(gcode, wall_codes).astype(np.uint8)
+    out.update(mesh_tables(mesh, solver, mesh_bc))
+    Fn = int(out["n_fine"])
 
     if turb == "SST":
         nodes = mesh._node_coords
@@ -384,6 +397,67 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(f"{name}: N={N} S={S} faces={len(out['owner_cell'])} colors={out['colors'].max() + 1} "
           f"norms={norms}", flush=True)
+    return out
+
+
+def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1e-3, inviscid_only=False):
+    """Run the reference's FRSolver.solve at ``order`` >= 2, which runs its
+    order continuation (core/utils/order_continuation.py:207-425), and store
+    every phase's tables (keys ``p<order>/<table>``, as that phase's mesh
+    and operators give them), each step's order and residual, the state at
+    the start and end of every phase and the SolverResult."""
+    import numba
+    from autoflowcfd.core.fr_solver import FRSolver
+
+    numba.set_num_threads(min(8, os.cpu_count() or 1))
+    mesh_bc = None
+    if plane_cfg is not None:
+        mesh_bc = {n: ("WALL" if plane_cfg[n]["type"] == "WALL" and plane_cfg[n].get("is_no_slip", True)
+                       else "FARFIELD") for n in boxmesh.PLANE_NAMES}
+    mesh = ref_mesh(box, order, mesh_bc)
+    rho_inf, u_inf, p_inf = free
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name="NONE", rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf,
+                      mu_molecular=mu, n_threads=min(8, os.cpu_count() or 1))
+    assert solver.order_continuation_enabled
+    if not box.periodic:
+        solver.boundary_ghost_provider = plane_provider(mesh, box, plane_cfg)
+    if inviscid_only:
+        solver.compute_viscous_residual = lambda *a, **k: np.zeros_like(solver.state.U)
+    out = dict(meta_name=np.array(name), order=np.int32(order), n_cells=np.int32(mesh.n_cells),
+               n_vars=np.int32(solver.state.n_vars), turb=np.array("NONE"), mu=np.float64(mu),
+               freestream=np.array(free, float), inviscid_only=np.int32(inviscid_only),
+               periodic=np.int32(box.periodic), global_dt_factor=np.float64(0.0),
+               max_iter=np.int32(max_iter), tol=np.float64(tol), dt=np.float64(dt))
+    real_step = solver.step
+    log_order, log_res = [], []
+
+    def step(dt_):
+        p = solver.current_order
+        if f"U_start_p{p}" not in out:
+            for k, v in mesh_tables(solver.mesh, solver, mesh_bc).items():
+                if v is not None and not (isinstance(v, np.ndarray) and v.dtype == object):
+                    out[f"p{p}/{k}"] = v
+            out[f"U_start_p{p}"] = solver.state.U.copy()
+        r = real_step(dt_)
+        if f"p{p}/mfs_cache" not in out:
+            out[f"p{p}/mfs_cache"] = np.asarray(solver._metric_flux_scale_cache, float).copy()
+        log_order.append(p)
+        log_res.append(r)
+        out[f"U_end_p{p}"] = solver.state.U.copy()
+        return r
+
+    solver.step = step
+    res = solver.solve(max_iter=max_iter, dt=dt, tol=tol)
+    out["step_order"] = np.array(log_order, np.int32)
+    out["step_residual"] = np.array(log_res)
+    out["result"] = np.array([float(res.converged), float(res.iterations), float(res.final_residual)])
+    out["U_final"] = solver.state.U.copy()
+    for k, v in out.items():
+        if isinstance(v, np.ndarray) and v.dtype.kind == "f":
+            assert np.all(np.isfinite(v)), f"{name}: non-finite reference output {k}"
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: N={mesh.n_cells} phases={sorted(set(log_order))} steps={len(log_res)} "
+          f"result={out['result']}", flush=True)
     return out
 
 
@@ -698,13 +772,42 @@ def main(which=None):
                   lambda x, y, z: vortex_state(x, y, L, L, 0.2 * L, rho, p, u),
                   inviscid_only=True, global_dt_factor=3.0, n_steps=3)
 
+    def k_cont_prism_p2():
+        """Order continuation P0 -> P1 -> P2 on a small wall-bump box (all five
+        boundary types), a few steps per phase."""
+        Ls = (1.5, 1.0, 1.0)
+        box = boxmesh.prism_box(3, 2, 2, Ls, jitter=0.1, seed=5, bump=(0.05, 0.75, 0.5, 0.3))
+        rho, p = 1.225, 101325.0
+        u = 0.2 * np.sqrt(GAMMA * p / rho)
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        cfg["x_min"] = {"type": "INLET", "Q_inlet": Qf}
+        cfg["x_max"] = {"type": "OUTLET", "p_outlet": p}
+        cfg["y_min"] = {"type": "SYMMETRY"}
+        cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
+        make_continuation("cont_prism_p2_ns", box, 2, rho * u / 1e5, (rho, u, p), cfg, max_iter=12, tol=1e-6)
+
+    def k_cont_tet_p2():
+        """Order continuation on a periodic box from the uniform free stream:
+        the residual (rounding of the free-stream preservation: ~4e-8 at P0,
+        ~4e-5 at P1, ~1.5 at P2) is under every phase tolerance at its first
+        step, so each phase converges at once and the run returns converged."""
+        L = 1.0
+        box = boxmesh.tet_box(2, 2, 2, (L, L, L), jitter=0.0, periodic=True)
+        rho, p = 1.225, 101325.0
+        u = 0.5 * np.sqrt(GAMMA * p / rho)
+        make_continuation("cont_tet_p2_uniform", box, 2, 1.8e-5, (rho, u, p), None, max_iter=30, tol=2.0,
+                          inviscid_only=True)
+
     cases = {"tet_p1_vortex": c_tet_p1, "prism_p2_sst": c_prism_p2_sst, "prism_p1_ns": c_prism_p1_ns,
              "tet_p3_tgv": c_tet_p3, "prism_p1_floors": c_prism_p1_floors, "tet_p1_align": c_tet_p1_align,
              "traj_c1_vortex": t_c1, "traj_c2_sample": t_c2_sample, "traj_p3_tgv": t_p3,
              "prism_p1_ns_dual_time": lambda: c_prism_p1_ns_scheme("dual_time", 2e-5),
              "prism_p1_ns_imex_euler": lambda: c_prism_p1_ns_scheme("imex_euler", 1e-3),
              "prism_p2_sst_dual_time": lambda: c_prism_p2_sst_scheme("dual_time", 2e-5),
-             "prism_p0_ns": c_prism_p0_ns, "tet_p0_vortex": c_tet_p0_vortex}
+             "prism_p0_ns": c_prism_p0_ns, "tet_p0_vortex": c_tet_p0_vortex,
+             "cont_prism_p2_ns": k_cont_prism_p2, "cont_tet_p2_uniform": k_cont_tet_p2}
     for k, fn in cases.items():
         if which and k not in which:
             continue

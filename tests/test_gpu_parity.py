@@ -7,7 +7,7 @@ conftest.case_tol)."""
 import numpy as np
 import pytest
 
-from conftest import CASES, case_tol, golden_path
+from conftest import CASES, P0_CASES, case_tol, golden_path
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,7 @@ def make_solver(case, **kw):
     return s
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + P0_CASES)
 def test_residuals_and_dt(golden, name):
     case = golden(name)
     s = make_solver(case, global_dt_factor=0.0)
@@ -55,7 +55,7 @@ def test_sst_update(golden):
     s.cleanup()
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + P0_CASES)
 def test_steps(golden, name):
     case = golden(name)
     s = make_solver(case)

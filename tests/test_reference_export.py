@@ -29,15 +29,17 @@ def _reference_available():
 
 
 @pytest.mark.skipif(not _reference_available(), reason="the reference checkout is not installed here")
-def test_exporter_reproduces_the_golden_tables():
-    """prism_p1_ns: a wall-bump box with WALL / FARFIELD / INLET / OUTLET /
-    SYMMETRY / slip-wall planes, exported from the reference's HighOrderMesh,
-    FROperators and BoundaryGhostStateProvider by the product code."""
+@pytest.mark.parametrize("order", [1, 0])
+def test_exporter_reproduces_the_golden_tables(order):
+    """prism_p1_ns / prism_p0_ns: a wall-bump box with WALL / FARFIELD / INLET /
+    OUTLET / SYMMETRY / slip-wall planes, exported from the reference's
+    HighOrderMesh, FROperators and BoundaryGhostStateProvider by the product
+    code (order 0: no over-integration points or operators)."""
     import make_golden as mg
     from autoflowcfd.core.fr_solver import FRSolver
     from autoflowcfd_b200 import boxmesh
 
-    g = np.load(golden_path("prism_p1_ns"))
+    g = np.load(golden_path(f"prism_p{order}_ns"))
     Ls = (2.0, 1.0, 1.0)
     box = boxmesh.prism_box(4, 3, 2, Ls, jitter=0.1, seed=5, bump=(0.05, 1.0, 0.5, 0.3))
     rho, p = 1.225, 101325.0
@@ -51,8 +53,8 @@ def test_exporter_reproduces_the_golden_tables():
     cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
     mesh_bc = {n: ("WALL" if cfg[n]["type"] == "WALL" and cfg[n].get("is_no_slip", True) else "FARFIELD")
                for n in boxmesh.PLANE_NAMES}
-    mesh = mg.ref_mesh(box, 1, mesh_bc)
-    solver = FRSolver(mesh=mesh, order=1, turb_model_name="NONE", rho_inf=rho, vel_inf=u, p_inf=p,
+    mesh = mg.ref_mesh(box, order, mesh_bc)
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name="NONE", rho_inf=rho, vel_inf=u, p_inf=p,
                       mu_molecular=float(g["mu"]), n_threads=1)
     provider = mg.plane_provider(mesh, box, cfg)
     case = export_case(mesh, solver.ops, provider)
