@@ -232,7 +232,8 @@ def build_case(box: BoxMesh, order: int, plane_cfg: Optional[dict] = None, wall_
     for k in ("D_3d_prism", "D_3d_tet", "c2f_prism", "c2f_tet", "Dfine_prism", "Dfine_tet", "f2c_prism",
               "f2c_tet", "filter_prism", "filter_tet", "boundary_extrap", "g_left", "g_right", "dist_fp_of_sp",
               "dist_axis_coord_of_sp"):
-        case[k] = T[k]
+        if k in T:  # order 0 has no over-integration operators
+            case[k] = T[k]
     # ---- face records replayed from the template ----
     n = np.array(box.shape)
     H = box.hex_index

@@ -156,6 +156,8 @@ def harvest(kind, order):
     fine, wf = gauss_legendre(nf1)
     out.update(sps_1d=sps, w_1d=w, fine_1d=fine, w_fine_1d=wf)
     path = os.path.join(HERE, f"tmpl_{kind}_p{order}.npz")
+    # operators the reference does not build at this order (None at P0) are left out
+    out = {k: v for k, v in out.items() if v is not None}
     np.savez_compressed(path, **out)
     print(f"{path}: records={R} unique matrices={len(table)} size={os.path.getsize(path) / 1e6:.2f} MB", flush=True)
 

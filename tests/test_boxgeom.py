@@ -17,6 +17,9 @@ BOXES = {
     "prism_p2_sst": lambda: boxmesh.prism_box(4, 3, 3, (4.0, 2.0, 1.5), jitter=0.1, seed=7),
     "prism_p1_ns": lambda: boxmesh.prism_box(4, 3, 2, (2.0, 1.0, 1.0), jitter=0.1, seed=5, bump=(0.05, 1.0, 0.5, 0.3)),
     "tet_p1_vortex": lambda: boxmesh.tet_box(3, 3, 3, (1.0, 1.0, 1.0), jitter=0.0, periodic=True),
+    # order 0 (finite volume): the same boxes as prism_p1_ns and tet_p1_vortex
+    "prism_p0_ns": lambda: boxmesh.prism_box(4, 3, 2, (2.0, 1.0, 1.0), jitter=0.1, seed=5, bump=(0.05, 1.0, 0.5, 0.3)),
+    "tet_p0_vortex": lambda: boxmesh.tet_box(3, 3, 3, (1.0, 1.0, 1.0), jitter=0.0, periodic=True),
 }
 
 
