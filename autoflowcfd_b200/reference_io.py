@@ -184,6 +184,8 @@ def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, fla
     out["det_jacs_fine"] = np.asarray(fine["det_jacs"], float).reshape(N, Fn)
     out["inv_jacs_fine"] = np.asarray(fine["inv_jacs"], float).reshape(N, Fn, 3, 3)
     out["cell_volumes"] = np.asarray(mesh.get_all_cell_volumes(), float)
+    if getattr(mesh, "cell_volumes", None) is not None:
+        out["fv_cell_volumes"] = np.asarray(mesh.cell_volumes, float)
     out.update(op_tables(ops))
     out.update(flat_tables(flat))
     out.update(lower_ghost_provider(boundary_ghost_provider, int(flat.n_faces)))
@@ -196,6 +198,30 @@ def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, fla
     if wall_distance is not None:
         out["wall_distance"] = np.asarray(wall_distance, float).reshape(N, S)
     return out
+
+
+def reference_case_for_order(mesh, boundary_ghost_provider=None, cd_wall_face=None):
+    """``order -> case`` over one reference ``HighOrderMesh``, for the order
+    continuation of ``B200FRSolver(case_for_order=...)``: switches the mesh to
+    that order (HighOrderMesh.set_order, as run_order_continuation does,
+    core/utils/order_continuation.py:330-345), exports its tables with that
+    order's operators (fr/operators.py generate_fr_operators) and switches the
+    mesh back.  The exported ``fv_cell_volumes`` is the mesh's cell_volumes
+    attribute, computed at its load order, which the reference divides the
+    order-0 finite-volume residual by."""
+    from autoflowcfd.fr.operators import generate_fr_operators
+
+    def case_for_order(order: int) -> Dict[str, np.ndarray]:
+        active = int(getattr(mesh, "_active_order", mesh.order))
+        mesh.set_order(order)
+        try:
+            ops = generate_fr_operators(order)
+            case = export_case(mesh, ops, boundary_ghost_provider, cd_wall_face=cd_wall_face)
+        finally:
+            mesh.set_order(active)
+        return case
+
+    return case_for_order
 
 
 def _solver_base():

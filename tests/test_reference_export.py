@@ -68,6 +68,43 @@ def test_exporter_reproduces_the_golden_tables(order):
         assert k in case
 
 
+@pytest.mark.skipif(not _reference_available(), reason="the reference checkout is not installed here")
+def test_case_for_order_reproduces_the_continuation_phases():
+    """reference_case_for_order over the reference's own P2 mesh gives, at
+    every order, the tables the reference's order continuation used in that
+    phase (cont_prism_p2_ns), including the load-order cell volumes."""
+    import make_golden as mg
+    from autoflowcfd_b200 import boxmesh
+    from autoflowcfd_b200.reference_io import reference_case_for_order
+
+    g = np.load(golden_path("cont_prism_p2_ns"))
+    Ls = (1.5, 1.0, 1.0)
+    box = boxmesh.prism_box(3, 2, 2, Ls, jitter=0.1, seed=5, bump=(0.05, 0.75, 0.5, 0.3))
+    rho, p = 1.225, 101325.0
+    u = 0.2 * np.sqrt(1.4 * p / rho)
+    Qf = [rho, u, 0.0, 0.0, p]
+    cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+    cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+    cfg["x_min"] = {"type": "INLET", "Q_inlet": Qf}
+    cfg["x_max"] = {"type": "OUTLET", "p_outlet": p}
+    cfg["y_min"] = {"type": "SYMMETRY"}
+    cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
+    mesh_bc = {n: ("WALL" if cfg[n]["type"] == "WALL" and cfg[n].get("is_no_slip", True) else "FARFIELD")
+               for n in boxmesh.PLANE_NAMES}
+    mesh = mg.ref_mesh(box, 2, mesh_bc)
+    case_for_order = reference_case_for_order(mesh, mg.plane_provider(mesh, box, cfg))
+    for order in (0, 1, 2):
+        case = case_for_order(order)
+        pre = f"p{order}/"
+        compared = 0
+        for k, v in case.items():
+            if pre + k in g.files and k != "cd_wall_face":
+                assert np.array_equal(np.asarray(v), g[pre + k]), (order, k)
+                compared += 1
+        assert compared >= 40 and "fv_cell_volumes" in case
+    assert int(mesh._active_order) == 2
+
+
 def _provider(cfgs, default, n_faces=4):
     return SimpleNamespace(group_code=np.array([0, -1, 1, -1][:n_faces]), code_to_config=cfgs,
                            default_config=default)
