@@ -647,6 +647,218 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def p0_algorithmic_bytes(case, nv=5):
+    """Minimum bytes each per-stage kernel of the order-0 path must move.
+
+    k_p0_face: per face record its owner / neighbour / ghost-face / penalty /
+    group indices, boundary flag, normal and area, the state once, and the
+    flux record it writes (8 doubles).
+    k_p0_cell: the flux records, the per-cell face references and slot lists,
+    volume, det and dt, the current and step-start state, the state it
+    writes and the two norm partials."""
+    N = int(case["n_cells"])
+    F = int(case["owner_cell"].shape[0])
+    isb = case["is_boundary"].astype(bool)
+    refs = F + int(np.sum(~isb))
+    slots = int(np.sum(case["owner_is_primary"].astype(bool))) + \
+        int(np.sum(~isb & case["neighbor_is_primary"].astype(bool)))
+    face = F * (4 * 5 + 1 + 24 + 8) + N * nv * 8 + F * 64
+    cell = F * 64 + (N + 1) * 4 * 2 + refs * 4 + slots * 4 + N * 8 * 3 + N * nv * 8 * 3 + N * 8 * 2
+    return {"k_p0_face": face, "k_p0_cell": cell}
+
+
+def _p0_setup(spec):
+    """Order-0 case of the C2 generator's box, laminar (the order-0 path has
+    no SST), with the C2 start state at the cell points."""
+    rho, u, p, mu, *_ = flow_conditions()
+    case = make_case(dict(spec, order=0))
+    U, *_ = initial_state(case, spec)
+    return case, np.ascontiguousarray(U[..., :5]), mu
+
+
+def p0_cpu_baseline(spec, max_seconds=25.0):
+    """The oracle's order-0 step (numpy restatement of the reference's
+    finite-volume path) on a bounded sample box."""
+    from oracle import fr_oracle as O
+
+    rho, u, p, mu, *_ = flow_conditions()
+    case = make_case(dict(spec, order=0), colorer=O.greedy_face_coloring)
+    U, *_ = initial_state(case, spec)
+    tab = case.pop("src_mat_table")
+    for key in ("nb_src0_mat", "nb_src1_mat", "ow_src0_mat", "ow_src1_mat"):
+        case[key] = tab[case.pop(key + "_index")]
+    s = O.Solver(O.Mesh.from_case(case), np.ascontiguousarray(U[..., :5]), mu)
+    N = s.U.shape[0]
+    s.step()
+    t0, n = time.perf_counter(), 0
+    while n < 20 and time.perf_counter() - t0 < max_seconds / 2:
+        s.step()
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": N * 5 * 3 * n / dt, "unit": UNIT, "cores": 1, "threads": _blas_threads(), "kind": "port",
+            "sample": f"{N} prisms P0 laminar ({spec['shape'][0]}x{spec['shape'][1]}x{spec['shape'][2]} hex), "
+                      f"{n} steps of the oracle's order-0 step (per-face Python loop, one core)"}
+
+
+def run_p0(args):
+    """Order 0 (the reference's finite-volume path, the first phase of its
+    order continuation): the C2 box at P0, 1,105,920 prisms, laminar
+    Navier-Stokes (wall + farfield), SSP-RK3 with local time stepping.
+    DOF-updates/s = n_cells * 5 * 3 per step; inputs larger than L2 (the
+    per-stage working set of face records and flux records is ~0.6 GB)."""
+    import tempfile
+
+    import torch
+
+    from autoflowcfd_b200 import profiling
+    from autoflowcfd_b200.solver import B200FRSolver
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = SMALL if args.small else FULL
+    t0 = time.perf_counter()
+    case, U, mu = _p0_setup(spec)
+    t_gen = time.perf_counter() - t0
+    rho, u, p, *_ = flow_conditions()
+    s = B200FRSolver(case, mu_molecular=mu, rho_inf=rho, vel_inf=u, p_inf=p, device=f"cuda:{local}")
+    s.set_state_from_cpu(U)
+    N = s.n_cells
+    stream = torch.cuda.current_stream()
+    start = s.U.clone()
+    for _ in range(max(args.warmup, 3)):
+        s.step(want_norm=False)
+    s.U.copy_(start)
+    clk_path = os.path.join(tempfile.gettempdir(), f"afr_bench_p0_clocks_{os.getpid()}.csv")
+    sampler = clocks_sampler(clk_path)
+    time.sleep(0.4 if sampler else 0.0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.step(want_norm=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.terminate()
+    ms = e0.elapsed_time(e1) / args.steps
+    s.status()
+    finite = bool(torch.isfinite(s.U).all().item())
+    # end to end through the public API: pinned host state in and out per step
+    host = torch.empty_like(s.U, device="cpu").pin_memory()
+    host.copy_(start.cpu())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        s.U.copy_(host, non_blocking=True)
+        s.step(want_norm=False)
+        host.copy_(s.U, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t1) * 1e3 / args.steps
+    s.U.copy_(start)
+    bd = profiling.step_breakdown(s)
+    s.cleanup()
+    alg = p0_algorithmic_bytes(case)
+    kern_ms = {"k_p0_face": bd["k_face_ms_per_launch"], "k_p0_cell": bd["k_cell_ms_per_launch"]}
+    per_kernel = {k: {"ms_per_launch": v, "algorithmic_bytes": alg[k], "achieved_gbs": alg[k] / (v * 1e-3) / 1e9}
+                  for k, v in kern_ms.items()}
+    dom = max(kern_ms, key=lambda k: kern_ms[k])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    dofs = N * 5 * 3
+    nbytes = N * 5 * 8
+    line = {
+        "metric": "DOF-updates/s, order 0 (finite volume)", "value": dofs / (ms * 1e-3), "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered mesh, C2 state)",
+        "config": {"workload": f"P0 laminar NS, C2 box {spec['shape'][0]}x{spec['shape'][1]}x{spec['shape'][2]} "
+                               f"hex -> {N} prisms, wall + farfield", "n_cells": N,
+                   "n_face_records": int(case["owner_cell"].shape[0]), "mesh_gen_s": round(t_gen, 1),
+                   "time_stepping": "SSP-RK3, local dt", "finite_after_timed_steps": finite,
+                   "l2": "inputs larger than L2 (face and flux records ~0.6 GB per stage)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_kernel[dom]["achieved_gbs"], "peak": hbm_peak,
+                     "unit": "GB/s", "frac": per_kernel[dom]["achieved_gbs"] / hbm_peak, "traffic": None,
+                     "per_kernel": per_kernel, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "breakdown_ms_per_step": bd["per_kernel_ms"], "gpu_launches": bd["launches_per_step"] * args.steps,
+        "e2e": {"value": dofs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = p0_cpu_baseline(SMALL if not args.small else SAMPLE)
+    clk = clocks_summary(clk_path, local)
+    if clk:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+
+
+def run_continuation(args):
+    """Order continuation as FRSolver.solve runs it for P >= 2
+    (core/utils/order_continuation.py:207-425): restart from the uniform free
+    stream at P0, then P0 -> P1 -> P2 with max_iter // 3 steps per phase, on
+    the C2 box (laminar: the order-0 path has no SST).  Reported: the solve's
+    wall time through B200FRSolver.solve (handles of each order built from
+    tables generated before the clock starts; device prolongation between
+    phases), each phase's steps and device time per step, and the residual at
+    every phase end."""
+    import torch
+
+    from autoflowcfd_b200 import boxgeom, boxmesh
+    from autoflowcfd_b200.solver import B200FRSolver
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = SMALL if args.small else FULL
+    rho, u, p, mu, *_ = flow_conditions()
+    box = boxmesh.prism_box(*spec["shape"], spec["lengths"], jitter=spec["jitter"], seed=spec["seed"])
+    t0 = time.perf_counter()
+    cases = {q: boxgeom.build_case(box, q, plane_cfg()) for q in (0, 1, 2)}
+    t_gen = time.perf_counter() - t0
+    s = B200FRSolver(cases[2], mu_molecular=mu, rho_inf=rho, vel_inf=u, p_inf=p, device=f"cuda:{local}",
+                     case_for_order=lambda q: cases[q])
+    max_iter = args.max_iter if args.max_iter != 20000 else 3 * args.steps
+    phase_ms = {0: 0.0, 1: 0.0, 2: 0.0}
+    phase_steps = {0: 0, 1: 0, 2: 0}
+    phase_end = {}
+    stream = torch.cuda.current_stream()
+    real_step = s.step
+    ev = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
+
+    def timed_step(dt=1e-3, want_norm=True):
+        ev[0].record(stream)
+        r = real_step(dt, want_norm)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        phase_ms[s.current_order] += ev[0].elapsed_time(ev[1])
+        phase_steps[s.current_order] += 1
+        phase_end[s.current_order] = r
+        return r
+
+    s.step = timed_step
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    res = s.solve(max_iter=max_iter, dt=1e-3, tol=1e-12)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t1
+    s.cleanup()
+    N = int(cases[2]["n_cells"])
+    line = {
+        "metric": "order continuation P0->P1->P2 solve wall time", "value": wall, "unit": "s",
+        "n_gpus": 1, "steps": int(res["iterations"]), "warmup": 0, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered mesh, uniform free stream start)",
+        "config": {"workload": f"order continuation to P2, laminar NS, C2 box {spec['shape'][0]}x{spec['shape'][1]}"
+                               f"x{spec['shape'][2]} hex -> {N} prisms", "max_iter": max_iter,
+                   "tables_gen_s_outside_clock": round(t_gen, 1)},
+        "phases": {f"P{q}": {"steps": phase_steps[q], "device_ms_per_step": phase_ms[q] / max(phase_steps[q], 1),
+                             "residual_at_end": phase_end.get(q)} for q in (0, 1, 2)},
+        "host_and_setup_s": wall - sum(phase_ms.values()) / 1e3,
+        "converged": res["converged"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """C5: serving loop (Poisson arrivals, HBM-gated admission, continuous batching)."""
     import torch
@@ -712,7 +924,7 @@ def main():
     ap.add_argument("--small", action="store_true", help="24x20x18 hex instead of 96x80x72 (profiling)")
     ap.add_argument("--shape", default=None, help="nx,ny,nz hex cells of a profiling-size box")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ensemble", "serve"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "ensemble", "serve", "p0", "continuation"])
     ap.add_argument("--mixed-opt-in", action="store_true",
                     help="c3: also build the mixed form past its conditioning bound and report its errors")
     ap.add_argument("--requests", type=int, default=32, help="serve: number of requests")
@@ -735,6 +947,12 @@ def main():
         return
     if args.workload == "c3":
         run_c3(args)
+        return
+    if args.workload == "p0":
+        run_p0(args)
+        return
+    if args.workload == "continuation":
+        run_continuation(args)
         return
 
     import torch
