@@ -93,6 +93,10 @@ SIGNATURES = {
     "afr_tc_check": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]),
     "afr_greedy_face_coloring": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, _P_I64, _P_I64, _P_U8, _P_I32]),
+    "afr_flux_point_jobs": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _P_D,
+                                           _P_I32, _P_I32, _P_D, _P_D, _P_D, ctypes.c_int64, _P_D, _P_D,
+                                           ctypes.c_int64] + [_P_I32] * 7 + [ctypes.POINTER(ctypes.c_uint32), _P_D,
+                                                                             _P_D, _P_D]),
     "afr_prolong": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _P_D,
                                    ctypes.c_void_p, ctypes.c_void_p]),
 }

@@ -21,6 +21,7 @@
  *   afr_step                FRSolver.step, core/fr_solver/step.py:15-221
  *                           (GPU form: GPUFRSolver.step, core/gpu/gpu_solver.py:295-401)
  *   afr_cd_cl               compute_aerodynamic_coefficients_fr, postprocess/fr_coefficients.py:27-152
+ *   afr_flux_point_jobs     build_face_flux_points (set-up), fr/face_flux_points_merge.py:51-434
  *   afr_prolong             interpolate_to_new_order (order continuation),
  *                           core/utils/order_continuation.py:62-124
  *   afr_destroy             GPUFRSolver.cleanup, core/gpu/gpu_solver_io.py:20-35
@@ -341,6 +342,35 @@ int afr_tc_check(int n, int k, const void* A, const void* B, float* D, void* str
  * matrix buffer on the handle; W is copied before the call returns. */
 int afr_prolong(afr_handle* h, const double* old_field, int32_t n_sps_old, int32_t n_cols, const double* W,
                 double* new_field, void* stream);
+
+/* Flux-point construction (set-up; no handle).  Each job locates the flux
+ * points of one face side on the other side's cell and forms that side's
+ * cross-interpolation rows:
+ *   job j: the order-`order` flux points of cube face src_code[j] of cell
+ *   src_cell[j] are mapped to physical space, shifted by the face's periodic
+ *   translation (sign[j] < 0: minus, owner -> neighbour; > 0: plus), located
+ *   on cube face tgt_code[j] of cell tgt_cell[j] (closed form on tets, the
+ *   reference's damped Newton iteration with backtracking on prisms, both
+ *   with the face's sqrt(area) as length scale), and the rows
+ *   V(located points) * v_inv of that cell type are written to mats[j]
+ *   (n_fp x n_sps); mode[j] = 0 writes every row, 1 only the rows whose bit is
+ *   set in mask[j], 2 only the others (the two halves of a split prism quad
+ *   face), the remaining rows are zero.  coords[j] gets the located free
+ *   coordinates (n_fp x 2), resid[j] the largest location residual.
+ * Restates build_fp_newton_parallel (fr/face_flux_points_numba.py:30-251) and
+ * build_ms_interp_parallel (fr/face_flux_points_ms_numba.py:31-317).  All
+ * pointers are HOST memory; cells are prisms [0, n_prism) then tets; v_inv_*
+ * is the (n_sps x n_sps) inverse modal Vandermonde matrix of that cell type
+ * (NULL when the type is absent); sps_1d the order+1 Gauss-Legendre points.
+ * Every index is range-checked before any kernel runs (AFR_EINDEX); the
+ * device memory is allocated per call and released before it returns. */
+int afr_flux_point_jobs(int32_t order, int32_t n_prism, int64_t n_tet, int64_t n_nodes, const double* nodes,
+                        const int32_t* prism_conn, const int32_t* tet_conn, const double* v_inv_prism,
+                        const double* v_inv_tet, const double* sps_1d, int64_t n_faces, const double* area,
+                        const double* translation, int64_t n_jobs, const int32_t* face, const int32_t* src_cell,
+                        const int32_t* src_code, const int32_t* tgt_cell, const int32_t* tgt_code,
+                        const int32_t* sign, const int32_t* mode, const uint32_t* mask, double* mats, double* coords,
+                        double* resid);
 
 /* Bytes of device memory the handle owns (tables + scratch). */
 int afr_device_bytes(const afr_handle* h, uint64_t* out);

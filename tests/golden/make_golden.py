@@ -461,6 +461,39 @@ def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1
     return out
 
 
+def make_fluxpoints(name, box, order, mesh_bc=None):
+    """Inputs and outputs of the reference's flux-point construction
+    (fr/face_flux_points_merge.py:51-434 with fr/face_flux_points_numba.py
+    and face_flux_points_ms_numba.py) on one box mesh: its FRFaceConnectivity
+    and cell connectivity in, the flattened face tables and the raw Newton
+    coordinates and residuals out."""
+    from autoflowcfd.core.fr_operators.face_kernels import get_flat_face_geometry
+    from autoflowcfd.fr.operators import generate_fr_operators
+
+    mesh = ref_mesh(box, order, mesh_bc)
+    fc = mesh.face_connectivity
+    ffp = mesh.face_flux_points
+    ops = generate_fr_operators(order)
+    out = dict(meta_name=np.array(name), order=np.int32(order), n_cells=np.int32(mesh.n_cells),
+               n_prism=np.int32(mesh.n_prism_cells), nodes=np.asarray(mesh._node_coords, float))
+    out["prism_conn"] = (np.asarray(mesh._fixed_prism_conn, np.int64) if mesh._fixed_prism_conn is not None
+                         else np.zeros((0, 6), np.int64))
+    out["tet_conn"] = (np.asarray(mesh._fixed_tet_conn, np.int64) if mesh._fixed_tet_conn is not None
+                       else np.zeros((0, 4), np.int64))
+    for k in ("owner_cell", "neighbor_cell", "owner_cube_face", "neighbor_cube_face", "area", "normal",
+              "face_node_ids", "is_boundary", "face_translation"):
+        out["fc_" + k] = np.asarray(getattr(fc, k))
+    out.update(flat_tables(mesh, ops))
+    out["true_area_weight"] = np.asarray(ffp.true_area_weight, float)
+    out["nb_fc"], out["ow_fc"] = np.asarray(ffp._nb_fc), np.asarray(ffp._ow_fc)
+    out["nb_resid"], out["ow_resid"] = np.asarray(ffp._nb_resid), np.asarray(ffp._ow_resid)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: N={mesh.n_cells} faces={fc.n_faces} multi-source nb={int(np.sum(out['nb_src1_idx'] >= 0))} "
+          f"ow={int(np.sum(out['ow_src1_idx'] >= 0))} periodic={bool(np.any(out['fc_face_translation'] != 0))}",
+          flush=True)
+    return out
+
+
 def _summaries(U, k=None, nut=None):
     """Per-variable sum, L2, max and min of a state (and k / nu_t maxima)."""
     flat = U.reshape(-1, U.shape[-1])
@@ -800,6 +833,17 @@ def main(which=None):
         make_continuation("cont_tet_p2_uniform", box, 2, 1.8e-5, (rho, u, p), None, max_iter=30, tol=2.0,
                           inviscid_only=True)
 
+    def f_fluxpoints():
+        wall = {n: "FARFIELD" for n in boxmesh.PLANE_NAMES}
+        wall["z_min"] = "WALL"
+        make_fluxpoints("fp_prism_p2", boxmesh.prism_box(4, 3, 3, (4.0, 2.0, 1.5), jitter=0.1, seed=7), 2, wall)
+        make_fluxpoints("fp_prism_p3_bump", boxmesh.prism_box(3, 2, 2, (1.5, 1.0, 1.0), jitter=0.1, seed=5,
+                                                              bump=(0.05, 0.75, 0.5, 0.3)), 3, wall)
+        make_fluxpoints("fp_prism_p1", boxmesh.prism_box(4, 3, 2, (2.0, 1.0, 1.0), jitter=0.1, seed=5,
+                                                         bump=(0.05, 1.0, 0.5, 0.3)), 1, wall)
+        make_fluxpoints("fp_tet_p3", boxmesh.tet_box(2, 2, 2, (1.0, 1.0, 1.0), jitter=0.05, seed=9, periodic=True), 3)
+        make_fluxpoints("fp_tet_p2", boxmesh.tet_box(3, 3, 3, (1.0, 1.0, 1.0), jitter=0.05, seed=4, periodic=True), 2)
+
     cases = {"tet_p1_vortex": c_tet_p1, "prism_p2_sst": c_prism_p2_sst, "prism_p1_ns": c_prism_p1_ns,
              "tet_p3_tgv": c_tet_p3, "prism_p1_floors": c_prism_p1_floors, "tet_p1_align": c_tet_p1_align,
              "traj_c1_vortex": t_c1, "traj_c2_sample": t_c2_sample, "traj_p3_tgv": t_p3,
@@ -807,7 +851,8 @@ def main(which=None):
              "prism_p1_ns_imex_euler": lambda: c_prism_p1_ns_scheme("imex_euler", 1e-3),
              "prism_p2_sst_dual_time": lambda: c_prism_p2_sst_scheme("dual_time", 2e-5),
              "prism_p0_ns": c_prism_p0_ns, "tet_p0_vortex": c_tet_p0_vortex,
-             "cont_prism_p2_ns": k_cont_prism_p2, "cont_tet_p2_uniform": k_cont_tet_p2}
+             "cont_prism_p2_ns": k_cont_prism_p2, "cont_tet_p2_uniform": k_cont_tet_p2,
+             "fluxpoints": f_fluxpoints}
     for k, fn in cases.items():
         if which and k not in which:
             continue
