@@ -244,7 +244,8 @@ def plan_jobs(face_conn, prism_conn, tet_conn, order: int) -> Dict:
                 prism_conn=prism_conn, tet_conn=tet_conn)
 
 
-def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colorer=None) -> Dict[str, np.ndarray]:
+def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colorer=None,
+                      timings: Dict = None) -> Dict[str, np.ndarray]:
     """The flattened face tables of a mesh (the keys ``afr_create`` takes).
 
     Args:
@@ -256,11 +257,17 @@ def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colore
         tet_conn: (n_tet, 4) node ids; nodes: (n_nodes, 3).
         colorer: ``f(owner, neighbor, is_boundary, n_cells) -> colors``
             (default: the library's greedy coloring).
+        timings: optional dict that receives the wall seconds of the host
+            planning ("plan_s"), the device jobs with their transfers
+            ("device_s") and the assembly with the colors ("assemble_s").
     Returns owner / neighbour cells and sides, primary flags, true normals
     and area weights, the source cells and interpolation matrices (dense,
     with the compact second-source table), colors, and the raw Newton
     coordinates and residuals (``nb_fc``, ``ow_fc``, ``nb_resid``,
     ``ow_resid``)."""
+    import time
+
+    t0 = time.perf_counter()
     pl = plan_jobs(face_conn, prism_conn, tet_conn, order)
     F, oc, nc, occ, ncc, isb = pl["F"], pl["oc"], pl["nc"], pl["occ"], pl["ncc"], pl["isb"]
     opr, npr, ms_nb, ms_ow, main_nb, main_ow = (pl[k] for k in ("opr", "npr", "ms_nb", "ms_ow", "main_nb",
@@ -276,6 +283,7 @@ def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colore
                                                                                        None)
     trans = np.zeros((F, 3)) if tr is None else np.ascontiguousarray(tr, np.float64).reshape(F, 3)
     J = len(jobs["face"])
+    t1 = time.perf_counter()
     mats = np.zeros((J, P, S))
     coords = np.zeros((J, P, 2))
     resid = np.zeros(J)
@@ -295,6 +303,7 @@ def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colore
                                                      "mode")],
             arr["mask"].ctypes.data_as(P_U), pd(mats), pd(coords), pd(resid))
         _lib.check(rc)
+    t2 = time.perf_counter()
     a, b, c = len(main_nb), len(main_nb) + len(main_ow), len(main_nb) + len(main_ow) + len(ms_nb)
 
     def dense(faces, rows):
@@ -322,6 +331,8 @@ def flux_point_tables(face_conn, prism_conn, tet_conn, nodes, order: int, colore
     if colorer is None:
         colorer = _lib.greedy_face_coloring
     colors = colorer(oc, nc, isb.astype(np.uint8), n_prism + n_tet)
+    if timings is not None:
+        timings.update(plan_s=t1 - t0, device_s=t2 - t1, assemble_s=time.perf_counter() - t2, n_jobs=J)
     return dict(
         owner_cell=oc, neighbor_cell=nc, is_boundary=isb.astype(np.uint8),
         owner_axis=FACE_AXIS[occ], owner_side=FACE_SIDE[occ],
