@@ -706,39 +706,51 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
       cp_async_wait0();  // this thread's copies of the tile
       __syncthreads();   // everyone's
     }
-    // ---- primitives (FP64), det and metric divergence of the tile ----
-    for (int t = tid; t < C * S; t += NT) {
-      const int c = t / S;
-      double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
-      if (c < nc) {
-        mxd::prim_T(L::STG ? sStg + t * nv : Ucur + ((size_t)e0 * S + t) * nv, q);
-        if (L::VP) {
-          sDet[t] = sStg[C * S * 8 + t];  // reciprocal: the readouts multiply
-          sMD[t * 3 + 0] = sStg[C * S * 9 + t * 3 + 0];
-          sMD[t * 3 + 1] = sStg[C * S * 9 + t * 3 + 1];
-          sMD[t * 3 + 2] = sStg[C * S * 9 + t * 3 + 2];
+    // ---- primitives (FP64), det and metric divergence of the tile; one
+    // warp per cell, lanes over its points: the cell means by a fixed-order
+    // shuffle reduction and the Euler flux at the means in the same pass ----
+    for (int c = warp; c < C; c += NT / 32) {
+      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int s0 = 0; s0 < S; s0 += 32) {
+        const int s = s0 + lane;
+        if (s < S) {
+          const int t = c * S + s;
+          double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
+          if (c < nc) {
+            mxd::prim_T(L::STG ? sStg + t * nv : Ucur + ((size_t)e0 * S + t) * nv, q);
+            if (L::VP) {
+              sDet[t] = sStg[C * S * 8 + t];  // reciprocal: the readouts multiply
+              sMD[t * 3 + 0] = sStg[C * S * 9 + t * 3 + 0];
+              sMD[t * 3 + 1] = sStg[C * S * 9 + t * 3 + 1];
+              sMD[t * 3 + 2] = sStg[C * S * 9 + t * 3 + 2];
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            sQ[t * 5 + v] = q[v];
+            acc[v] += q[v];
+          }
         }
       }
 #pragma unroll
-      for (int v = 0; v < 5; ++v) sQ[t * 5 + v] = q[v];
+      for (int v = 0; v < 5; ++v)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+      if (lane == 0) {
+        double qb[5], F[3][5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qb[v] = acc[v] * (1.0 / S);
+        euler_flux<double>(qb, F);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sQb[c * 5 + v] = qb[v];
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+          for (int v = 0; v < 5; ++v) sFb[c * 15 + n * 5 + v] = F[n][v];
+      }
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) stage(tile + (int)gridDim.x);  // the staging buffer is free again
-    for (int t = tid; t < C * 5; t += NT) {
-      const int c = t / 5, v = t % 5;
-      double acc = 0.0;
-      for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 5 + v];
-      sQb[t] = acc * (1.0 / S);
-    }
-    __syncthreads();
-    for (int c = tid; c < C; c += NT) {
-      double F[3][5];
-      euler_flux<double>(sQb + c * 5, F);
-#pragma unroll
-      for (int n = 0; n < 3; ++n)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) sFb[c * 15 + n * 5 + v] = F[n][v];
-    }
     // ---- A operands: q - qbar at the solution points; contravariant viscous flux ----
     for (int idx = tid; idx < C * Sq; idx += NT) {
       int c, s;
@@ -780,6 +792,20 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
             mxd::st_split(sAD, 128 * 3 * Sq, tc::kmajor_index(v * C + c, m * Sq + s, 128), Gt[m][v]);
       }
     }
+    // the fine-point adjugate rows of this thread's flux items, loaded now so
+    // that their latency overlaps the products and the readout below
+    constexpr int NFI = (C * Fq + NT - 1) / NT;
+    float4 adf[NFI][3];
+#pragma unroll
+    for (int k = 0; k < NFI; ++k) {
+      const int idx = tid + k * NT;
+      int c, i;
+      mxd::cell_point(idx, Fq, c, i);
+      const bool live = idx < C * Fq && c < nc && i < FN;
+      const float4* ad = mo.adjf + ((size_t)(e0 + (live ? c : 0)) * FN + (live ? i : 0)) * 3;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) adf[k][m] = live ? __ldg(ad + m) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     tc::fence_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -807,7 +833,10 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
     }
     __syncthreads();
     // ---- contravariant Euler flux deviations at the fine points -> A_W ----
-    for (int idx = tid; idx < C * Fq; idx += NT) {
+#pragma unroll
+    for (int k = 0; k < NFI; ++k) {
+      const int idx = tid + k * NT;
+      if (idx >= C * Fq) break;
       int c, i;
       mxd::cell_point(idx, Fq, c, i);
       float Ft[3][5];
@@ -816,7 +845,6 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
 #pragma unroll
         for (int v = 0; v < 5; ++v) Ft[m][v] = 0.f;
       if (c < nc && i < FN) {
-        const float4* ad = mo.adjf + ((size_t)(e0 + c) * FN + i) * 3;
         float qb[5], dq[5], dF[3][5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -826,7 +854,7 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
         mxd::euler_flux_delta(qb, dq, dF);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          const float4 x = __ldg(ad + m);
+          const float4 x = adf[k][m];
 #pragma unroll
           for (int v = 0; v < 5; ++v) Ft[m][v] = x.x * dF[0][v] + x.y * dF[1][v] + x.z * dF[2][v];
         }
