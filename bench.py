@@ -716,6 +716,8 @@ def run_p0(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     spec = SMALL if args.small else FULL
+    if args.shape:
+        spec = dict(FULL, shape=tuple(int(x) for x in args.shape.split(",")))
     t0 = time.perf_counter()
     case, U, mu = _p0_setup(spec)
     t_gen = time.perf_counter() - t0
