@@ -183,6 +183,39 @@ def half_masks(cells6: np.ndarray, codes: np.ndarray, face_nodes: np.ndarray, or
     return (m.astype(np.uint64) << np.arange(m.shape[1], dtype=np.uint64)).sum(1).astype(np.uint32)
 
 
+def distribution_maps(n1d: int):
+    """(fp_of_sp, axis_coord_of_sp), each (3, n1d^3): the lifting of a face's
+    flux-point row onto the solution points along `axis` (the index form of
+    _distribute_from_face, core/fr_operators/face_kernels.py:68-115): point
+    (i0, i1, i2) takes g'[i_axis] times flux point (i_o0 * n1d + i_o1), o0 < o1
+    the other two axes."""
+    S = n1d**3
+    idx = np.array(np.unravel_index(np.arange(S), (n1d, n1d, n1d)))  # (3, S): i0, i1, i2
+    fp = np.empty((3, S), np.int64)
+    co = np.empty((3, S), np.int64)
+    for ax in range(3):
+        o0, o1 = [a for a in range(3) if a != ax]
+        fp[ax] = idx[o0] * n1d + idx[o1]
+        co[ax] = idx[ax]
+    return fp, co
+
+
+def operator_face_tables(ops, order: int) -> Dict[str, np.ndarray]:
+    """The per-order face tables that come from the operators, not the mesh:
+    the boundary extrapolation matrices by (cell type, axis, side), g' at the
+    two ends and the distribution maps (core/fr_operators/face_kernels.py:297-305)."""
+    n1d = order + 1
+    P, S = n1d * n1d, n1d**3
+    ext = np.zeros((2, 3, 2, P, S))
+    for axis in range(3):
+        for si, side in enumerate((-1.0, 1.0)):
+            ext[0, axis, si] = ops.boundary_extrap_prism[(axis, side)]
+            ext[1, axis, si] = ops.boundary_extrap_tet[(axis, side)]
+    fp, co = distribution_maps(n1d)
+    return dict(boundary_extrap=ext, g_left=np.asarray(ops.g_left, np.float64),
+                g_right=np.asarray(ops.g_right, np.float64), dist_fp_of_sp=fp, dist_axis_coord_of_sp=co)
+
+
 def _get(fc, name):
     return np.asarray(fc[name] if isinstance(fc, dict) else getattr(fc, name))
 

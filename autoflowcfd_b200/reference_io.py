@@ -25,6 +25,7 @@ AFR_EUNSUPPORTED.  An unknown boundary type raises ValueError, as the
 reference's provider does (boundary/fr_ghost_state.py:189).
 """
 
+from types import SimpleNamespace
 from typing import Dict, Optional
 
 import numpy as np
@@ -153,7 +154,7 @@ def _wall_face_mask(mesh) -> Optional[np.ndarray]:
 
 
 def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, flat=None,
-                cd_wall_face=None) -> Dict[str, np.ndarray]:
+                cd_wall_face=None, flux_points: str = "reference") -> Dict[str, np.ndarray]:
     """Flat tables of a reference mesh for ``afr_create``.
 
     Args:
@@ -168,7 +169,23 @@ def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, fla
             reference's cached ``get_flat_face_geometry(mesh, ops)``.
         cd_wall_face: (n_faces,) faces of the force integral; by default from
             the mesh's WALL boundary groups.
+        flux_points: "reference" takes the face tables from the mesh's own
+            flux-point construction; "device" builds them on the GPU from the
+            mesh's face connectivity (autoflowcfd_b200.facegeom) and the
+            operators.
     """
+    if flux_points not in ("reference", "device"):
+        raise ValueError(f"flux_points must be 'reference' or 'device', got {flux_points!r}")
+    if flux_points == "device":
+        from .facegeom import flux_point_tables, operator_face_tables
+
+        prism = mesh._fixed_prism_conn if mesh._fixed_prism_conn is not None else np.zeros((0, 6), np.int64)
+        tet = mesh._fixed_tet_conn if mesh._fixed_tet_conn is not None else np.zeros((0, 4), np.int64)
+        t = flux_point_tables(mesh.face_connectivity, prism, tet, mesh._node_coords, int(mesh.order))
+        for k in ("nb_fc", "ow_fc", "nb_resid", "ow_resid"):
+            t.pop(k)
+        t.update(operator_face_tables(ops, int(mesh.order)))
+        flat = SimpleNamespace(n_faces=len(t["owner_cell"]), _tables=t)
     if flat is None:
         from autoflowcfd.core.fr_operators.face_kernels import get_flat_face_geometry
 
@@ -187,7 +204,7 @@ def export_case(mesh, ops, boundary_ghost_provider=None, wall_distance=None, fla
     if getattr(mesh, "cell_volumes", None) is not None:
         out["fv_cell_volumes"] = np.asarray(mesh.cell_volumes, float)
     out.update(op_tables(ops))
-    out.update(flat_tables(flat))
+    out.update(flat._tables if hasattr(flat, "_tables") else flat_tables(flat))
     out.update(lower_ghost_provider(boundary_ghost_provider, int(flat.n_faces)))
     taw = getattr(getattr(mesh, "face_flux_points", None), "true_area_weight", None)
     if taw is not None:

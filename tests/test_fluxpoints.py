@@ -67,3 +67,10 @@ def test_half_masks_are_complementary_and_cover_the_face():
     m = pl["nb_mask"][pl["ms_nb"]].astype(np.int64)
     counts = np.array([bin(int(v)).count("1") for v in m])
     assert np.all((counts > 0) & (counts < P))
+
+
+@pytest.mark.parametrize("name", ["prism_p0_ns", "prism_p1_ns", "prism_p2_sst", "tet_p3_tgv"])
+def test_distribution_maps_match_reference(golden, name):
+    g = golden(name)
+    fp, co = FG.distribution_maps(int(g["order"]) + 1)
+    assert np.array_equal(fp, g["dist_fp_of_sp"]) and np.array_equal(co, g["dist_axis_coord_of_sp"])

@@ -71,3 +71,39 @@ def test_case_from_constructed_tables_reproduces_reference_residuals(golden):
     assert rel(s.compute_inviscid_residual().cpu().numpy(), case["R_inv"]) < 1e-9
     assert rel(s.compute_viscous_residual().cpu().numpy(), case["R_visc"]) < 1e-9
     s.cleanup()
+
+
+def test_exporter_builds_the_face_tables_on_the_device(golden):
+    """export_case(..., flux_points="device") on stand-ins of the reference's
+    objects for prism_p2_sst (whose box is fp_prism_p2's): the constructed face
+    tables and, through the C-ABI, the reference's residuals."""
+    import refstandins
+    from autoflowcfd_b200.reference_io import export_case
+    from autoflowcfd_b200.solver import B200FRSolver
+
+    case = dict(golden("prism_p2_sst"))
+    fp = load("fp_prism_p2")
+    mesh, ops, _ = refstandins.mesh_ops_flat(case)
+    mesh.face_connectivity = type("FC", (), face_conn(fp))()
+    mesh._fixed_prism_conn, mesh._fixed_tet_conn, mesh._node_coords = fp["prism_conn"], None, fp["nodes"]
+    ext = case["boundary_extrap"]
+    ops.boundary_extrap_prism = {(a, s): ext[0, a, i] for a in range(3) for i, s in enumerate((-1.0, 1.0))}
+    ops.boundary_extrap_tet = {(a, s): ext[1, a, i] for a in range(3) for i, s in enumerate((-1.0, 1.0))}
+    ops.g_left, ops.g_right = case["g_left"], case["g_right"]
+    out = export_case(mesh, ops, refstandins.provider(case), wall_distance=case["wall_distance"],
+                      flux_points="device")
+    for k in ("owner_is_primary", "neighbor_is_primary", "nb_src1_idx", "ow_src1_idx", "colors", "dist_fp_of_sp",
+              "dist_axis_coord_of_sp", "bc_group"):
+        assert np.array_equal(np.asarray(out[k]).astype(np.int64), np.asarray(case[k]).astype(np.int64)), k
+    assert rel(out["nb_src0_mat"], case["nb_src0_mat"]) < 1e-11
+    assert np.array_equal(out["boundary_extrap"], case["boundary_extrap"])
+    for k in ("freestream", "U0", "k0", "omega0", "nu_t0", "mu", "turb", "R_inv", "R_visc"):
+        out[k] = case[k]
+    free = case["freestream"]
+    s = B200FRSolver(out, turb_model_name="SST", mu_molecular=float(case["mu"]), rho_inf=free[0], vel_inf=free[1],
+                     p_inf=free[2])
+    s.set_state_from_cpu(case["U0"])
+    s.set_turbulence(case["k0"], case["omega0"], case["nu_t0"])
+    assert rel(s.compute_inviscid_residual().cpu().numpy(), case["R_inv"]) < 1e-9
+    assert rel(s.compute_viscous_residual().cpu().numpy(), case["R_visc"]) < 1e-9
+    s.cleanup()
