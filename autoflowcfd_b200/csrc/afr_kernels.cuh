@@ -64,6 +64,7 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
@@ -468,21 +469,14 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     for (int t = tid; t < (k_end - k_beg) * NP * 10; t += blockDim.x) sJ[t] = J[(size_t)k_beg * NP * 10 + t];
   __syncthreads();
 
-  // ---- Q at fine points (c2f) and viscous contravariant fluxes ----
-  for (int t = tid; t < FN * 5; t += blockDim.x) {
-    const int i = t / 5, v = t % 5;
-    const double* c = ops.c2f[ct] + i * S;
-    double acc[CPB];
-#pragma unroll
-    for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-    for (int s = 0; s < S; ++s) {
-      const double w = __ldg(c + s);
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] += w * sPF[(b * S + s) * PFW + v];
-    }
-#pragma unroll
-    for (int b = 0; b < CPB; ++b)
-      if (b < nc) sQf[(b * FN + i) * 5 + v] = acc[b];
+  // ---- Q at fine points (c2f, an FP64 tensor-core product: rows the fine
+  // points, columns (cell, variable)) and viscous contravariant fluxes ----
+  {
+    const double* C2F = ops.c2f[ct];
+    dmma_product(
+        FN, 5 * nc, S, [&](int i, int s) { return __ldg(C2F + (size_t)i * S + s); },
+        [&](int s, int col) { return sPF[((col / 5) * S + s) * PFW + col % 5]; },
+        [&](int i, int col, double x) { sQf[((col / 5) * FN + i) * 5 + col % 5] = x; });
   }
   if (visc) {
     for (int t = tid; t < nc * S; t += blockDim.x) {
@@ -511,40 +505,27 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
         sFt[(t * 3 + m) * 5 + v] = am[m * 3 + 0] * F[0][v] + am[m * 3 + 1] * F[1][v] + am[m * 3 + 2] * F[2][v];
   }
   __syncthreads();
-  // ---- divergences: inviscid W (S x 3FN) in two K halves, viscous D3 (S x 3S) ----
+  // ---- divergences on the FP64 tensor path: inviscid W (S x 3FN) applied to
+  // the fine-point fluxes, viscous D3 (S x 3S) to the point fluxes; rows the
+  // solution points, columns (cell, variable) ----
   {
-    double* sWp = sm + L::oWp;  // [half][b][s*5+v]
-    constexpr int KH = FN * 3 / 2;  // first half [0, KH), second [KH, 3FN) (3FN is odd at P1)
-    const int n_w = 2 * S * 5, n_all = visc ? 3 * S * 5 : 2 * S * 5;
-    for (int t = tid; t < n_all; t += blockDim.x) {
-      const bool inv = t < n_w;
-      const int u = inv ? t % (S * 5) : t - n_w;
-      const int half = inv ? t / (S * 5) : 0;
-      const int s = u / 5, v = u % 5;
-      const int K = inv ? (half == 0 ? KH : FN * 3 - KH) : S * 3;
-      const double* w = inv ? ops.W[ct] + (size_t)s * FN * 3 + half * KH : ops.D3[ct] + (size_t)s * S * 3;
-      const double* X = inv ? sFt + half * KH * 5 : sGt;
-      const int ldb = inv ? FN * 15 : S * 15;
-      double acc[CPB];
-#pragma unroll
-      for (int b = 0; b < CPB; ++b) acc[b] = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < K; ++k) {
-        const double wk = __ldg(w + k);
-#pragma unroll
-        for (int b = 0; b < CPB; ++b) acc[b] += wk * X[b * ldb + k * 5 + v];
-      }
-#pragma unroll
-      for (int b = 0; b < CPB; ++b)
-        if (b < nc) {
-          if (inv) sWp[(half * CPB + b) * S * 5 + u] = acc[b];
-          else sRv[(b * S + s) * 5 + v] = acc[b] / sDet[b * S + s];
-        }
-    }
-    __syncthreads();
-    for (int t = tid; t < nc * S * 5; t += blockDim.x) {
-      const int b = t / (S * 5), u = t % (S * 5);
-      sRi[t] = -(sWp[b * S * 5 + u] + sWp[(CPB + b) * S * 5 + u]) / sDet[b * S + u / 5];
+    const double* Wm = ops.W[ct];
+    dmma_product(
+        S, 5 * nc, FN * 3, [&](int s, int k) { return __ldg(Wm + (size_t)s * FN * 3 + k); },
+        [&](int k, int col) { return sFt[(col / 5) * FN * 15 + k * 5 + col % 5]; },
+        [&](int s, int col, double x) {
+          const int b = col / 5;
+          sRi[(b * S + s) * 5 + col % 5] = -x / sDet[b * S + s];
+        });
+    if (visc) {
+      const double* Dm = ops.D3[ct];
+      dmma_product(
+          S, 5 * nc, S * 3, [&](int s, int k) { return __ldg(Dm + (size_t)s * S * 3 + k); },
+          [&](int k, int col) { return sGt[(col / 5) * S * 15 + k * 5 + col % 5]; },
+          [&](int s, int col, double x) {
+            const int b = col / 5;
+            sRv[(b * S + s) * 5 + col % 5] = x / sDet[b * S + s];
+          });
     }
   }
   __syncthreads();
@@ -629,16 +610,13 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     part[CPB * S + p] = Lr[0] * Lr[0];
   }
   __syncthreads();
-  // modal filter on the first five variables; lanes of a warp share the
-  // filter row s (broadcast loads), each output summed over j in order
+  // modal filter on the first five variables as an FP64 tensor-core product
+  // (rows s, columns (cell, variable), K the cell's points)
   const double* Fm = ops.filt[ct];
-  for (int t = tid; t < S * CPB * 5; t += blockDim.x) {
-    const int s = t / (CPB * 5), r = t % (CPB * 5), b = r / 5, v = r % 5;
-    if (b >= nc) continue;
-    double acc = 0.0;
-    for (int j = 0; j < S; ++j) acc += __ldg(Fm + s * S + j) * Up[(b * S + j) * US + v];
-    a.Unext[((size_t)(e0 + b) * S + s) * nv + v] = acc;
-  }
+  dmma_product(
+      S, 5 * nc, S, [&](int s, int j) { return __ldg(Fm + (size_t)s * S + j); },
+      [&](int j, int col) { return Up[((col / 5) * S + j) * US + col % 5]; },
+      [&](int s, int col, double x) { a.Unext[((size_t)(e0 + col / 5) * S + s) * nv + col % 5] = x; });
   for (int p = tid; p < nc * S; p += blockDim.x)
     for (int v = 5; v < nv; ++v) a.Unext[((size_t)e0 * S + p) * nv + v] = Up[p * US + v];
   if (a.stage == 0 && tid < nc) {
