@@ -706,51 +706,39 @@ __global__ void __launch_bounds__(MX_VOL_THREADS, 1)
       cp_async_wait0();  // this thread's copies of the tile
       __syncthreads();   // everyone's
     }
-    // ---- primitives (FP64), det and metric divergence of the tile; one
-    // warp per cell, lanes over its points: the cell means by a fixed-order
-    // shuffle reduction and the Euler flux at the means in the same pass ----
-    for (int c = warp; c < C; c += NT / 32) {
-      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-      for (int s0 = 0; s0 < S; s0 += 32) {
-        const int s = s0 + lane;
-        if (s < S) {
-          const int t = c * S + s;
-          double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
-          if (c < nc) {
-            mxd::prim_T(L::STG ? sStg + t * nv : Ucur + ((size_t)e0 * S + t) * nv, q);
-            if (L::VP) {
-              sDet[t] = sStg[C * S * 8 + t];  // reciprocal: the readouts multiply
-              sMD[t * 3 + 0] = sStg[C * S * 9 + t * 3 + 0];
-              sMD[t * 3 + 1] = sStg[C * S * 9 + t * 3 + 1];
-              sMD[t * 3 + 2] = sStg[C * S * 9 + t * 3 + 2];
-            }
-          }
-#pragma unroll
-          for (int v = 0; v < 5; ++v) {
-            sQ[t * 5 + v] = q[v];
-            acc[v] += q[v];
-          }
+    // ---- primitives (FP64), det and metric divergence of the tile ----
+    for (int t = tid; t < C * S; t += NT) {
+      const int c = t / S;
+      double q[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
+      if (c < nc) {
+        mxd::prim_T(L::STG ? sStg + t * nv : Ucur + ((size_t)e0 * S + t) * nv, q);
+        if (L::VP) {
+          sDet[t] = sStg[C * S * 8 + t];  // reciprocal: the readouts multiply
+          sMD[t * 3 + 0] = sStg[C * S * 9 + t * 3 + 0];
+          sMD[t * 3 + 1] = sStg[C * S * 9 + t * 3 + 1];
+          sMD[t * 3 + 2] = sStg[C * S * 9 + t * 3 + 2];
         }
       }
 #pragma unroll
-      for (int v = 0; v < 5; ++v)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
-      if (lane == 0) {
-        double qb[5], F[3][5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qb[v] = acc[v] * (1.0 / S);
-        euler_flux<double>(qb, F);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) sQb[c * 5 + v] = qb[v];
-#pragma unroll
-        for (int n = 0; n < 3; ++n)
-#pragma unroll
-          for (int v = 0; v < 5; ++v) sFb[c * 15 + n * 5 + v] = F[n][v];
-      }
+      for (int v = 0; v < 5; ++v) sQ[t * 5 + v] = q[v];
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) stage(tile + (int)gridDim.x);  // the staging buffer is free again
+    for (int t = tid; t < C * 5; t += NT) {
+      const int c = t / 5, v = t % 5;
+      double acc = 0.0;
+      for (int s = 0; s < S; ++s) acc += sQ[(c * S + s) * 5 + v];
+      sQb[t] = acc * (1.0 / S);
+    }
+    __syncthreads();
+    for (int c = tid; c < C; c += NT) {
+      double F[3][5];
+      euler_flux<double>(sQb + c * 5, F);
+#pragma unroll
+      for (int n = 0; n < 3; ++n)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sFb[c * 15 + n * 5 + v] = F[n][v];
+    }
     // ---- A operands: q - qbar at the solution points; contravariant viscous flux ----
     for (int idx = tid; idx < C * Sq; idx += NT) {
       int c, s;
