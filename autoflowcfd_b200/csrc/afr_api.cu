@@ -309,10 +309,11 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm = nullptr) {
-    const int nt = h->slots.n * NP;
-    if (nt > 0)
-      k_face<S, NP><<<(nt + 127) / 128, 128, 0, st>>>(h->g, h->ops, h->fc, h->bc, h->slots, h->PF, h->prm.mu,
-                                                      a.inviscid_only ? 0 : 1, h->J);
+    constexpr int SPW = 32 / NP;  // slots per warp of the face kernel
+    const int nwarps = (h->slots.n + SPW - 1) / SPW;
+    if (nwarps > 0)
+      k_face<S, NP><<<(nwarps + FACE_WARPS - 1) / FACE_WARPS, 32 * FACE_WARPS, 0, st>>>(
+          h->g, h->ops, h->fc, h->bc, h->slots, h->PF, h->prm.mu, a.inviscid_only ? 0 : 1, h->J);
     if (tm) tm->mark(st);
     const size_t smem = cell_smem();
     static bool attr = false;

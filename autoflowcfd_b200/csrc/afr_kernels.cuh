@@ -291,48 +291,171 @@ __device__ __forceinline__ void ld18(const double* __restrict__ p, double x[18])
   }
 }
 
+// one warp's m8n8k4 FP64 product C (M x N) = A (M x K) * B (K x N), all
+// tiles by this warp (see dmma_product for the fragment layout)
+template <class FA, class FB, class FC>
+__device__ __forceinline__ void dmma_warp(int M, int N, int K, FA a, FB b, FC c) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
+  for (int tile = 0; tile < mt * nt; ++tile) {
+    const int m = (tile / nt) * 8 + g, n0 = (tile % nt) * 8;
+    double c0 = 0.0, c1 = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + t;
+      const double a0 = (m < M && k < K) ? a(m, k) : 0.0;
+      const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
+      dmma884(c0, c1, a0, b0);
+    }
+    const int n = n0 + 2 * t;
+    if (m < M) {
+      if (n < N) c(m, n, c0);
+      if (n + 1 < N) c(m, n + 1, c1);
+    }
+  }
+}
+
+// one warp's product C (M x N) = A (M x K) * B (K x N) with every tile's
+// accumulators held in registers (MT row tiles, NT column tiles): each k-step
+// loads the A fragments of all row tiles and the B fragments of all column
+// tiles, so the operand loads of the whole product are independent of one
+// another and of the products.  Per element the k-steps accumulate in the
+// same order as dmma_warp.
+template <int MT, int NT, int K, class FA, class FB, class FC>
+__device__ __forceinline__ void dmma_warp_rb(int M, int N, FA a, FB b, FC c) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double acc[MT][NT][2];
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 4) {
+    const int k = k0 + t;
+    double av[MT], bv[NT];
+#pragma unroll
+    for (int mi = 0; mi < MT; ++mi) {
+      const int m = mi * 8 + g;
+      av[mi] = (m < M && k < K) ? a(m, k) : 0.0;
+    }
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) {
+      const int n = ni * 8 + g;
+      bv[ni] = (n < N && k < K) ? b(k, n) : 0.0;
+    }
+#pragma unroll
+    for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+  }
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) {
+      const int m = mi * 8 + g, n = ni * 8 + 2 * t;
+      if (m < M) {
+        if (n < N) c(m, n, acc[mi][ni][0]);
+        if (n + 1 < N) c(m, n + 1, acc[mi][ni][1]);
+      }
+    }
+}
+
+// Face kernel: one warp per group of SPW = 32 / NP slots (a slot is one side
+// of one face record whose correction lifts into a cell; lane = slot-in-group
+// * NP + flux point in the flux phase).  Per slot, the own side's
+// extrapolation E * [q, adjugate row of the face's axis, grads, mu_t] and the
+// other side's interpolation M_src0 * [q, grads, mu_t] (+ M_src1 * ...) are
+// FP64 tensor-core products into the warp's shared rows; the lanes then form
+// the ghost state, AUSM+up with the alignment fallback and the BR1 common
+// flux with the boundary penalty
+// (core/fr_residual/inviscid_kernel_colored.py:86-236,
+// core/fr_residual/viscous_flux_kernel.py:335-520) and write the jumps
+// J (n_slots, NP, 10).  A weight of zero contributes nothing to the products
+// while the state is finite (the reference skips zero weights,
+// inviscid_kernel_colored.py:117-121; a non-finite state makes the step
+// non-finite either way).
+// Slot flags: bit0 neighbour side, bit1 boundary face, bits2-3 axis, bit4 side>0.
+constexpr int FACE_WARPS = 4;
+constexpr int FW_OWN = 21, FW_OTH = 18;  // doubles per face point: own side, other side
+
 template <int S, int NP>
-__global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc bc, SlotTable st,
-                                                 const double* __restrict__ PF, double mu, int visc,
-                                                 double* __restrict__ J) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= st.n * NP) return;
-  const int sl = t / NP, i = t % NP;
+__global__ void __launch_bounds__(32 * FACE_WARPS, 4) k_face(Geom g, Ops ops, Faces fc, Bc bc, SlotTable st,
+                                                          const double* __restrict__ PF, double mu, int visc,
+                                                          double* __restrict__ J) {
+  constexpr int SPW = 32 / NP;  // slots per warp
+  constexpr int MT = (NP + 7) / 8;  // row tiles of the face points
+  __shared__ double sOw[FACE_WARPS][SPW * NP * FW_OWN];
+  __shared__ double sOt[FACE_WARPS][SPW * NP * FW_OTH];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sl0 = (blockIdx.x * FACE_WARPS + warp) * SPW;
+  if (sl0 >= st.n) return;  // whole warps leave together
+  const int nsl = min(SPW, st.n - sl0);
+  double* ow_s = sOw[warp];
+  double* ot_s = sOt[warp];
+  for (int j = 0; j < nsl; ++j) {
+    const int sl = sl0 + j;
+    const int f = st.face[sl];
+    const int e = st.cell[sl];
+    const int fl = st.flags[sl];
+    const bool is_owner = (fl & 1) == 0;
+    const bool bnd = (fl & 2) != 0;
+    const int ax = (fl >> 2) & 3;
+    const int sb = (fl & 16) ? 1 : 0;
+    const int ct = cell_type(g, e);
+    // own side: rows face points, columns [q(5), adj row(3), grads + mu_t(13)]
+    const double* Er = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + sb) * S * NP;
+    const double* pf = PF + (size_t)e * S * PFW;
+    const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
+    double* ow = ow_s + j * NP * FW_OWN;
+    {
+      auto fa = [&](int i, int s) { return __ldg(Er + s * NP + i); };
+      auto fb = [&](int s, int n) {
+        return n < 5 ? __ldg(pf + s * PFW + n) : (n < 8 ? __ldg(ad + s * 9 + (n - 5)) : __ldg(pf + s * PFW + n - 3));
+      };
+      auto fc_ = [&](int i, int n, double x) { ow[i * FW_OWN + n] = x; };
+      if (visc) dmma_warp_rb<MT, 3, S>(NP, FW_OWN, fa, fb, fc_);
+      else dmma_warp_rb<MT, 1, S>(NP, 8, fa, fb, fc_);  // columns 8.. are not read without viscosity
+    }
+    // other side: the interpolation sources (the first, then the second added)
+    double* ot = ot_s + j * NP * FW_OTH;
+    if (!bnd) {
+      for (int src = 0; src < 2; ++src) {
+        const int c = src == 0 ? st.c0[sl] : st.c1[sl];
+        if (c < 0) {
+          if (src == 0)
+            for (int t = lane; t < NP * FW_OTH; t += 32) ot[t] = 0.0;
+          continue;
+        }
+        const double* M = src == 0 ? (is_owner ? fmat(fc.nb_m0, fc.nb_m0i, f, 0, NP, S)
+                                               : fmat(fc.ow_m0, fc.ow_m0i, f, 0, NP, S))
+                                   : (is_owner ? fmat(fc.nb_m1, fc.nb_m1i, st.i1[sl], 0, NP, S)
+                                               : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], 0, NP, S));
+        const double* pc = PF + (size_t)c * S * PFW;
+        __syncwarp();
+        auto fa = [&](int i, int s) { return __ldg(M + s * NP + i); };
+        auto fb = [&](int s, int n) { return __ldg(pc + s * PFW + n); };
+        auto fc_ = [&](int i, int n, double x) {
+          if (src == 0) ot[i * FW_OTH + n] = x;
+          else ot[i * FW_OTH + n] += x;
+        };
+        if (visc) dmma_warp_rb<MT, 3, S>(NP, FW_OTH, fa, fb, fc_);
+        else dmma_warp_rb<MT, 1, S>(NP, 5, fa, fb, fc_);  // columns 5.. are not read without viscosity
+      }
+    }
+  }
+  __syncwarp();
+  // flux phase: lane = slot-in-group * NP + face point
+  const int j = lane / NP, i = lane % NP;
+  if (j >= nsl || lane >= SPW * NP) return;
+  const int sl = sl0 + j;
   const int f = st.face[sl];
   const int e = st.cell[sl];
   const int fl = st.flags[sl];
   const bool is_owner = (fl & 1) == 0;
   const bool bnd = (fl & 2) != 0;
-  const int ax = (fl >> 2) & 3;
   const double side = (fl & 16) ? 1.0 : -1.0;
-  const int ct = cell_type(g, e);
-  // own-side extrapolation: q(5), adjugate row of this axis(3), grads+mu_t(13)
-  double ow[21];
+  double ow[21], ot[18];
 #pragma unroll
-  for (int k = 0; k < 21; ++k) ow[k] = 0.0;
-  {
-    const double* Er = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + (side < 0.0 ? 0 : 1)) * S * NP + i;
-    const double* pf = PF + (size_t)e * S * PFW;
-    const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
-#pragma unroll 3
-    for (int s = 0; s < S; ++s) {
-      const double w = __ldg(Er + s * NP);
-      double x[18];
-      ld18(pf + s * PFW, x);
-#pragma unroll
-      for (int k = 0; k < 5; ++k) ow[k] += w * x[k];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) ow[5 + d] += w * __ldg(ad + s * 9 + d);
-      if (visc) {
-#pragma unroll
-        for (int k = 0; k < 13; ++k) ow[8 + k] += w * x[5 + k];
-      }
-    }
-  }
-  // other side: interpolation sources (sum src0 then src1, zero weights skipped)
-  double ot[18];
-#pragma unroll
-  for (int k = 0; k < 18; ++k) ot[k] = 0.0;
+  for (int k = 0; k < 21; ++k) ow[k] = (k < 8 || visc) ? ow_s[(j * NP + i) * FW_OWN + k] : 0.0;
   const double* tn = fc.tnormal + ((size_t)f * NP + i) * 3;
   if (bnd) {
     double qo[5], n[3], gq[5];
@@ -342,30 +465,8 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
     for (int v = 0; v < 5; ++v) ot[v] = gq[v];
     for (int k = 0; k < 13; ++k) ot[5 + k] = ow[8 + k];
   } else {
-    for (int src = 0; src < 2; ++src) {
-      const int c = src == 0 ? st.c0[sl] : st.c1[sl];
-      if (c < 0) continue;
-      const double* M = src == 0 ? (is_owner ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S)
-                                             : fmat(fc.ow_m0, fc.ow_m0i, f, i, NP, S))
-                                 : (is_owner ? fmat(fc.nb_m1, fc.nb_m1i, st.i1[sl], i, NP, S)
-                                             : fmat(fc.ow_m1, fc.ow_m1i, st.i1[sl], i, NP, S));
-      const double* pf = PF + (size_t)c * S * PFW;
-#pragma unroll 3
-      for (int s = 0; s < S; ++s) {
-        const double w = __ldg(M + s * NP);
-        // the reference skips zero weights (inviscid_kernel_colored.py:117-121):
-        // a zero weight adds exactly nothing, even next to a non-finite value
-        const bool nz = w != 0.0;
-        double x[18];
-        ld18(pf + s * PFW, x);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) ot[k] += nz ? w * x[k] : 0.0;
-        if (visc) {
-#pragma unroll
-          for (int k = 0; k < 13; ++k) ot[5 + k] += nz ? w * x[5 + k] : 0.0;
-        }
-      }
-    }
+    for (int k = 0; k < 18; ++k) ot[k] = (k < 5 || visc) ? ot_s[(j * NP + i) * FW_OTH + k] : 0.0;
   }
   // pointwise fluxes
   const double a0 = ow[5], a1 = ow[6], a2 = ow[7];
@@ -378,7 +479,7 @@ __global__ void __launch_bounds__(128, 4) k_face(Geom g, Ops ops, Faces fc, Bc b
   double Fc[5], Fp[3][5];
   ausm_up(ow, ot, dir, Fc);
   euler_flux(ow, Fp);
-  double* Jo = J + (size_t)t * 10;
+  double* Jo = J + ((size_t)sl * NP + i) * 10;
   for (int v = 0; v < 5; ++v) Jo[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
   if (visc) {
     double qa[5], ga[13];

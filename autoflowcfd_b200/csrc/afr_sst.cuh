@@ -212,11 +212,11 @@ constexpr int SST_FACE_WARPS = 4;
 template <int S, int NP>
 __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
   constexpr int W = SST_FACE_WARPS, RW = 17;  // RW: po (8), pn of the first (4) and second (4) source, pad
+  constexpr int MT = (NP + 7) / 8;            // row tiles of the face points
   __shared__ double sR[W][NP * RW];
   const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int f = blockIdx.x * W + wi;
   if (f >= fc.F) return;  // whole warps: only warp-level synchronisation below
-  const int gq = lane >> 2, tq = lane & 3;
   const int oc = fc.owner[f];
   const int c0 = fc.nb_c0[f], i1 = fc.nb_i1[f];
   const int c1 = i1 >= 0 ? fc.nb_c1[i1] : -1;
@@ -227,43 +227,19 @@ __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops op
     const int ax = fc.o_axis[f];
     const double* ET = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * S * NP;
     const double* X = a.sp8 + (size_t)oc * S * 8;
-    for (int m0 = 0; m0 < NP; m0 += 8) {
-      const int i = m0 + gq;
-      double d0 = 0.0, d1 = 0.0;
-      for (int k0 = 0; k0 < S; k0 += 4) {
-        const int s = k0 + tq;
-        const double a0 = (i < NP && s < S) ? __ldg(ET + s * NP + i) : 0.0;
-        const double b0 = s < S ? __ldg(X + s * 8 + gq) : 0.0;
-        dmma884(d0, d1, a0, b0);
-      }
-      if (i < NP) {
-        R[i * RW + 2 * tq] = d0;
-        R[i * RW + 2 * tq + 1] = d1;
-      }
-    }
+    dmma_warp_rb<MT, 1, S>(
+        NP, 8, [&](int i, int s) { return __ldg(ET + s * NP + i); }, [&](int s, int n) { return __ldg(X + s * 8 + n); },
+        [&](int i, int n, double x) { R[i * RW + n] = x; });
   }
   if (!bnd) {
     for (int src = 0; src < 2; ++src) {
       const int c = src == 0 ? c0 : c1;
       if (c < 0) continue;
       const double* X = a.sp8 + (size_t)c * S * 8 + 4;
-      for (int m0 = 0; m0 < NP; m0 += 8) {
-        const int i = m0 + gq;
-        const double* M = i < NP ? (src == 0 ? fmat(fc.nb_m0, fc.nb_m0i, f, i, NP, S)
-                                             : fmat(fc.nb_m1, fc.nb_m1i, i1, i, NP, S))
-                                 : nullptr;
-        double d0 = 0.0, d1 = 0.0;
-        for (int k0 = 0; k0 < S; k0 += 4) {
-          const int s = k0 + tq;
-          const double a0 = (M && s < S) ? __ldg(M + s * NP) : 0.0;
-          const double b0 = (s < S && gq < 4) ? __ldg(X + s * 8 + gq) : 0.0;
-          dmma884(d0, d1, a0, b0);
-        }
-        if (i < NP && tq < 2) {
-          R[i * RW + 8 + src * 4 + 2 * tq] = d0;
-          R[i * RW + 8 + src * 4 + 2 * tq + 1] = d1;
-        }
-      }
+      const double* M = src == 0 ? fmat(fc.nb_m0, fc.nb_m0i, f, 0, NP, S) : fmat(fc.nb_m1, fc.nb_m1i, i1, 0, NP, S);
+      dmma_warp_rb<MT, 1, S>(
+          NP, 4, [&](int i, int s) { return __ldg(M + s * NP + i); }, [&](int s, int n) { return __ldg(X + s * 8 + n); },
+          [&](int i, int n, double x) { R[i * RW + 8 + src * 4 + n] = x; });
     }
   }
   __syncwarp();
