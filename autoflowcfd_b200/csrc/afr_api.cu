@@ -305,7 +305,14 @@ struct Launch {
   static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 2 : 1);
   static size_t cell_smem() { return sizeof(double) * CellSmem<S, FN, CPB, NP>::total; }
   static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
-    k_pre<S><<<h->N, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
+    constexpr int CPB = PreTile<S>::CPB;
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n > 0)
+        k_pre<S><<<(n + CPB - 1) / CPB, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF, ranges[r],
+                                                      ranges[r + 1]);
+    }
     return cudaGetLastError();
   }
   static cudaError_t stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm = nullptr) {
@@ -483,7 +490,14 @@ struct Launch {
 // integral's pre-pass) use the generic one-point kernels.
 struct LaunchP0 {
   static cudaError_t pre(afr_handle* h, const double* U, const double* nut, bool grads, cudaStream_t st) {
-    k_pre<1><<<h->N, 32, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF);
+    constexpr int CPB = PreTile<1>::CPB;
+    const int ranges[3] = {0, h->n_prism, h->N};
+    for (int r = 0; r < 2; ++r) {
+      const int n = ranges[r + 1] - ranges[r];
+      if (n > 0)
+        k_pre<1><<<(n + CPB - 1) / CPB, 128, 0, st>>>(h->g, h->ops, U, h->nv, nut, grads ? 1 : 0, h->PF, ranges[r],
+                                                      ranges[r + 1]);
+    }
     return cudaGetLastError();
   }
   static cudaError_t eval(afr_handle* h, StageArgs a, const double* U, const double* nut, bool grads,
@@ -1108,6 +1122,25 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
   h->g = Geom{h->N, h->n_prism, det, inv, adj, adjf, vol, mfs, wd, hvol};
 
   // ---- operators ----
+  // fragment-major image of an M x K operator whose element (m, k) is
+  // A[m * rs + k * cs] (layout in Ops)
+  auto frag_image = [](const double* A, size_t M, size_t K, size_t rs, size_t cs, std::vector<double>& out) {
+    const size_t MT = (M + 7) / 8, KS = (K + 3) / 4, base = out.size();
+    out.resize(base + MT * KS * 32, 0.0);
+    for (size_t mt = 0; mt < MT; ++mt)
+      for (size_t ks = 0; ks < KS; ++ks)
+        for (size_t l = 0; l < 32; ++l) {
+          const size_t mm = mt * 8 + l / 4, k = ks * 4 + l % 4;
+          if (mm < M && k < K) out[base + (mt * KS + ks) * 32 + l] = A[mm * rs + k * cs];
+        }
+  };
+  auto upload_frag = [&](double** d, const double* A, size_t M, size_t K, size_t rs, size_t cs) {
+    std::vector<double> img;
+    frag_image(A, M, K, rs, cs, img);
+    const int r = upload(h, d, img.data(), img.size(), st);
+    cudaStreamSynchronize(st);  // img leaves scope
+    return r;
+  };
   std::vector<double> Wkeep[2];
   for (int t = 0; t < 2; ++t) {
     const bool present = t == 0 ? h->n_prism > 0 : h->N > h->n_prism;
@@ -1145,6 +1178,19 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload(h, &wdev, Wh.data(), Wh.size(), st))) return bail(rc);
     cudaStreamSynchronize(st);
     h->ops.W[t] = wdev;
+    {
+      double *fd3, *fd3g, *fc2f, *fw, *fflt;
+      if ((rc = upload_frag(&fd3, m->D_3d[t], S, 3 * S, 3 * S, 1))) return bail(rc);
+      if ((rc = upload_frag(&fd3g, g2.data(), 3 * S, S, S, 1))) return bail(rc);
+      if ((rc = upload_frag(&fc2f, c2f_h, Fn, S, S, 1))) return bail(rc);
+      if ((rc = upload_frag(&fw, Wh.data(), S, 3 * Fn, 3 * Fn, 1))) return bail(rc);
+      if ((rc = upload_frag(&fflt, m->filter[t], S, S, S, 1))) return bail(rc);
+      h->ops.fD3[t] = fd3;
+      h->ops.fD3g[t] = fd3g;
+      h->ops.fc2f[t] = fc2f;
+      h->ops.fW[t] = fw;
+      h->ops.ffilt[t] = fflt;
+    }
     Wkeep[t] = Wh;
     h->ops.D3[t] = d3;
     h->ops.D3g[t] = d3g;
@@ -1164,6 +1210,12 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     if ((rc = upload(h, &gr, m->g_right, (size_t)n1d, st))) return bail(rc);
     if ((rc = upload_i32(h, &dfp, m->dist_fp_of_sp, 3 * S, st, tmp))) return bail(rc);
     if ((rc = upload_i32(h, &dco, m->dist_axis_coord_of_sp, 3 * S, st, tmp))) return bail(rc);
+    std::vector<double> fex;
+    for (int q = 0; q < 12; ++q) frag_image(m->boundary_extrap + (size_t)q * P * S, P, S, S, 1, fex);
+    double* fexd;
+    if ((rc = upload(h, &fexd, fex.data(), fex.size(), st))) return bail(rc);
+    cudaStreamSynchronize(st);  // fex leaves scope
+    h->ops.fextrap = fexd;
     h->ops.extrap = ex;
     h->ops.extrapT = exT;
     h->ops.g_left = gl;

@@ -46,6 +46,16 @@ struct Ops {
   const double* g_right;    // (n1d)
   const int32_t* dist_fp;   // (3, S)
   const int32_t* dist_co;   // (3, S)
+  // fragment-major images of the A operands of the FP64 tensor-core products
+  // (element (m, k) of an M x K operator at [((m/8) * ceil(K/4) + k/4) * 32 +
+  // (m%8) * 4 + k%4], zero outside the operator): one warp's fragment load is
+  // 256 contiguous bytes
+  const double* fD3[2];     // D3 as (S, 3S)
+  const double* fD3g[2];    // D3g (3S, S)
+  const double* fc2f[2];    // c2f (Fn, S)
+  const double* fW[2];      // W (S, 3Fn)
+  const double* ffilt[2];   // filt (S, S)
+  const double* fextrap;    // extrap: 12 images of (P, S), ceil(P/8) * ceil(S/4) * 32 doubles each
 };
 
 struct Geom {

@@ -105,6 +105,32 @@ __device__ __forceinline__ void dmma_product(int M, int N, int K, FA a, FB b, FC
   }
 }
 
+// dmma_product with A read from a fragment-major image (layout in Ops): one
+// contiguous 256-byte load per warp and k-step; the image's zeros stand for
+// the rows and columns outside the operator
+template <class FB, class FC>
+__device__ __forceinline__ void dmma_product_f(int M, int N, int K, const double* __restrict__ Af, FB b, FC c) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3, KS = (K + 3) >> 2;
+  for (int tile = threadIdx.x >> 5; tile < mt * nt; tile += nw) {
+    const int mi = tile / nt, m = mi * 8 + g, n0 = (tile % nt) * 8;
+    const double* ap = Af + (size_t)mi * KS * 32 + lane;
+    double c0 = 0.0, c1 = 0.0;
+    for (int ks = 0; ks < KS; ++ks) {
+      const int k = ks * 4 + t;
+      const double a0 = __ldg(ap + ks * 32);
+      const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
+      dmma884(c0, c1, a0, b0);
+    }
+    const int n = n0 + 2 * t;
+    if (m < M) {
+      if (n < N) c(m, n, c0);
+      if (n + 1 < N) c(m, n + 1, c1);
+    }
+  }
+}
+
 // Median-based outlier zeroing (core/fr_operators/troubled_cell.py:346-408):
 // per cell and variable, |R| > 1e4 * max(median |R|, 1e-9 mean|U|, 1e-300)
 // is set to zero.  A column has nothing to zero when that threshold is at
@@ -230,37 +256,61 @@ __device__ void suppress_outliers_cells(double* sRi, double* sRv, const double* 
 constexpr int PFW = 18;
 
 template <int S>
+struct PreTile {
+  static constexpr int CPB = S <= 8 ? 16 : (S <= 27 ? 4 : 2);  // cells per CTA
+};
+
+// CPB cells per CTA; cells [cell_base, cell_end) share one cell type.  The
+// reference-space gradients are one FP64 tensor-core product (rows s*3+m of
+// D3g, columns (cell, field)); the tile's PF rows are assembled in shared
+// memory and stored as one contiguous block.
+template <int S>
 __global__ void __launch_bounds__(128) k_pre(Geom g, Ops ops, const double* __restrict__ U, int nv,
                                              const double* __restrict__ nut, int want_grads,
-                                             double* __restrict__ PF) {
-  __shared__ double f[S * 4];
-  __shared__ double gc[S * 3 * 4];
-  const int e = blockIdx.x;
-  const int ct = cell_type(g, e);
-  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+                                             double* __restrict__ PF, int cell_base, int cell_end) {
+  constexpr int CPB = PreTile<S>::CPB;
+  __shared__ double sPF[CPB * S * PFW];
+  __shared__ double f[CPB * S * 4];
+  __shared__ double gc[CPB * S * 3 * 4];
+  const int e0 = cell_base + blockIdx.x * CPB;
+  const int nc = min(CPB, cell_end - e0);
+  const int ct = cell_type(g, e0);
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+    const size_t p = (size_t)e0 * S + t;
     double q[5];
-    const double* u = U + ((size_t)e * S + s) * nv;
+    const double* u = U + p * nv;
     cons_to_prim(u, q);
-    double* o = PF + ((size_t)e * S + s) * PFW;
+    double* o = sPF + t * PFW;
     for (int v = 0; v < 5; ++v) o[v] = q[v];
-    o[17] = nut ? fmax(u[0], 1e-10) * nut[(size_t)e * S + s] : 0.0;
-    f[s * 4 + 0] = q[1];
-    f[s * 4 + 1] = q[2];
-    f[s * 4 + 2] = q[3];
-    f[s * 4 + 3] = q[4] / (fmax(q[0], 1e-10) * R_AIR);
+    o[17] = nut ? fmax(u[0], 1e-10) * nut[p] : 0.0;
+    f[t * 4 + 0] = q[1];
+    f[t * 4 + 1] = q[2];
+    f[t * 4 + 2] = q[3];
+    f[t * 4 + 3] = q[4] / (fmax(q[0], 1e-10) * R_AIR);
   }
-  if (!want_grads) return;
   __syncthreads();
-  block_gemm<S * 3, 4, S>(gc, 4, ops.D3g[ct], S, f, 4);
-  __syncthreads();
-  for (int t = threadIdx.x; t < S * 12; t += blockDim.x) {
-    const int s = t / 12, c = t % 12;
-    const int q = c / 3, n = c % 3;  // c = q*3+n: q in (u,v,w,T)
-    const double* inv = g.inv + ((size_t)e * S + s) * 9;
-    double acc = 0.0;
-    for (int m = 0; m < 3; ++m) acc += gc[(s * 3 + m) * 4 + q] * inv[m * 3 + n];
-    PF[((size_t)e * S + s) * PFW + 5 + c] = acc;
+  if (want_grads) {
+    dmma_product_f(
+        3 * S, 4 * nc, S, ops.fD3g[ct], [&](int j, int col) { return f[((col >> 2) * S + j) * 4 + (col & 3)]; },
+        [&](int r, int col, double x) { gc[((col >> 2) * S * 3 + r) * 4 + (col & 3)] = x; });
+    __syncthreads();
+    for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
+      double inv[9];
+      const double* ip = g.inv + ((size_t)e0 * S + t) * 9;
+      for (int k = 0; k < 9; ++k) inv[k] = __ldg(ip + k);
+      for (int c = 0; c < 12; ++c) {
+        const int q = c / 3, n = c % 3;  // c = q*3+n: q in (u,v,w,T)
+        double acc = 0.0;
+        for (int m = 0; m < 3; ++m) acc += gc[(t * 3 + m) * 4 + q] * inv[m * 3 + n];
+        sPF[t * PFW + 5 + c] = acc;
+      }
+    }
+  } else {
+    for (int t = threadIdx.x; t < nc * S * 12; t += blockDim.x) sPF[(t / 12) * PFW + 5 + t % 12] = 0.0;
   }
+  __syncthreads();
+  double* out = PF + (size_t)e0 * S * PFW;
+  for (int t = threadIdx.x; t < nc * S * PFW; t += blockDim.x) out[t] = sPF[t];
 }
 
 // ---------------------------------------------------------------------------
@@ -359,6 +409,45 @@ __device__ __forceinline__ void dmma_warp_rb(int M, int N, FA a, FB b, FC c) {
     }
 }
 
+// dmma_warp_rb with A read from a fragment-major image (layout in Ops) of an
+// operator with at most MT * 8 rows and K columns
+template <int MT, int NT, int K, class FB, class FC>
+__device__ __forceinline__ void dmma_warp_rb_f(int M, int N, const double* __restrict__ Af, FB b, FC c) {
+  constexpr int KS = (K + 3) / 4;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double acc[MT][NT][2];
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    const int k = ks * 4 + t;
+    double av[MT], bv[NT];
+#pragma unroll
+    for (int mi = 0; mi < MT; ++mi) av[mi] = __ldg(Af + (mi * KS + ks) * 32 + lane);
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) {
+      const int n = ni * 8 + g;
+      bv[ni] = (n < N && k < K) ? b(k, n) : 0.0;
+    }
+#pragma unroll
+    for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) dmma884(acc[mi][ni][0], acc[mi][ni][1], av[mi], bv[ni]);
+  }
+#pragma unroll
+  for (int mi = 0; mi < MT; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) {
+      const int m = mi * 8 + g, n = ni * 8 + 2 * t;
+      if (m < M) {
+        if (n < N) c(m, n, acc[mi][ni][0]);
+        if (n + 1 < N) c(m, n + 1, acc[mi][ni][1]);
+      }
+    }
+}
+
 // Face kernel: one warp per group of SPW = 32 / NP slots (a slot is one side
 // of one face record whose correction lifts into a cell; lane = slot-in-group
 // * NP + flux point in the flux phase).  Per slot, the own side's
@@ -402,18 +491,17 @@ __global__ void __launch_bounds__(32 * FACE_WARPS, 4) k_face(Geom g, Ops ops, Fa
     const int sb = (fl & 16) ? 1 : 0;
     const int ct = cell_type(g, e);
     // own side: rows face points, columns [q(5), adj row(3), grads + mu_t(13)]
-    const double* Er = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + sb) * S * NP;
+    const double* Ef = ops.fextrap + (((size_t)ct * 3 + ax) * 2 + sb) * (MT * ((S + 3) / 4) * 32);
     const double* pf = PF + (size_t)e * S * PFW;
     const double* ad = g.adj + (size_t)e * S * 9 + ax * 3;
     double* ow = ow_s + j * NP * FW_OWN;
     {
-      auto fa = [&](int i, int s) { return __ldg(Er + s * NP + i); };
       auto fb = [&](int s, int n) {
         return n < 5 ? __ldg(pf + s * PFW + n) : (n < 8 ? __ldg(ad + s * 9 + (n - 5)) : __ldg(pf + s * PFW + n - 3));
       };
       auto fc_ = [&](int i, int n, double x) { ow[i * FW_OWN + n] = x; };
-      if (visc) dmma_warp_rb<MT, 3, S>(NP, FW_OWN, fa, fb, fc_);
-      else dmma_warp_rb<MT, 1, S>(NP, 8, fa, fb, fc_);  // columns 8.. are not read without viscosity
+      if (visc) dmma_warp_rb_f<MT, 3, S>(NP, FW_OWN, Ef, fb, fc_);
+      else dmma_warp_rb_f<MT, 1, S>(NP, 8, Ef, fb, fc_);  // columns 8.. are not read without viscosity
     }
     // other side: the interpolation sources (the first, then the second added)
     double* ot = ot_s + j * NP * FW_OTH;
@@ -573,9 +661,8 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   // ---- Q at fine points (c2f, an FP64 tensor-core product: rows the fine
   // points, columns (cell, variable)) and viscous contravariant fluxes ----
   {
-    const double* C2F = ops.c2f[ct];
-    dmma_product(
-        FN, 5 * nc, S, [&](int i, int s) { return __ldg(C2F + (size_t)i * S + s); },
+    dmma_product_f(
+        FN, 5 * nc, S, ops.fc2f[ct],
         [&](int s, int col) { return sPF[((col / 5) * S + s) * PFW + col % 5]; },
         [&](int i, int col, double x) { sQf[((col / 5) * FN + i) * 5 + col % 5] = x; });
   }
@@ -610,18 +697,16 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   // the fine-point fluxes, viscous D3 (S x 3S) to the point fluxes; rows the
   // solution points, columns (cell, variable) ----
   {
-    const double* Wm = ops.W[ct];
-    dmma_product(
-        S, 5 * nc, FN * 3, [&](int s, int k) { return __ldg(Wm + (size_t)s * FN * 3 + k); },
+    dmma_product_f(
+        S, 5 * nc, FN * 3, ops.fW[ct],
         [&](int k, int col) { return sFt[(col / 5) * FN * 15 + k * 5 + col % 5]; },
         [&](int s, int col, double x) {
           const int b = col / 5;
           sRi[(b * S + s) * 5 + col % 5] = -x / sDet[b * S + s];
         });
     if (visc) {
-      const double* Dm = ops.D3[ct];
-      dmma_product(
-          S, 5 * nc, S * 3, [&](int s, int k) { return __ldg(Dm + (size_t)s * S * 3 + k); },
+      dmma_product_f(
+          S, 5 * nc, S * 3, ops.fD3[ct],
           [&](int k, int col) { return sGt[(col / 5) * S * 15 + k * 5 + col % 5]; },
           [&](int s, int col, double x) {
             const int b = col / 5;
@@ -713,9 +798,8 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   __syncthreads();
   // modal filter on the first five variables as an FP64 tensor-core product
   // (rows s, columns (cell, variable), K the cell's points)
-  const double* Fm = ops.filt[ct];
-  dmma_product(
-      S, 5 * nc, S, [&](int s, int j) { return __ldg(Fm + (size_t)s * S + j); },
+  dmma_product_f(
+      S, 5 * nc, S, ops.ffilt[ct],
       [&](int j, int col) { return Up[((col / 5) * S + j) * US + col % 5]; },
       [&](int s, int col, double x) { a.Unext[((size_t)(e0 + col / 5) * S + s) * nv + col % 5] = x; });
   for (int p = tid; p < nc * S; p += blockDim.x)

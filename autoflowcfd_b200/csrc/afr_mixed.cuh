@@ -1239,9 +1239,8 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   // outputs are assembled in the residual buffers (no longer needed) and
   // stored as one contiguous block
   double* sOut = sRi;  // (nc*S, nv) row-major, fits in sRi + sRv
-  const double* Fm = ops.filt[ct];
-  dmma_product(
-      S, 5 * nc, S, [&](int s, int j) { return __ldg(Fm + s * S + j); },
+  dmma_product_f(
+      S, 5 * nc, S, ops.ffilt[ct],
       [&](int j, int col) { return sU[((col / 5) * S + j) * nv + col % 5]; },
       [&](int s, int col, double x) { sOut[((col / 5) * S + s) * nv + col % 5] = x; });
   for (int p = tid; p < nc * S; p += blockDim.x)

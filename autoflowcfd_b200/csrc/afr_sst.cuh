@@ -100,9 +100,8 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
   // reference-space gradients (rows s*3+m of D3g) as one FP64 tensor-core
   // product: columns (cell, field)
   {
-    const double* D = ct ? ops.D3g[1] : ops.D3g[0];
-    dmma_product(
-        3 * S, 5 * nc, S, [&](int r, int j) { return __ldg(D + r * S + j); },
+    dmma_product_f(
+        3 * S, 5 * nc, S, ops.fD3g[ct],
         [&](int j, int col) { return f[((col / 5) * S + j) * 5 + col % 5]; },
         [&](int r, int col, double x) { gc[((col / 5) * S * 3 + r) * 5 + col % 5] = x; });
   }
@@ -225,10 +224,11 @@ __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops op
   {
     const int ct = cell_type(g, oc);
     const int ax = fc.o_axis[f];
-    const double* ET = ops.extrapT + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * S * NP;
+    const double* Ef =
+        ops.fextrap + (((size_t)ct * 3 + ax) * 2 + (fc.o_side[f] <= 0.0 ? 0 : 1)) * (MT * ((S + 3) / 4) * 32);
     const double* X = a.sp8 + (size_t)oc * S * 8;
-    dmma_warp_rb<MT, 1, S>(
-        NP, 8, [&](int i, int s) { return __ldg(ET + s * NP + i); }, [&](int s, int n) { return __ldg(X + s * 8 + n); },
+    dmma_warp_rb_f<MT, 1, S>(
+        NP, 8, Ef, [&](int s, int n) { return __ldg(X + s * 8 + n); },
         [&](int i, int n, double x) { R[i * RW + n] = x; });
   }
   if (!bnd) {
@@ -319,9 +319,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   // grad k, grad w in reference space (D3g rows s*3+m) as one FP64
   // tensor-core product: columns (cell, field)
   {
-    const double* D = ct ? ops.D3g[1] : ops.D3g[0];
-    dmma_product(
-        3 * S, 2 * nc, S, [&](int r, int j) { return __ldg(D + r * S + j); },
+    dmma_product_f(
+        3 * S, 2 * nc, S, ops.fD3g[ct],
         [&](int j, int col) { return fl[((col >> 1) * S + j) * 9 + (col & 1)]; },
         [&](int r, int col, double x) { gc[((col >> 1) * S * 3 + r) * 2 + (col & 1)] = x; });
   }
@@ -357,9 +356,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   // (K = (j, m), columns (cell, field)); then the face corrections of every
   // face side in ascending color order
   {
-    const double* D = ct ? ops.D3[1] : ops.D3[0];
-    dmma_product(
-        S, 4 * nc, 3 * S, [&](int s, int k) { return __ldg(D + s * S * 3 + k); },
+    dmma_product_f(
+        S, 4 * nc, 3 * S, ops.fD3[ct],
         [&](int k, int col) { return Ft[((col >> 2) * S * 3 + k) * 4 + (col & 3)]; },
         [&](int s, int col, double x) {
           const int b = col >> 2;
