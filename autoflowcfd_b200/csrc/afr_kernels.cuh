@@ -619,7 +619,8 @@ struct CellSmem {
   static constexpr int oGt = oFt + CPB * FN * 15;  // CPB*S*15
   static constexpr int oJ = oGt + CPB * S * 15;    // staged jumps of the CTA's slots
   static constexpr int oWp = oJ + CPB * CELL_MAXSLOT * NPMAX * 10;  // 2 halves of the W divergence
-  static constexpr int work = oWp + 2 * CPB * S * 5;  // CPB*2*OUT_WORK (outliers) + 32
+  static constexpr int oAf = oWp + 2 * CPB * S * 5;  // CPB*FN*9 adjugates at the fine points
+  static constexpr int work = oAf + CPB * FN * 9;     // CPB*2*OUT_WORK (outliers) + 32
   static constexpr int total = work + CPB * 2 * OUT_WORK + 32;
 };
 
@@ -645,17 +646,22 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   const bool visc = !a.inviscid_only;
   const int tid = threadIdx.x;
 
-  // ---- load ----
-  for (int t = tid; t < nc * S * PFW; t += blockDim.x) sPF[t] = a.PF[(size_t)e0 * S * PFW + t];
-  for (int t = tid; t < nc * S * 9; t += blockDim.x) sAdj[t] = g.adj[(size_t)e0 * S * 9 + t];
-  for (int t = tid; t < nc * S * nv; t += blockDim.x) sU[(t / nv) * US + t % nv] = a.Ucur[(size_t)e0 * S * nv + t];
-  for (int t = tid; t < nc * S; t += blockDim.x) sDet[t] = g.det[(size_t)e0 * S + t];
+  double* sAf = sm + L::oAf;
+  // ---- load: asynchronous 8-byte copies, all in flight at once ----
+  for (int t = tid; t < nc * S * PFW; t += blockDim.x) cp_async8(sPF + t, a.PF + (size_t)e0 * S * PFW + t);
+  for (int t = tid; t < nc * S * 9; t += blockDim.x) cp_async8(sAdj + t, g.adj + (size_t)e0 * S * 9 + t);
+  for (int t = tid; t < nc * S * nv; t += blockDim.x)
+    cp_async8(sU + (t / nv) * US + t % nv, a.Ucur + (size_t)e0 * S * nv + t);
+  for (int t = tid; t < nc * S; t += blockDim.x) cp_async8(sDet + t, g.det + (size_t)e0 * S + t);
+  for (int t = tid; t < nc * FN * 9; t += blockDim.x) cp_async8(sAf + t, g.adj_fine + (size_t)e0 * FN * 9 + t);
   // the jumps of this CTA's slots are contiguous (slots are stored cell-major)
   const int k_beg = fc.slot_ptr[e0], k_end = fc.slot_ptr[e0 + nc];
   const bool staged = (k_end - k_beg) <= CPB * CELL_MAXSLOT;
   double* sJ = sm + L::oJ;
   if (staged)
-    for (int t = tid; t < (k_end - k_beg) * NP * 10; t += blockDim.x) sJ[t] = J[(size_t)k_beg * NP * 10 + t];
+    for (int t = tid; t < (k_end - k_beg) * NP * 10; t += blockDim.x)
+      cp_async8(sJ + t, J + (size_t)k_beg * NP * 10 + t);
+  cp_async_wait_all();
   __syncthreads();
 
   // ---- Q at fine points (c2f, an FP64 tensor-core product: rows the fine
@@ -685,9 +691,9 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
     double q[5], F[3][5];
     for (int v = 0; v < 5; ++v) q[v] = sQf[t * 5 + v];
     euler_flux(q, F);
-    const double* ad = g.adj_fine + ((size_t)(e0 + b) * FN + i) * 9;
+    const double* ad = sAf + (size_t)(b * FN + i) * 9;
     double am[9];
-    for (int k = 0; k < 9; ++k) am[k] = __ldg(ad + k);
+    for (int k = 0; k < 9; ++k) am[k] = ad[k];
     for (int m = 0; m < 3; ++m)
       for (int v = 0; v < 5; ++v)
         sFt[(t * 3 + m) * 5 + v] = am[m * 3 + 0] * F[0][v] + am[m * 3 + 1] * F[1][v] + am[m * 3 + 2] * F[2][v];
