@@ -131,6 +131,42 @@ __device__ __forceinline__ void dmma_product_f(int M, int N, int K, const double
   }
 }
 
+// dmma_product_f with each warp computing all column tiles of a row tile
+// (at most NT of them): the A fragment is loaded once per k-step and the NT
+// accumulations are independent, so their tensor-core latencies overlap.  Per
+// element the k-steps accumulate in the same order as dmma_product_f.
+template <int NT, class FB, class FC>
+__device__ __forceinline__ void dmma_product_rb(int M, int N, int K, const double* __restrict__ Af, FB b, FC c) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  const int mt = (M + 7) >> 3, KS = (K + 3) >> 2;
+  for (int mi = threadIdx.x >> 5; mi < mt; mi += nw) {
+    const double* ap = Af + (size_t)mi * KS * 32 + lane;
+    double acc[NT][2];
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni) acc[ni][0] = acc[ni][1] = 0.0;
+    for (int ks = 0; ks < KS; ++ks) {
+      const int k = ks * 4 + t;
+      const double a0 = __ldg(ap + ks * 32);
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) {
+        const int n = ni * 8 + g;
+        const double b0 = (k < K && n < N) ? b(k, n) : 0.0;
+        dmma884(acc[ni][0], acc[ni][1], a0, b0);
+      }
+    }
+    const int m = mi * 8 + g;
+    if (m < M) {
+#pragma unroll
+      for (int ni = 0; ni < NT; ++ni) {
+        const int n = ni * 8 + 2 * t;
+        if (n < N) c(m, n, acc[ni][0]);
+        if (n + 1 < N) c(m, n + 1, acc[ni][1]);
+      }
+    }
+  }
+}
+
 // Median-based outlier zeroing (core/fr_operators/troubled_cell.py:346-408):
 // per cell and variable, |R| > 1e4 * max(median |R|, 1e-9 mean|U|, 1e-300)
 // is set to zero.  A column has nothing to zero when that threshold is at
@@ -202,11 +238,13 @@ __device__ __forceinline__ void outlier_zero(double* R, int r, int v, const doub
 // Uref + b*S*ldU (first 5 columns), all blocks in one pass per phase.  work >= OUT_WORK doubles per block.
 template <int S>
 __device__ void suppress_outliers_blocks(double* R, const double* Uref, int ldU, int nb, double* work) {
+  int flagged = 0;
   for (int t = threadIdx.x; t < nb * 5; t += blockDim.x) {
     const int b = t / 5, v = t % 5;
     outlier_column<S>(R + b * S * 5, Uref + b * S * ldU, ldU, v, work + b * OUT_WORK);
+    flagged |= work[b * OUT_WORK + 20 + v] != 0.0;
   }
-  __syncthreads();
+  if (!__syncthreads_or(flagged)) return;  // no column takes the rank pass: nothing is zeroed
   for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
     const int b = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     double* w = work + b * OUT_WORK;
@@ -227,12 +265,14 @@ __device__ void suppress_outliers_blocks(double* R, const double* Uref, int ldU,
 template <int S>
 __device__ void suppress_outliers_cells(double* sRi, double* sRv, const double* sU, int nc, bool visc, double* work) {
   const int nb = nc * (visc ? 2 : 1);
+  int flagged = 0;
   for (int t = threadIdx.x; t < nb * 5; t += blockDim.x) {
     const int bb = t / 5, v = t % 5;
     const double* R = bb < nc ? sRi + bb * S * 5 : sRv + (bb - nc) * S * 5;
     outlier_column<S>(R, sU + (bb % nc) * S * US, US, v, work + bb * OUT_WORK);
+    flagged |= work[bb * OUT_WORK + 20 + v] != 0.0;
   }
-  __syncthreads();
+  if (!__syncthreads_or(flagged)) return;  // no column takes the rank pass: nothing is zeroed
   for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
     const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     double* w = work + bb * OUT_WORK;
@@ -290,7 +330,7 @@ __global__ void __launch_bounds__(128) k_pre(Geom g, Ops ops, const double* __re
   }
   __syncthreads();
   if (want_grads) {
-    dmma_product_f(
+    dmma_product_rb<(4 * CPB + 7) / 8>(
         3 * S, 4 * nc, S, ops.fD3g[ct], [&](int j, int col) { return f[((col >> 2) * S + j) * 4 + (col & 3)]; },
         [&](int r, int col, double x) { gc[((col >> 2) * S * 3 + r) * 4 + (col & 3)] = x; });
     __syncthreads();
@@ -667,7 +707,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 3) k_cell(Geom g, Ops ops, Faces
   // ---- Q at fine points (c2f, an FP64 tensor-core product: rows the fine
   // points, columns (cell, variable)) and viscous contravariant fluxes ----
   {
-    dmma_product_f(
+    dmma_product_rb<(5 * CPB + 7) / 8>(
         FN, 5 * nc, S, ops.fc2f[ct],
         [&](int s, int col) { return sPF[((col / 5) * S + s) * PFW + col % 5]; },
         [&](int i, int col, double x) { sQf[((col / 5) * FN + i) * 5 + col % 5] = x; });

@@ -996,6 +996,7 @@ __device__ void mx_suppress_outliers(double* sRi, double* sRv, const double* sU,
   const int nb = nc * (visc ? 2 : 1);
   const int ncol = nb * 5;
   const int n4 = (ncol * 4 + (int)blockDim.x - 1) / (int)blockDim.x * (int)blockDim.x;
+  int flagged = 0;
   for (int base = 0; base < n4; base += blockDim.x) {
     const int t = base + threadIdx.x;
     const bool on = t < ncol * 4;
@@ -1044,9 +1045,10 @@ __device__ void mx_suppress_outliers(double* sRi, double* sRv, const double* sU,
       w[5 + v] = mean;
       w[v] = bound;
       w[20 + v] = skip ? 0.0 : 1.0;
+      flagged |= !skip;
     }
   }
-  __syncthreads();
+  if (!__syncthreads_or(flagged)) return;  // no column takes the rank pass: nothing is zeroed
   for (int t = threadIdx.x; t < nb * S * 5; t += blockDim.x) {
     const int bb = t / (S * 5), r = t % (S * 5), s = r / 5, v = r % 5;
     double* w = work + bb * OUT_WORK;
@@ -1239,7 +1241,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   // outputs are assembled in the residual buffers (no longer needed) and
   // stored as one contiguous block
   double* sOut = sRi;  // (nc*S, nv) row-major, fits in sRi + sRv
-  dmma_product_f(
+  dmma_product_rb<(5 * CPB + 7) / 8>(
       S, 5 * nc, S, ops.ffilt[ct],
       [&](int j, int col) { return sU[((col / 5) * S + j) * nv + col % 5]; },
       [&](int s, int col, double x) { sOut[((col / 5) * S + s) * nv + col % 5] = x; });

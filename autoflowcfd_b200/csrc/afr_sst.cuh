@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
   // reference-space gradients (rows s*3+m of D3g) as one FP64 tensor-core
   // product: columns (cell, field)
   {
-    dmma_product_f(
+    dmma_product_rb<(5 * CPB + 7) / 8>(
         3 * S, 5 * nc, S, ops.fD3g[ct],
         [&](int j, int col) { return f[((col / 5) * S + j) * 5 + col % 5]; },
         [&](int r, int col, double x) { gc[((col / 5) * S * 3 + r) * 5 + col % 5] = x; });
@@ -275,46 +275,76 @@ __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops op
 
 // per cell: volume transport terms, gather of the face corrections, outlier
 // suppression and the point-implicit k / omega update.  CPB cells per CTA.
+// transport slots of a tile whose corrections are staged in shared memory
+// (6 per cell at P1 / P2; at P3 there is no room and they are read from global)
+template <int S>
+__host__ __device__ constexpr int sst_stage_slots() { return S <= 27 ? SstTile<S>::CPB * 6 : 1; }
+
+// 16-byte asynchronous copy global -> shared (both 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
 template <int S, int NP>
 __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a, int cell_base,
                                                     int cell_end) {
   constexpr int CPB = SstTile<S>::CPB;
+  // the face corrections of the tile's transport slots (slot j's face rows at
+  // sC + j*NP*4), copied at the start so they arrive during the volume terms
+  constexpr int NSTG = sst_stage_slots<S>();
+  __shared__ __align__(16) double sC[NSTG * NP * 4];
   // point values packed by k_sst_point, row stride 9: rho (clamped as the
   // reference's), u, v, w, k, omega, gamma_k, gamma_w
   __shared__ double sP[CPB * S * 9];
   __shared__ double gc[CPB * S * 3 * 2];  // reference-space grads of k, w
   __shared__ double Ft[CPB * S * 3 * 4];  // contravariant fluxes: conv k, diff k, conv w, diff w
-  // inverse Jacobians and adjugates (rows of 9) until the fluxes are formed;
-  // then R (volume residuals, then with the interface corrections), T
-  // (transport k, w + padding for the outlier helper) and Ref
-  __shared__ double X[CPB * S * 18];
+  // inverse Jacobians (rows of 9) until the fluxes are formed; then R (volume
+  // residuals, then with the interface corrections), T (transport k, w +
+  // padding for the outlier helper) and Ref
+  __shared__ double X[CPB * S * 14];
   __shared__ double sRd[CPB * S];         // det, then 1 / det
   __shared__ double work[CPB * OUT_WORK];
+  __shared__ double sG[8];                // g_left, g_right
+  __shared__ int sCode[NSTG];
+  __shared__ int sDfp[3 * S], sDco[3 * S];
   double* sInv = X;
-  double* sAdj = X + CPB * S * 9;
   double* R = X;
   double* T = X + CPB * S * 4;
   double* Ref = X + CPB * S * 9;
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
-  // the tile's blocks are contiguous: asynchronous 8-byte copies, all in flight at once
+  // the tile's transport slots are contiguous (cell-major)
+  const int k_beg = fc.tslot_ptr[e0], k_end = fc.tslot_ptr[e0 + nc];
+  const bool staged = S <= 27 && k_end - k_beg <= NSTG;
+  // the tile's blocks are contiguous: asynchronous copies, all in flight at once
   {
     const double* pb = a.sp8 + (size_t)e0 * S * 8;
     for (int t = threadIdx.x; t < nc * S * 8; t += blockDim.x) cp_async8(sP + (t >> 3) * 9 + (t & 7), pb + t);
     const double* ib = g.inv + (size_t)e0 * S * 9;
-    const double* ab = g.adj + (size_t)e0 * S * 9;
-    for (int t = threadIdx.x; t < nc * S * 9; t += blockDim.x) {
-      cp_async8(sInv + t, ib + t);
-      cp_async8(sAdj + t, ab + t);
-    }
+    for (int t = threadIdx.x; t < nc * S * 9; t += blockDim.x) cp_async8(sInv + t, ib + t);
     for (int t = threadIdx.x; t < nc * S; t += blockDim.x) cp_async8(sRd + t, g.det + (size_t)e0 * S + t);
+    if (staged)
+      for (int t = threadIdx.x; t < (k_end - k_beg) * NP * 2; t += blockDim.x) {
+        const int j = t / (NP * 2), q = t - j * (NP * 2);
+        const int face = __ldg(fc.tslot + k_beg + j) >> 4;
+        cp_async16(sC + j * NP * 4 + 2 * q, a.cfp + (size_t)face * NP * 4 + 2 * q);
+      }
+    if (staged)
+      for (int t = threadIdx.x; t < k_end - k_beg; t += blockDim.x) sCode[t] = __ldg(fc.tslot + k_beg + t);
+    for (int t = threadIdx.x; t < 3 * S; t += blockDim.x) {
+      sDfp[t] = __ldg(ops.dist_fp + t);
+      sDco[t] = __ldg(ops.dist_co + t);
+    }
+    if (threadIdx.x < 4) {
+      constexpr int N1D = S == 1 ? 1 : (S == 8 ? 2 : (S == 27 ? 3 : 4));
+      sG[threadIdx.x] = threadIdx.x < N1D ? ops.g_left[threadIdx.x] : 0.0;
+      sG[4 + threadIdx.x] = threadIdx.x < N1D ? ops.g_right[threadIdx.x] : 0.0;
+    }
     cp_async_wait_all();
   }
   __syncthreads();
-  // one reciprocal of det per point (published by the next barrier): each use
-  // differs from a division by det by at most an ulp
-  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) sRd[t] = 1.0 / sRd[t];
   const double* fl = sP + 4;  // k, w, gamma_k, gamma_w of point p at fl[p * 9 + 0..3]
   // grad k, grad w in reference space (D3g rows s*3+m) as one FP64
   // tensor-core product: columns (cell, field)
@@ -327,7 +357,11 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   __syncthreads();
   for (int t = threadIdx.x; t < nc * S; t += blockDim.x) {
     const double* inv = sInv + t * 9;
-    const double* adj = sAdj + t * 9;
+    // adjugate rows det * inv, formed here exactly as at create
+    const double det = sRd[t];
+    double adj[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) adj[k] = det * inv[k];
     const double* pv = sP + t * 9;  // rho = max(U0, 1e-10) and u = U1..3 / rho, as formed by k_sst_point
     const double rho = pv[0];
     const double vel[3] = {pv[1], pv[2], pv[3]};
@@ -352,11 +386,15 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     }
   }
   __syncthreads();
+  // one reciprocal of det per point: each use differs from a division by det
+  // by at most an ulp
+  for (int t = threadIdx.x; t < nc * S; t += blockDim.x) sRd[t] = 1.0 / sRd[t];
+  __syncthreads();
   // divergence sum_{j,m} D[s,j,m] Ft[j,m] as one FP64 tensor-core product
   // (K = (j, m), columns (cell, field)); then the face corrections of every
   // face side in ascending color order
   {
-    dmma_product_f(
+    dmma_product_rb<(4 * CPB + 7) / 8>(
         S, 4 * nc, 3 * S, ops.fD3[ct],
         [&](int k, int col) { return Ft[((col >> 2) * S * 3 + k) * 4 + (col & 3)]; },
         [&](int s, int col, double x) {
@@ -364,40 +402,34 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
           R[(b * S + s) * 4 + (col & 3)] = -x * sRd[b * S + s];
         });
   }
-  // one thread per point, all four fields; the slots are fetched four at a time
-  // (independent loads) and summed in slot order
+  // one thread per point, all four fields, slots in order
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
     const int s = p % S;
     const int e = e0 + p / S;
     const double rdj = sRd[p];
     double C[4] = {0.0, 0.0, 0.0, 0.0};
     const int sb = fc.tslot_ptr[e], se = fc.tslot_ptr[e + 1];
-    for (int s0 = sb; s0 < se; s0 += 4) {
-      int code[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) code[u] = s0 + u < se ? __ldg(fc.tslot + s0 + u) : -1;
-      double gw[4];
-      double2 c01[4], c23[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (code[u] < 0) continue;
-        const int ax = (code[u] >> 2) & 3;
-        gw[u] = ((code[u] & 1) ? ops.g_right : ops.g_left)[ops.dist_co[ax * S + s]];
-        const double2* cr =
-            reinterpret_cast<const double2*>(a.cfp + ((size_t)(code[u] >> 4) * NP + ops.dist_fp[ax * S + s]) * 4);
-        c01[u] = cr[0];
-        c23[u] = cr[1];
+    for (int k = sb; k < se; ++k) {
+      const int code = staged ? sCode[k - k_beg] : __ldg(fc.tslot + k);
+      const int ax = (code >> 2) & 3;
+      const double gw = sG[((code & 1) ? 4 : 0) + sDco[ax * S + s]];
+      const int fp = sDfp[ax * S + s];
+      double2 c01, c23;
+      if (staged) {
+        const double2* cr = reinterpret_cast<const double2*>(sC + ((k - k_beg) * NP + fp) * 4);
+        c01 = cr[0];
+        c23 = cr[1];
+      } else {
+        const double2* cr = reinterpret_cast<const double2*>(a.cfp + ((size_t)(code >> 4) * NP + fp) * 4);
+        c01 = __ldg(cr);
+        c23 = __ldg(cr + 1);
       }
+      const double cv[4] = {c01.x, c01.y, c23.x, c23.y};
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (code[u] < 0) continue;
-        const double cv[4] = {c01[u].x, c01[u].y, c23[u].x, c23[u].y};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const double contrib = gw[u] * cv[q];
-          if (code[u] & 2) C[q] += contrib * rdj;
-          else C[q] -= contrib * rdj;
-        }
+      for (int q = 0; q < 4; ++q) {
+        const double contrib = gw * cv[q];
+        if (code & 2) C[q] += contrib * rdj;
+        else C[q] -= contrib * rdj;
       }
     }
 #pragma unroll
