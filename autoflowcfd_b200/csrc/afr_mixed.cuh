@@ -252,7 +252,9 @@ struct MxPreSmem {
   // (P1, P2; at P3 the tile's loads are direct: no room)
   static constexpr bool STG = S <= 27;
   static constexpr int oStg = oM + MX_PRE_CELLS * 9 * 8;
-  static constexpr int total = oStg + (STG ? MX_PRE_CELLS * S * 9 * 8 : 0);
+  // and the next tile's FP32 inverse-Jacobian rows (float4 x 3 per point), 16-byte aligned
+  static constexpr int oInv = (oStg + (STG ? MX_PRE_CELLS * S * 9 * 8 : 0) + 15) / 16 * 16;
+  static constexpr int total = oInv + (STG ? MX_PRE_CELLS * S * 48 : 0);
   static constexpr int NCOL = pow2_cols(cmax(NB1, NB2MAX));
 };
 
@@ -303,6 +305,7 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
   // asynchronous copies of a tile's contiguous state and nu_t blocks into the
   // staging buffer; issued one tile ahead, so they overlap the tile before
   double* sStg = reinterpret_cast<double*>(smem + L::oStg);
+  float4* sInvs = reinterpret_cast<float4*>(smem + L::oInv);
   auto stage = [&](int tl) {
     if constexpr (L::STG) {
       const size_t eb = (size_t)cell_base + (size_t)tl * C;
@@ -314,7 +317,23 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
       cp_async_commit();
     }
   };
-  if (blockIdx.x < ntiles) stage(blockIdx.x);
+  // the tile's inverse-Jacobian rows: read by the gradient phase, so the next
+  // tile's copies are issued only once that phase of the current tile is over
+  auto stage_inv = [&](int tl) {
+    if constexpr (L::STG) {
+      if (visc) {
+        const size_t eb = (size_t)cell_base + (size_t)tl * C;
+        const int nn = min(C, cell_end - (int)eb);
+        const float4* ib = mo.invs + eb * S * 3;
+        for (int t = tid; t < nn * S * 3; t += MX_THREADS) cp_async16(sInvs + t, ib + t);
+        cp_async_commit();
+      }
+    }
+  };
+  if (blockIdx.x < ntiles) {
+    stage(blockIdx.x);
+    stage_inv(blockIdx.x);
+  }
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = cell_base + tile * C;
@@ -324,7 +343,7 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
       const size_t en = (size_t)cell_base + (size_t)(tile + gridDim.x) * C;
       const size_t nn = min((size_t)C, (size_t)cell_end - en), NS = (size_t)g.N * S;
       if (!L::STG) mxd::prefetch_l2(U, NS * nv * 8, en * S * nv * 8, nn * S * nv * 8);
-      if (visc) mxd::prefetch_l2(mo.invs, NS * 48, en * S * 48, nn * S * 48);
+      if (visc && !L::STG) mxd::prefetch_l2(mo.invs, NS * 48, en * S * 48, nn * S * 48);
       if (nut && !L::STG) mxd::prefetch_l2(nut, NS * 8, en * S * 8, nn * S * 8);
     }
     if constexpr (L::STG) {
@@ -406,11 +425,11 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
         const int c = t % C, s = t / C;
         float gr[12];
         if (c < nc) {
-          const float4* inv = mo.invs + ((size_t)(e0 + c) * S + s) * 3;
+          const float4* inv = L::STG ? sInvs + (c * S + s) * 3 : mo.invs + ((size_t)(e0 + c) * S + s) * 3;
           float iv[9];
 #pragma unroll
           for (int m = 0; m < 3; ++m) {
-            const float4 x = __ldg(inv + m);
+            const float4 x = L::STG ? inv[m] : __ldg(inv + m);
             iv[m * 3 + 0] = x.x;
             iv[m * 3 + 1] = x.y;
             iv[m * 3 + 2] = x.z;
@@ -434,6 +453,7 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
       }
       tc::fence_async_smem();
       __syncthreads();
+      if (tile + (int)gridDim.x < ntiles) stage_inv(tile + (int)gridDim.x);  // the rows are consumed
     }
     // extrapolation of every field to all face points: D[fp][f*8+c]
     if (tid == 0) {

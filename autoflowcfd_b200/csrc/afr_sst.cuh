@@ -280,12 +280,6 @@ __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops op
 template <int S>
 __host__ __device__ constexpr int sst_stage_slots() { return S <= 27 ? SstTile<S>::CPB * 6 : 1; }
 
-// 16-byte asynchronous copy global -> shared (both 16-byte aligned)
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
 template <int S, int NP>
 __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a, int cell_base,
                                                     int cell_end) {

@@ -100,6 +100,14 @@ def initial_state(case, spec):
     return U, k, om, nut, mu
 
 
+# algorithmic bytes per cell and RK stage of the C2 step in the reference's FP64
+# layout: 3*8*7*27 (U_stage, U0, U_next) + 8*10*27 (det, adjugate) + 8*9*64
+# (fine-point adjugates) + 8*3*9*R (face normals) + 8*9*27*M (interpolation
+# matrices used) + 56*R (face metadata) + 8*27 (mu_t) + 8*6*27/3 (SST fields per
+# step), with R = 4.04 face records and M = 7.9 used matrices per cell
+C2_BYTES_PER_CELL_STAGE = 3 * 8 * 7 * 27 + 8 * 10 * 27 + 8 * 9 * 64 + 8 * 3 * 9 * 4.04 + 8 * 9 * 27 * 7.9 + 56 * 4.04 \
+    + 8 * 27 + 8 * 6 * 27 / 3
+
 # DRAM bytes per cell and launch of the mixed stage kernels, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 76,800-prism P2 SST
 # case; a full-size launch moves these times the number of cells.
@@ -1133,6 +1141,15 @@ def main():
                      "traffic_source": "ncu DRAM bytes per cell on 76,800 prisms, scaled to this launch",
                      "kernel": dom, "algorithmic_bytes_per_launch": alg[dom], "per_kernel": per_kernel,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        # whole step against HBM: the reference-layout algorithmic bytes per
+        # cell and RK stage of the C2 configuration (every distinct array once
+        # per stage in FP64: state in/out, metrics, fine-point adjugates,
+        # face normals, the used interpolation matrices, face metadata, mu_t,
+        # SST fields amortised over the stages)
+        "step_roofline": {"bytes_per_cell_stage": C2_BYTES_PER_CELL_STAGE,
+                          "achieved": C2_BYTES_PER_CELL_STAGE * N * 3 / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                          "unit": "GB/s",
+                          "frac": C2_BYTES_PER_CELL_STAGE * N * 3 / (ms * 1e-3) / 1e9 / hbm_peak},
         "gpu_launches": bd.get("launches_per_step", 0) * args.steps,
         "breakdown_ms_per_step": bd.get("per_kernel_ms"),
         "device_bytes": head["device_bytes"],
