@@ -84,3 +84,20 @@ def test_request_too_large_for_the_device_is_rejected():
     lp.bytes_per_cell = {1: 1e12, 2: 1e12}
     res = lp.run(requests()[:1], tables=tables())
     assert res[0].status == "rejected" and res[0].iterations == 0
+
+
+def test_residual_drop_stop():
+    """The stopping rule: a request finishes as "converged" at the first slice
+    boundary where its density residual has dropped to ``drop`` times its
+    first step's (the 4x2x2-hex P1 request reaches half at iteration 101 =
+    1 + 2 slices of 50), and as "max_iter" when the cap comes first."""
+    req = requests()[1]
+    lp = SV.ServingLoop(precision="mixed", max_active=1, steps_per_slice=50, drop=0.5, max_iter=500)
+    got = lp.run([req], tables=tables())[0]
+    assert got.status == "converged"
+    assert got.iterations == 101 and got.residual_drop <= 0.5
+    slow = requests()[0]  # its residual stays above 0.9 of the first for thousands of steps
+    lp = SV.ServingLoop(precision="mixed", max_active=1, steps_per_slice=50, drop=0.5, max_iter=200)
+    got = lp.run([slow], tables=tables())[0]
+    assert got.status == "max_iter" and got.iterations >= 200 and got.residual_drop > 0.5
+
