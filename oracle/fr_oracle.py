@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY.  This is a numpy restatement of the reference
 (AutoFlowCFD) algorithm, used by ``tests/``, ``__graft_entry__.smoke()`` and
-the ``cpu_baseline`` leg of ``bench.py`` as the checker.  The product path
+the ``cpu_baseline`` leg of ``bench.py`` to check results.  The product path
 (``autoflowcfd_b200``) never imports it.
 
 It is pinned against the golden fixtures in ``tests/golden`` that the

@@ -58,7 +58,7 @@ def test_oracle_continuation_matches_reference(golden, name):
 
 class Scripted:
     """A solver whose residuals follow a script per phase; records the
-    order changes the driver asks for."""
+    order changes the continuation asks for."""
 
     def __init__(self, order, script, start_sps=None):
         self.order = order

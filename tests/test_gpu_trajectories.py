@@ -84,7 +84,7 @@ def test_c1_mixed_form_against_reference_after_100_steps(c1):
     assert np.all(np.isfinite(a))
     errs = per_field(a, g["U_s100"])
     report("c1 mixed step 100 vs reference", errs)
-    assert worst(errs, 0) < 1e-6  # field L2 (north_star target)
+    assert worst(errs, 0) < 1e-6  # the field relative L2 target of the mixed form
     assert worst(errs, 1) < 1e-5
     s.cleanup()
 

@@ -2,7 +2,7 @@
 
 The fixtures were produced by running the reference implementation
 (tests/golden/make_golden.py); the oracle must reproduce them before it may be
-used as the checker for the CUDA path."""
+used to check the CUDA path."""
 import copy
 
 import numpy as np
