@@ -139,7 +139,9 @@ __device__ __forceinline__ void dmma_product_f(int M, int N, int K, const double
 // dmma_product_f with each warp computing all column tiles of a row tile
 // (at most NT of them): the A fragment is loaded once per k-step and the NT
 // accumulations are independent, so their tensor-core latencies overlap.  Per
-// element the k-steps accumulate in the same order as dmma_product_f.
+// element the k-steps accumulate in the same order as dmma_product_f.  Pays
+// when the row tiles keep every warp busy (measured: slower than
+// dmma_product_f for the 27-row filter and SST divergence with 4 row tiles).
 template <int NT, class FB, class FC>
 __device__ __forceinline__ void dmma_product_rb(int M, int N, int K, const double* __restrict__ Af, FB b, FC c) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;

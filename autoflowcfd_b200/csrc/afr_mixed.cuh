@@ -1261,7 +1261,7 @@ __global__ void __launch_bounds__(MxUpdSmem<S, NP, CPB>::THREADS, 5)
   // outputs are assembled in the residual buffers (no longer needed) and
   // stored as one contiguous block
   double* sOut = sRi;  // (nc*S, nv) row-major, fits in sRi + sRv
-  dmma_product_rb<(5 * CPB + 7) / 8>(
+  dmma_product_f(
       S, 5 * nc, S, ops.ffilt[ct],
       [&](int j, int col) { return sU[((col / 5) * S + j) * nv + col % 5]; },
       [&](int s, int col, double x) { sOut[((col / 5) * S + s) * nv + col % 5] = x; });

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   // (K = (j, m), columns (cell, field)); then the face corrections of every
   // face side in ascending color order
   {
-    dmma_product_rb<(4 * CPB + 7) / 8>(
+    dmma_product_f(
         S, 4 * nc, 3 * S, ops.fD3[ct],
         [&](int k, int col) { return Ft[((col >> 2) * S * 3 + k) * 4 + (col & 3)]; },
         [&](int s, int col, double x) {
