@@ -275,24 +275,22 @@ __global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops op
 
 // per cell: volume transport terms, gather of the face corrections, outlier
 // suppression and the point-implicit k / omega update.  CPB cells per CTA.
-// transport slots of a tile whose corrections are staged in shared memory
-// (6 per cell at P1 / P2; at P3 there is no room and they are read from global)
-template <int S>
-__host__ __device__ constexpr int sst_stage_slots() { return S <= 27 ? SstTile<S>::CPB * 6 : 1; }
+// transport slots per cell whose slot codes are staged in shared memory; the
+// slots' face corrections are staged in the contravariant-flux buffer once the
+// divergence has consumed it (when they fit; otherwise read from global)
+constexpr int SST_STAGE_SLOTS = 12;
 
 template <int S, int NP>
 __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, SstArgs a, int cell_base,
                                                     int cell_end) {
   constexpr int CPB = SstTile<S>::CPB;
-  // the face corrections of the tile's transport slots (slot j's face rows at
-  // sC + j*NP*4), copied at the start so they arrive during the volume terms
-  constexpr int NSTG = sst_stage_slots<S>();
-  __shared__ __align__(16) double sC[NSTG * NP * 4];
   // point values packed by k_sst_point, row stride 9: rho (clamped as the
   // reference's), u, v, w, k, omega, gamma_k, gamma_w
   __shared__ double sP[CPB * S * 9];
   __shared__ double gc[CPB * S * 3 * 2];  // reference-space grads of k, w
-  __shared__ double Ft[CPB * S * 3 * 4];  // contravariant fluxes: conv k, diff k, conv w, diff w
+  // contravariant fluxes (conv k, diff k, conv w, diff w); then the face
+  // corrections of the tile's transport slots (slot j's face rows at Ft + j*NP*4)
+  __shared__ __align__(16) double Ft[CPB * S * 3 * 4];
   // inverse Jacobians (rows of 9) until the fluxes are formed; then R (volume
   // residuals, then with the interface corrections), T (transport k, w +
   // padding for the outlier helper) and Ref
@@ -300,7 +298,7 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   __shared__ double sRd[CPB * S];         // det, then 1 / det
   __shared__ double work[CPB * OUT_WORK];
   __shared__ double sG[8];                // g_left, g_right
-  __shared__ int sCode[NSTG];
+  __shared__ int sCode[CPB * SST_STAGE_SLOTS];
   __shared__ int sDfp[3 * S], sDco[3 * S];
   double* sInv = X;
   double* R = X;
@@ -311,7 +309,8 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
   const int ct = cell_type(g, e0);
   // the tile's transport slots are contiguous (cell-major)
   const int k_beg = fc.tslot_ptr[e0], k_end = fc.tslot_ptr[e0 + nc];
-  const bool staged = S <= 27 && k_end - k_beg <= NSTG;
+  const bool staged = (k_end - k_beg) * NP * 4 <= CPB * S * 12 && k_end - k_beg <= CPB * SST_STAGE_SLOTS;
+  double* sC = Ft;
   // the tile's blocks are contiguous: asynchronous copies, all in flight at once
   {
     const double* pb = a.sp8 + (size_t)e0 * S * 8;
@@ -319,12 +318,6 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
     const double* ib = g.inv + (size_t)e0 * S * 9;
     for (int t = threadIdx.x; t < nc * S * 9; t += blockDim.x) cp_async8(sInv + t, ib + t);
     for (int t = threadIdx.x; t < nc * S; t += blockDim.x) cp_async8(sRd + t, g.det + (size_t)e0 * S + t);
-    if (staged)
-      for (int t = threadIdx.x; t < (k_end - k_beg) * NP * 2; t += blockDim.x) {
-        const int j = t / (NP * 2), q = t - j * (NP * 2);
-        const int face = __ldg(fc.tslot + k_beg + j) >> 4;
-        cp_async16(sC + j * NP * 4 + 2 * q, a.cfp + (size_t)face * NP * 4 + 2 * q);
-      }
     if (staged)
       for (int t = threadIdx.x; t < k_end - k_beg; t += blockDim.x) sCode[t] = __ldg(fc.tslot + k_beg + t);
     for (int t = threadIdx.x; t < 3 * S; t += blockDim.x) {
@@ -396,6 +389,17 @@ __global__ void __launch_bounds__(128) k_sst_update(Geom g, Ops ops, Faces fc, S
           R[(b * S + s) * 4 + (col & 3)] = -x * sRd[b * S + s];
         });
   }
+  // the fluxes are consumed: the slots' face corrections arrive in their space
+  __syncthreads();
+  if (staged) {
+    for (int t = threadIdx.x; t < (k_end - k_beg) * NP * 2; t += blockDim.x) {
+      const int j = t / (NP * 2), q = t - j * (NP * 2);
+      const int face = sCode[j] >> 4;
+      cp_async16(sC + j * NP * 4 + 2 * q, a.cfp + (size_t)face * NP * 4 + 2 * q);
+    }
+    cp_async_wait_all();
+  }
+  __syncthreads();
   // one thread per point, all four fields, slots in order
   for (int p = threadIdx.x; p < nc * S; p += blockDim.x) {
     const int s = p % S;
