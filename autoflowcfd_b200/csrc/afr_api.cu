@@ -1200,12 +1200,9 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     h->ops.filt[t] = flt;
   }
   {
-    double *ex, *exT, *gl, *gr;
+    double *ex, *gl, *gr;
     int32_t *dfp, *dco;
     if ((rc = upload(h, &ex, m->boundary_extrap, 12 * P * S, st))) return bail(rc);
-    const std::vector<double> exT_h = transpose_mats(m->boundary_extrap, 12, P, S);
-    if ((rc = upload(h, &exT, exT_h.data(), exT_h.size(), st))) return bail(rc);
-    cudaStreamSynchronize(st);  // exT_h leaves scope
     if ((rc = upload(h, &gl, m->g_left, (size_t)n1d, st))) return bail(rc);
     if ((rc = upload(h, &gr, m->g_right, (size_t)n1d, st))) return bail(rc);
     if ((rc = upload_i32(h, &dfp, m->dist_fp_of_sp, 3 * S, st, tmp))) return bail(rc);
@@ -1217,7 +1214,6 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     cudaStreamSynchronize(st);  // fex leaves scope
     h->ops.fextrap = fexd;
     h->ops.extrap = ex;
-    h->ops.extrapT = exT;
     h->ops.g_left = gl;
     h->ops.g_right = gr;
     h->ops.dist_fp = dfp;

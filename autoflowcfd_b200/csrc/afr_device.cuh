@@ -41,7 +41,6 @@ struct Ops {
   const double* W[2];       // (S, 3Fn) = f2c * D_fine, folded once at create
   const double* filt[2];    // (S, S)
   const double* extrap;     // (2, 3, 2, P, S)
-  const double* extrapT;    // (2, 3, 2, S, P): the same, face point fastest (lanes of a face read one line)
   const double* g_left;     // (n1d)
   const double* g_right;    // (n1d)
   const int32_t* dist_fp;   // (3, S)

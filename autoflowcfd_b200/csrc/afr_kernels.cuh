@@ -42,20 +42,6 @@ __device__ __forceinline__ int cell_type(const Geom& g, int e) { return e < g.n_
 // Odd, so that threads reading consecutive points' rows hit different banks.
 constexpr int US = 9;
 
-// out[r][c] (+)= sum_k A[r*lda + k] * B[k*ldb + c] for r<R, c<C; A global, B/out shared.
-template <int R, int C, int K>
-__device__ __forceinline__ void block_gemm(double* out, int ldo, const double* __restrict__ A, int lda,
-                                           const double* B, int ldb) {
-  for (int t = threadIdx.x; t < R * C; t += blockDim.x) {
-    const int r = t / C, c = t % C;
-    const double* a = A + (size_t)r * lda;
-    double acc = 0.0;
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) acc += __ldg(a + k) * B[k * ldb + c];
-    out[r * ldo + c] = acc;
-  }
-}
-
 // asynchronous 8-byte copy global -> shared (both 8-byte aligned); completed
 // by cp_async_wait_all before the block barrier that publishes the data
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -69,17 +55,10 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// Small FP64 products C (M x N) = A (M x K) * B (K x N) on the FP64 tensor
-// path: mma.sync m8n8k4 .f64, one 8 x 8 output tile per warp at a time,
-// K in steps of 4 (padding rows / columns read as zero).  a(m, k), b(k, n)
-// fetch operands and c(m, n, value) stores results; block-wide work split by
-// warp, no barrier inside.  The sum order over k is the unit's, so results
-// can differ from a sequential FP64 sum in the last bits.
 // one m8n8k4 FP64 step: lane (g = lane/4, t = lane%4) supplies A[g][t] and
 // B[t][g] and holds D[g][2t], D[g][2t+1]
 __device__ __forceinline__ void dmma884(double& d0, double& d1, double a0, double b0) {
@@ -88,31 +67,15 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a0, doubl
                : "d"(a0), "d"(b0));
 }
 
-template <class FA, class FB, class FC>
-__device__ __forceinline__ void dmma_product(int M, int N, int K, FA a, FB b, FC c) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int nw = blockDim.x >> 5;
-  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
-  for (int tile = threadIdx.x >> 5; tile < mt * nt; tile += nw) {
-    const int m = (tile / nt) * 8 + g, n0 = (tile % nt) * 8;
-    double c0 = 0.0, c1 = 0.0;
-    for (int k0 = 0; k0 < K; k0 += 4) {
-      const int k = k0 + t;
-      const double a0 = (m < M && k < K) ? a(m, k) : 0.0;
-      const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
-      dmma884(c0, c1, a0, b0);
-    }
-    const int n = n0 + 2 * t;
-    if (m < M) {
-      if (n < N) c(m, n, c0);
-      if (n + 1 < N) c(m, n + 1, c1);
-    }
-  }
-}
 
-// dmma_product with A read from a fragment-major image (layout in Ops): one
-// contiguous 256-byte load per warp and k-step; the image's zeros stand for
-// the rows and columns outside the operator
+// Small FP64 products C (M x N) = A (M x K) * B (K x N) on the FP64 tensor
+// path: mma.sync m8n8k4 .f64, one 8 x 8 output tile per warp at a time, K in
+// steps of 4.  A is read from a fragment-major image (layout in Ops): one
+// contiguous 256-byte load per warp and k-step, the image's zeros standing for
+// the rows and columns outside the operator; b(k, n) fetches B (padding reads
+// as zero) and c(m, n, value) stores results; block-wide work split by warp,
+// no barrier inside.  The sum order over k is the unit's, so results can
+// differ from a sequential FP64 sum in the last bits.
 template <class FB, class FC>
 __device__ __forceinline__ void dmma_product_f(int M, int N, int K, const double* __restrict__ Af, FB b, FC c) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -378,45 +341,14 @@ struct SlotTable {
   const int32_t* i1;        // (n) row of the compact second-source table
 };
 
-__device__ __forceinline__ void ld18(const double* __restrict__ p, double x[18]) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-  for (int j = 0; j < 9; ++j) {
-    const double2 v = __ldg(q + j);
-    x[2 * j] = v.x;
-    x[2 * j + 1] = v.y;
-  }
-}
 
-// one warp's m8n8k4 FP64 product C (M x N) = A (M x K) * B (K x N), all
-// tiles by this warp (see dmma_product for the fragment layout)
-template <class FA, class FB, class FC>
-__device__ __forceinline__ void dmma_warp(int M, int N, int K, FA a, FB b, FC c) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
-  for (int tile = 0; tile < mt * nt; ++tile) {
-    const int m = (tile / nt) * 8 + g, n0 = (tile % nt) * 8;
-    double c0 = 0.0, c1 = 0.0;
-    for (int k0 = 0; k0 < K; k0 += 4) {
-      const int k = k0 + t;
-      const double a0 = (m < M && k < K) ? a(m, k) : 0.0;
-      const double b0 = (k < K && n0 + g < N) ? b(k, n0 + g) : 0.0;
-      dmma884(c0, c1, a0, b0);
-    }
-    const int n = n0 + 2 * t;
-    if (m < M) {
-      if (n < N) c(m, n, c0);
-      if (n + 1 < N) c(m, n + 1, c1);
-    }
-  }
-}
 
-// one warp's product C (M x N) = A (M x K) * B (K x N) with every tile's
-// accumulators held in registers (MT row tiles, NT column tiles): each k-step
-// loads the A fragments of all row tiles and the B fragments of all column
-// tiles, so the operand loads of the whole product are independent of one
-// another and of the products.  Per element the k-steps accumulate in the
-// same order as dmma_warp.
+// one warp's m8n8k4 FP64 product C (M x N) = A (M x K) * B (K x N) with
+// every tile's accumulators held in registers (MT row tiles, NT column
+// tiles): each k-step loads the A fragments of all row tiles and the B
+// fragments of all column tiles, so the operand loads of the whole product
+// are independent of one another and of the products.  a(m, k), b(k, n)
+// fetch operands (padding reads as zero), c(m, n, value) stores results.
 template <int MT, int NT, int K, class FA, class FB, class FC>
 __device__ __forceinline__ void dmma_warp_rb(int M, int N, FA a, FB b, FC c) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
