@@ -111,7 +111,7 @@ C2_BYTES_PER_CELL_STAGE = 3 * 8 * 7 * 27 + 8 * 10 * 27 + 8 * 9 * 64 + 8 * 3 * 9 
 # DRAM bytes per cell and launch of the mixed stage kernels, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 76,800-prism P2 SST
 # case; a full-size launch moves these times the number of cells.
-MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 8383.0, "k_mx_face": 7075.0, "k_mx_vol": 9912.0, "k_mx_update": 6126.0}
+MEASURED_TRAFFIC_PER_CELL = {"k_mx_pre": 8353.0, "k_mx_face": 7101.0, "k_mx_vol": 9921.0, "k_mx_update": 6126.0}
 
 
 def mixed_algorithmic_bytes(case, nv=7):
