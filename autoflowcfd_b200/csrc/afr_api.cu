@@ -300,6 +300,30 @@ static cudaError_t resident_ctas(const void* fn, int threads, size_t dyn_smem, i
   return cudaSuccess;
 }
 
+// SST source, transport and point-implicit update of one step (the three
+// per-step kernels); cells of each type in their own launches
+template <int S, int NP>
+cudaError_t sst_launch(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm) {
+  constexpr int CPB = SstTile<S>::CPB, TH = SstTile<S>::THREADS;
+  const int ranges[3] = {0, h->n_prism, h->N};
+  for (int r = 0; r < 2; ++r) {
+    const int n = ranges[r + 1] - ranges[r];
+    if (n > 0) k_sst_point<S><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, a, ranges[r], ranges[r + 1]);
+  }
+  if (tm) tm->mark(st);
+  if (h->F > 0)
+    k_sst_face<S, NP><<<(h->F + SST_FACE_WARPS - 1) / SST_FACE_WARPS, 32 * SST_FACE_WARPS, 0, st>>>(h->g, h->ops,
+                                                                                                    h->fc, a);
+  if (tm) tm->mark(st);
+  for (int r = 0; r < 2; ++r) {
+    const int n = ranges[r + 1] - ranges[r];
+    if (n > 0)
+      k_sst_update<S, NP><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, h->fc, a, ranges[r], ranges[r + 1]);
+  }
+  if (tm) tm->mark(st);
+  return cudaGetLastError();
+}
+
 template <int S, int FN, int NP, int N1D>
 struct Launch {
   static constexpr int CPB = S <= 8 ? 8 : (S <= 27 ? 2 : 1);
@@ -458,23 +482,7 @@ struct Launch {
     return r;
   }
   static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
-    constexpr int CPB = SstTile<S>::CPB, TH = SstTile<S>::THREADS;
-    const int ranges[3] = {0, h->n_prism, h->N};
-    for (int r = 0; r < 2; ++r) {
-      const int n = ranges[r + 1] - ranges[r];
-      if (n > 0) k_sst_point<S><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, a, ranges[r], ranges[r + 1]);
-    }
-    if (tm) tm->mark(st);
-    k_sst_face<S, NP><<<(h->F + SST_FACE_WARPS - 1) / SST_FACE_WARPS, 32 * SST_FACE_WARPS, 0, st>>>(h->g, h->ops,
-                                                                                                    h->fc, a);
-    if (tm) tm->mark(st);
-    for (int r = 0; r < 2; ++r) {
-      const int n = ranges[r + 1] - ranges[r];
-      if (n > 0)
-        k_sst_update<S, NP><<<(n + CPB - 1) / CPB, TH, 0, st>>>(h->g, h->ops, h->fc, a, ranges[r], ranges[r + 1]);
-    }
-    if (tm) tm->mark(st);
-    return cudaGetLastError();
+    return sst_launch<S, NP>(h, a, st, tm);
   }
   static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
     if (h->n_cd_faces == 0) return cudaSuccess;
@@ -513,8 +521,10 @@ struct LaunchP0 {
     if (nl) *nl += 2;
     return cudaGetLastError();
   }
-  static cudaError_t sst(afr_handle*, const SstArgs&, cudaStream_t, StepTimer* = nullptr) {
-    return cudaErrorNotSupported;  // refused at create
+  // SST at one point per cell: the generic kernels with S = P = 1 (the
+  // reference runs its FR transport and closure there, not a finite-volume form)
+  static cudaError_t sst(afr_handle* h, const SstArgs& a, cudaStream_t st, StepTimer* tm = nullptr) {
+    return sst_launch<1, 1>(h, a, st, tm);
   }
   static cudaError_t force(afr_handle* h, const double* U, const double* nut, cudaStream_t st) {
     if (h->n_cd_faces == 0) return cudaSuccess;
@@ -1033,8 +1043,6 @@ int afr_create(const afr_mesh_desc* m, const afr_params* prm, void* stream, afr_
     return bail(fail(h, AFR_EINVAL, "precision must be AFR_PREC_FP64 or AFR_PREC_MIXED"));
   if (h->order == 0 && prm->precision != AFR_PREC_FP64)
     return bail(fail(h, AFR_EUNSUPPORTED, "order 0 (finite volume) runs in the FP64 form only"));
-  if (h->order == 0 && prm->turb == AFR_TURB_SST)
-    return bail(fail(h, AFR_EUNSUPPORTED, "order 0 (finite volume) supports laminar and inviscid flow"));
   if (h->order == 0 && !m->true_area_weight)
     return bail(fail(h, AFR_EINVAL, "order 0 needs true_area_weight (the face areas)"));
   const int fine_1d = std::min(2 * h->order, 3) + 1;

@@ -129,6 +129,12 @@ class B200FRSolver:
         self._fv_volumes = np.asarray(case["fv_cell_volumes"] if case.get("fv_cell_volumes") is not None
                                       else case["cell_volumes"], float)
         self._mfs_cache = None
+        # SST: the wall distance at the target order's points; an order
+        # continuation restarts from its cell means and prolongs them between
+        # phases (core/utils/order_continuation.py:137-144, 270-275)
+        self._wd_target = (np.asarray(case["wall_distance"], float)
+                           if name == "SST" and case.get("wall_distance") is not None else None)
+        self._wd_phase = None
         self._open(case)
         self.initialize_uniform(rho_inf, vel_inf, 0.0, 0.0, p_inf)
         self.residual_history = []
@@ -181,12 +187,16 @@ class B200FRSolver:
             c = self._mfs_cache
             case["metric_flux_scale"] = np.ascontiguousarray(
                 np.broadcast_to(c, (self.n_cells, S)) if c.shape[1] in (1, S) else np.tile(c, (1, -(-S // c.shape[1])))[:, :S])
+        if self._wd_phase is not None:
+            case["wall_distance"] = np.ascontiguousarray(self._wd_phase)
         return case
 
     def _restart_at_p0(self):
         """run_order_continuation's restart (core/utils/order_continuation.py:236-288):
         the uniform free stream on a P0 handle (SST fields at their initial values)."""
         self._mfs_cache = None
+        if self._wd_target is not None:
+            self._wd_phase = np.tile(np.mean(self._wd_target, axis=1, keepdims=True), (1, 1))
         self._open(self._phase_case(0))
         f = self.freestream
         self.initialize_uniform(f["rho_inf"], f["vel_inf"], 0.0, 0.0, f["p_inf"])
@@ -197,6 +207,8 @@ class B200FRSolver:
         (interpolate_to_new_order_checked, core/utils/order_continuation.py:180-205)."""
         old = {"U": self.U, "k": self.k, "omega": self.omega, "nu_t": self.nu_t}
         s_old = self.n_sps
+        if self._wd_phase is not None:
+            self._wd_phase = np.einsum("ab,cb->ca", np.asarray(W, dtype=np.float64), self._wd_phase)
         self._open(self._phase_case(new_order))
         Wc = np.ascontiguousarray(W, dtype=np.float64)
         if Wc.shape != (self.n_sps, s_old):

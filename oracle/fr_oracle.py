@@ -1069,7 +1069,8 @@ def interp_matrix_3d(old_1d, new_1d):
     return W
 
 
-def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max_iter, dt, tol):
+def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max_iter, dt, tol, turb=None,
+                       wall_distance=None):
     """run_order_continuation, core/utils/order_continuation.py:207-425, on
     the oracle's solver: restart from the uniform free stream at P0
     (FRState.initialize_uniform, core/fr_solver/state.py:50-74), phases
@@ -1078,14 +1079,28 @@ def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max
     residual dropped 100x, the state prolonged between phases by
     np.einsum("ab,cbv->cav", W, U) (interpolate_to_new_order, :62-124).
 
+    With ``turb == "SST"`` (core/utils/order_continuation.py:120-144, 245-276):
+    the restart sets k = 1e-6, omega = 1, nu_t = 0 and the wall distance to
+    the cell means of ``wall_distance`` (the target order's field); k, omega,
+    nu_t and the wall distance are prolonged by np.einsum("ab,cb->ca", W, .)
+    between phases.
+
     Returns (step_order, step_residual, states, result): ``states`` maps
-    "U_start_p<p>" / "U_end_p<p>" to the phase's first and last states."""
+    "U_start_p<p>" / "U_end_p<p>" to the phase's first and last states (and
+    "k_end_p<p>", "w_end_p<p>", "nut_end_p<p>" with SST)."""
     rho, u, p = freestream
     c0 = case_for_order(0)
     N = int(c0["n_cells"])
     e = p / ((GAMMA - 1.0) * rho) + 0.5 * (u**2 + 0.0**2 + 0.0**2)
-    U = np.zeros((N, 1, 5))
+    sst = turb == "SST"
+    U = np.zeros((N, 1, 7 if sst else 5))
     U[:, :, 0], U[:, :, 1], U[:, :, 2], U[:, :, 3], U[:, :, 4] = rho, rho * u, rho * 0.0, rho * 0.0, rho * e
+    tk = tw = tn = wd = None
+    if sst:
+        # FRState.initialize_uniform's turbulence columns (k 1e-6, omega 1e-2)
+        U[:, :, 5], U[:, :, 6] = rho * 1e-6, rho * 1e-2
+        tk, tw, tn = np.full((N, 1), 1e-6), np.ones((N, 1)), np.zeros((N, 1))
+        wd = np.tile(np.mean(wall_distance, axis=1, keepdims=True), (1, 1))
     orders = list(range(0, order + 1))
     step_order, step_res, states = [], [], {}
     total, final = 0, 1e10
@@ -1098,13 +1113,16 @@ def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max
         if tp > 0:
             W = interp_matrix_3d(np.polynomial.legendre.leggauss(cur + 1)[0], np.polynomial.legendre.leggauss(tp + 1)[0])
             U = np.einsum("ab,cbv->cav", W, U)
+            if sst:
+                tk, tw, tn = (np.einsum("ab,cb->ca", W, x) for x in (tk, tw, tn))
+                wd = np.einsum("ab,cb->ca", W, wd)
             cur = tp
         mesh = Mesh.from_case(case_for_order(tp))
         if mfs_cache is None:
             mfs_cache = metric_flux_scale(mesh)
         mesh.extras["mfs"] = np.broadcast_to(mfs_cache, (mesh.N, mesh.S)) if mfs_cache.shape[1] in (1, mesh.S) \
             else np.tile(mfs_cache, (1, -(-mesh.S // mfs_cache.shape[1])))[:, :mesh.S]
-        s = Solver(mesh, U, mu, None, None, inviscid_only, 0.0)
+        s = Solver(mesh, U, mu, TurbState(tk, tw, tn) if sst else None, wd, inviscid_only, 0.0)
         states[f"U_start_p{tp}"] = s.U.copy()
         phase_max, phase_tol = max_iter // len(orders), tol * (10 ** (order - tp))
         init, converged = None, False
@@ -1123,6 +1141,9 @@ def order_continuation(case_for_order, order, mu, inviscid_only, freestream, max
                 break
         U = s.U
         states[f"U_end_p{tp}"] = U.copy()
+        if sst:
+            tk, tw, tn = s.turb.k, s.turb.w, s.turb.nut
+            states[f"k_end_p{tp}"], states[f"w_end_p{tp}"], states[f"nut_end_p{tp}"] = tk.copy(), tw.copy(), tn.copy()
         if tp == order and converged:
             return step_order, step_res, states, (True, total, final)
     return step_order, step_res, states, (False, total, final)

@@ -23,7 +23,7 @@ def golden_path(name):
 
 CASES = ["tet_p1_vortex", "prism_p2_sst", "prism_p1_ns", "tet_p3_tgv", "prism_p1_floors", "tet_p1_align"]
 # order 0: the finite-volume path of the reference (one point per cell)
-P0_CASES = ["prism_p0_ns", "tet_p0_vortex"]
+P0_CASES = ["prism_p0_ns", "prism_p0_sst", "tet_p0_vortex"]
 # steps of the dual-time (BDF1 then BDF2) and IMEX Euler schemes
 SCHEME_CASES = ["prism_p1_ns_dual_time", "prism_p1_ns_imex_euler", "prism_p2_sst_dual_time"]
 # cases with a wall force integral in their fixture

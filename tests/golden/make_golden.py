@@ -400,7 +400,8 @@ def make_case(name, box, order, turb, mu, free, plane_cfg, state_fn, inviscid_on
     return out
 
 
-def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1e-3, inviscid_only=False):
+def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1e-3, inviscid_only=False,
+                      turb="NONE"):
     """Run the reference's FRSolver.solve at ``order`` >= 2, which runs its
     order continuation (core/utils/order_continuation.py:207-425), and store
     every phase's tables (keys ``p<order>/<table>``, as that phase's mesh
@@ -416,7 +417,7 @@ def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1
                        else "FARFIELD") for n in boxmesh.PLANE_NAMES}
     mesh = ref_mesh(box, order, mesh_bc)
     rho_inf, u_inf, p_inf = free
-    solver = FRSolver(mesh=mesh, order=order, turb_model_name="NONE", rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf,
+    solver = FRSolver(mesh=mesh, order=order, turb_model_name=turb, rho_inf=rho_inf, vel_inf=u_inf, p_inf=p_inf,
                       mu_molecular=mu, n_threads=min(8, os.cpu_count() or 1))
     assert solver.order_continuation_enabled
     if not box.periodic:
@@ -424,10 +425,16 @@ def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1
     if inviscid_only:
         solver.compute_viscous_residual = lambda *a, **k: np.zeros_like(solver.state.U)
     out = dict(meta_name=np.array(name), order=np.int32(order), n_cells=np.int32(mesh.n_cells),
-               n_vars=np.int32(solver.state.n_vars), turb=np.array("NONE"), mu=np.float64(mu),
+               n_vars=np.int32(solver.state.n_vars), turb=np.array(turb), mu=np.float64(mu),
                freestream=np.array(free, float), inviscid_only=np.int32(inviscid_only),
                periodic=np.int32(box.periodic), global_dt_factor=np.float64(0.0),
                max_iter=np.int32(max_iter), tol=np.float64(tol), dt=np.float64(dt))
+    if turb == "SST":
+        # wall distance at the target order's points (the continuation's P0
+        # restart compresses it to cell means and each phase prolongs it)
+        nodes = np.asarray(mesh._node_coords, float)
+        solver.compute_wall_distance_field(nodes, np.flatnonzero(np.abs(nodes[:, 2]) < 1e-12))
+        out["wall_distance"] = solver.wall_distance.copy()
     real_step = solver.step
     log_order, log_res = [], []
 
@@ -438,12 +445,21 @@ def make_continuation(name, box, order, mu, free, plane_cfg, max_iter, tol, dt=1
                 if v is not None and not (isinstance(v, np.ndarray) and v.dtype == object):
                     out[f"p{p}/{k}"] = v
             out[f"U_start_p{p}"] = solver.state.U.copy()
+            if turb == "SST":
+                out[f"wall_distance_p{p}"] = np.asarray(solver.wall_distance, float).copy()
+                out[f"k_start_p{p}"] = solver.turb_model.k_field.copy()
+                out[f"w_start_p{p}"] = solver.turb_model.omega_field.copy()
+                out[f"nut_start_p{p}"] = np.asarray(solver.turb_model.nu_t, float).copy()
         r = real_step(dt_)
         if f"p{p}/mfs_cache" not in out:
             out[f"p{p}/mfs_cache"] = np.asarray(solver._metric_flux_scale_cache, float).copy()
         log_order.append(p)
         log_res.append(r)
         out[f"U_end_p{p}"] = solver.state.U.copy()
+        if turb == "SST":
+            out[f"k_end_p{p}"] = solver.turb_model.k_field.copy()
+            out[f"w_end_p{p}"] = solver.turb_model.omega_field.copy()
+            out[f"nut_end_p{p}"] = np.asarray(solver.turb_model.nu_t, float).copy()
         return r
 
     solver.step = step
@@ -796,6 +812,33 @@ def main(which=None):
         make_case("prism_p0_ns", box, 0, "NONE", mu, (rho, u, p), cfg,
                   lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 5), n_steps=3)
 
+    def c_prism_p0_sst():
+        """Order 0 with the SST closure: the finite-volume mean flow and the
+        reference's generic FR transport / source / point-implicit update at
+        one point per cell (core/fr_solver/turbulence.py, core/turbulence/)."""
+        Ls = (2.0, 1.0, 1.0)
+        box = boxmesh.prism_box(4, 3, 2, Ls, jitter=0.1, seed=5)
+        rho, p = 1.225, 101325.0
+        u = 0.1 * np.sqrt(GAMMA * p / rho)
+        mu = rho * u / 1e6
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        k_in = 1.5 * (0.01 * u) ** 2
+        w_in = rho * k_in / (10 * mu)
+
+        def turb_init(xyz):
+            rng = np.random.default_rng(3)
+            N, S = xyz.shape[:2]
+            pert = 1 + 0.2 * np.sin(2 * np.pi * xyz[..., 0] / Ls[0] + 0.3) * np.cos(np.pi * xyz[..., 2] / Ls[2])
+            k = k_in * pert
+            w = w_in * (1 + 0.3 * np.cos(2 * np.pi * xyz[..., 1] / Ls[1]))
+            nut = 10 * mu / rho * (1 + 0.5 * rng.uniform(size=(N, S)))
+            return k, w, nut
+
+        make_case("prism_p0_sst", box, 0, "SST", mu, (rho, u, p), cfg,
+                  lambda x, y, z: channel_state(x, y, z, Ls, rho, u, p, 5), turb_init=turb_init, n_steps=3)
+
     def c_tet_p0_vortex():
         L = 1.0
         box = boxmesh.tet_box(3, 3, 3, (L, L, L), jitter=0.0, periodic=True)
@@ -820,6 +863,21 @@ def main(which=None):
         cfg["y_min"] = {"type": "SYMMETRY"}
         cfg["y_max"] = {"type": "WALL", "is_no_slip": False}
         make_continuation("cont_prism_p2_ns", box, 2, rho * u / 1e5, (rho, u, p), cfg, max_iter=12, tol=1e-6)
+
+    def k_cont_prism_p2_sst():
+        """Order continuation P0 -> P1 -> P2 with the SST closure on a jittered
+        box with a no-slip wall at z = 0: the P0 restart of k, omega, nu_t and
+        the wall distance (cell means of the target order's field) and their
+        prolongation between phases."""
+        Ls = (1.5, 1.0, 1.0)
+        box = boxmesh.prism_box(3, 2, 2, Ls, jitter=0.1, seed=5)
+        rho, p = 1.225, 101325.0
+        u = 0.1 * np.sqrt(GAMMA * p / rho)
+        Qf = [rho, u, 0.0, 0.0, p]
+        cfg = {n: {"type": "FARFIELD", "Q_free": Qf} for n in boxmesh.PLANE_NAMES}
+        cfg["z_min"] = {"type": "WALL", "is_no_slip": True}
+        make_continuation("cont_prism_p2_sst", box, 2, rho * u / 1e6, (rho, u, p), cfg, max_iter=12, tol=1e-6,
+                          turb="SST")
 
     def k_cont_tet_p2():
         """Order continuation on a periodic box from the uniform free stream:
@@ -850,8 +908,9 @@ def main(which=None):
              "prism_p1_ns_dual_time": lambda: c_prism_p1_ns_scheme("dual_time", 2e-5),
              "prism_p1_ns_imex_euler": lambda: c_prism_p1_ns_scheme("imex_euler", 1e-3),
              "prism_p2_sst_dual_time": lambda: c_prism_p2_sst_scheme("dual_time", 2e-5),
-             "prism_p0_ns": c_prism_p0_ns, "tet_p0_vortex": c_tet_p0_vortex,
+             "prism_p0_ns": c_prism_p0_ns, "prism_p0_sst": c_prism_p0_sst, "tet_p0_vortex": c_tet_p0_vortex,
              "cont_prism_p2_ns": k_cont_prism_p2, "cont_tet_p2_uniform": k_cont_tet_p2,
+             "cont_prism_p2_sst": k_cont_prism_p2_sst,
              "fluxpoints": f_fluxpoints}
     for k, fn in cases.items():
         if which and k not in which:

@@ -8,7 +8,7 @@ residuals are the rounding noise of free-stream preservation."""
 import numpy as np
 import pytest
 
-from test_continuation import CONT_CASES, RES_ATOL
+from test_continuation import CONT_CASES, RES_ATOL, RES_RTOL
 
 pytestmark = pytest.mark.gpu
 
@@ -34,19 +34,28 @@ def test_device_continuation_matches_reference(golden, name):
     order = int(g["order"])
     case_at = phase_cases(g)
     free = g["freestream"]
-    s = B200FRSolver(case_at(order), mu_molecular=float(g["mu"]), rho_inf=free[0], vel_inf=free[1], p_inf=free[2],
-                     inviscid_only=bool(g["inviscid_only"]), case_for_order=case_at)
-    ends, orders = {}, []
+    sst = str(g["turb"]) == "SST"
+    target = dict(case_at(order))
+    if sst:
+        target["wall_distance"] = g["wall_distance"]  # the target order's field
+    s = B200FRSolver(target, turb_model_name=str(g["turb"]), mu_molecular=float(g["mu"]), rho_inf=free[0],
+                     vel_inf=free[1], p_inf=free[2], inviscid_only=bool(g["inviscid_only"]), case_for_order=case_at)
+    ends, turb_ends, orders = {}, {}, []
 
     def cb(sol, it):
         orders.append(sol.current_order)
         ends[sol.current_order] = sol.U.detach().cpu().numpy()
+        if sst:
+            turb_ends[sol.current_order] = [x.detach().cpu().numpy() for x in (sol.k, sol.omega, sol.nu_t)]
 
     r = s.solve(max_iter=int(g["max_iter"]), dt=float(g["dt"]), tol=float(g["tol"]), checkpoint_callback=cb)
     assert orders == list(g["step_order"])
-    assert np.allclose(r["residual_history"], g["step_residual"], rtol=1e-12, atol=RES_ATOL[name])
+    assert np.allclose(r["residual_history"], g["step_residual"], rtol=RES_RTOL[name], atol=RES_ATOL[name])
     for p, U in ends.items():
         assert rel(U, g[f"U_end_p{p}"]) < 1e-12, p
+    for p, (k, w, nut) in turb_ends.items():
+        assert rel(k, g[f"k_end_p{p}"]) < 1e-12 and rel(w, g[f"w_end_p{p}"]) < 1e-12, p
+        assert rel(nut, g[f"nut_end_p{p}"]) < 1e-12, p
     assert rel(s.U, g["U_final"]) < 1e-12
     assert r["converged"] == bool(g["result"][0]) and r["iterations"] == int(g["result"][1])
     assert s.current_order == order and s.n_sps == (order + 1) ** 3

@@ -44,8 +44,9 @@ def test_residuals_and_dt(golden, name):
     s.cleanup()
 
 
-def test_sst_update(golden):
-    case = golden("prism_p2_sst")
+@pytest.mark.parametrize("name", ["prism_p2_sst", "prism_p0_sst"])
+def test_sst_update(golden, name):
+    case = golden(name)
     s = make_solver(case)
     dt = s._compute_local_time_step()
     Sk, Sw, tk, tw = s.compute_turbulence_source(dt, diag=True)

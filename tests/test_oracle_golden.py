@@ -31,8 +31,9 @@ def test_residuals_match_reference(name):
         assert np.all(case["R_inv"][..., 5:] == 0) and np.all(case["R_visc"][..., 5:] == 0)
 
 
-def test_sst_source_transport_update_match_reference():
-    case, m, s = O.load_case(golden_path("prism_p2_sst"))
+@pytest.mark.parametrize("name", ["prism_p2_sst", "prism_p0_sst"])
+def test_sst_source_transport_update_match_reference(name):
+    case, m, s = O.load_case(golden_path(name))
     U = case["U0"]
     Q = O.state_primitives(U)
     dt = O.local_dt(m, Q, s.mu, s.mu_t(Q))
