@@ -80,8 +80,10 @@ typedef struct afr_handle afr_handle;
  * (core/fr_operators/face_kernels.py:124-187).  All host pointers.
  * order 0 is the reference's finite-volume path (one point per cell,
  * core/fr_residual/inviscid_p0.py:18-85): n_sps = n_fine = n_fp = 1, the FP64
- * form, laminar or inviscid; c2f, D_fine and f2c may be NULL there (the
- * reference has none) and true_area_weight is required (the face areas). */
+ * form, laminar, inviscid or SST (the SST closure and transport run the
+ * generic one-point kernels, as the reference runs its FR transport there);
+ * c2f, D_fine and f2c may be NULL there (the reference has none) and
+ * true_area_weight is required (the face areas). */
 typedef struct afr_mesh_desc {
   int32_t n_cells, n_prism, order, n_sps, n_fine, n_fp, n_faces;
   int32_t n_nb_src1, n_ow_src1; /* rows of the compact second-source tables */
