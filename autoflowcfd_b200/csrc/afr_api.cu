@@ -72,6 +72,12 @@ struct afr_handle {
   int mx_pre_occ = 0, mx_vol_occ = 0;          // occupancy-API CTAs per SM, before the tensor-memory cap
   // launch shapes chosen by afr_autotune (defaults until then)
   int mx_face_block = 128;  // threads per face-kernel CTA: 64, 128 or 256
+  // matched interior face points paired across the face's two slots, and the
+  // remaining slot points (boundary, interpolated, unpaired)
+  int2* mx_pairs = nullptr;
+  int32_t* mx_rest = nullptr;
+  int mx_npairs = 0, mx_nrest = 0;
+  bool mx_paired = false;
   int mx_upd_var = 1;       // update-kernel cells per CTA: 0 = half, 1 = base, 2 = double
   // dual-time / IMEX buffers, allocated by the first call of either scheme
   double* iRinv = nullptr;   // (N,S,nv) inviscid residual (dU/dt)
@@ -440,9 +446,20 @@ struct Launch {
   }
   static cudaError_t mx_stage(afr_handle* h, StageArgs a, cudaStream_t st, StepTimer* tm) {
     const int nt = h->slots.n * NP;
-    if (nt > 0)
-      k_mx_face<S, NP><<<(nt + h->mx_face_block - 1) / h->mx_face_block, h->mx_face_block, 0, st>>>(
-          h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell, (float)h->prm.mu, a.inviscid_only ? 0 : 1);
+    const int fb = h->mx_face_block;
+    if (h->mx_paired) {
+      if (h->mx_npairs > 0)
+        k_mx_face_pair<S, NP><<<(h->mx_npairs + fb - 1) / fb, fb, 0, st>>>(
+            h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell, (float)h->prm.mu, a.inviscid_only ? 0 : 1,
+            h->mx_pairs, h->mx_npairs);
+      if (h->mx_nrest > 0)
+        k_mx_face<S, NP><<<(h->mx_nrest + fb - 1) / fb, fb, 0, st>>>(
+            h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell, (float)h->prm.mu, a.inviscid_only ? 0 : 1,
+            h->mx_rest, h->mx_nrest);
+    } else if (nt > 0) {
+      k_mx_face<S, NP><<<(nt + fb - 1) / fb, fb, 0, st>>>(h->fc, h->bc, h->slots, h->mf, h->mb, h->mo.hcell,
+                                                           (float)h->prm.mu, a.inviscid_only ? 0 : 1, nullptr, 0);
+    }
     if (tm) tm->mark(st);
     const int ranges[3] = {0, h->n_prism, h->N};
     for (int r = 0; r < 2; ++r) {
@@ -939,6 +956,56 @@ static int mixed_setup(afr_handle* h, const afr_mesh_desc* m, const std::vector<
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form set-up");
   cudaMemsetAsync(h->status, 0, sizeof(unsigned), st);
+  // pair the matched slot points of interior faces across the face's two
+  // slots: owner point (slot s, i) matched to the neighbour's face point j,
+  // whose own match points back at (s's face, i)
+  if (ns > 0) {
+    const size_t nt = ns * P;
+    std::vector<uint8_t> hofp(nt);
+    std::vector<int32_t> hface(ns), hflag(ns);
+    e = cudaMemcpy(hofp.data(), ofp, nt, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hface.data(), h->slots.face, ns * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hflag.data(), h->slots.flags, ns * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form face pairs");
+    std::vector<int32_t> nb_slot(h->F, -1);
+    for (size_t sl = 0; sl < ns; ++sl)
+      if (hflag[sl] & 1) nb_slot[hface[sl]] = (int32_t)sl;
+    std::vector<int2> pairs;
+    std::vector<uint8_t> taken(nt, 0);
+    for (size_t sl = 0; sl < ns; ++sl) {
+      const int fl = hflag[sl];
+      if ((fl & 1) || (fl & 2)) continue;  // owner sides of interior faces
+      const int s2 = nb_slot[hface[sl]];
+      if (s2 < 0) continue;
+      const int code = ((fl >> 2) & 3) * 2 + ((fl & 16) ? 1 : 0);
+      const int fl2 = hflag[s2];
+      const int code2 = ((fl2 >> 2) & 3) * 2 + ((fl2 & 16) ? 1 : 0);
+      for (int i = 0; i < P; ++i) {
+        const size_t t = sl * P + i;
+        const int o = hofp[t];
+        if (o == MX_OFP_GENERAL || o / P != code2) continue;
+        const size_t t2 = (size_t)s2 * P + o % P;
+        if (hofp[t2] != code * P + i || taken[t2]) continue;
+        pairs.push_back(make_int2((int)t, (int)t2));
+        taken[t] = taken[t2] = 1;
+      }
+    }
+    std::vector<int32_t> rest;
+    for (size_t t = 0; t < nt; ++t)
+      if (!taken[t]) rest.push_back((int32_t)t);
+    int32_t* dpairs = nullptr;
+    int32_t* drest = nullptr;
+    if (!pairs.empty() && (rc = upload(h, &dpairs, reinterpret_cast<const int32_t*>(pairs.data()), pairs.size() * 2, st)))
+      return rc;
+    if (!rest.empty() && (rc = upload(h, &drest, rest.data(), rest.size(), st))) return rc;
+    e = cudaStreamSynchronize(st);  // host vectors leave scope
+    if (e != cudaSuccess) return cuda_fail(h, e, "mixed-form face pairs");
+    h->mx_pairs = reinterpret_cast<int2*>(dpairs);
+    h->mx_rest = drest;
+    h->mx_npairs = (int)pairs.size();
+    h->mx_nrest = (int)rest.size();
+    h->mx_paired = true;
+  }
   h->prec = AFR_PREC_MIXED;
   // The FP64 fine-point adjugates were needed only for MD and the FP32 copy;
   // the FP64 solution-point adjugates only for the set-up and the SST kernels.

@@ -503,11 +503,69 @@ __global__ void __launch_bounds__(MX_THREADS, 2)  // 64 registers: two CTAs per 
 // ---------------------------------------------------------------------------
 // face kernel: one thread per (slot, flux point), fields read at face points
 // ---------------------------------------------------------------------------
+// The jumps of slot point t from its own face-point fields ow and the other
+// side's ot (core/fr_residual/inviscid_kernel_colored.py:86-236,
+// core/fr_residual/viscous_flux_kernel.py:335-520)
+template <int NP>
+__device__ __forceinline__ void mx_face_jump(const Faces& fc, const SlotTable& st, const MxFace& mf, const MxBuf& mb,
+                                             const double* __restrict__ hcell, float mu, int visc, int t,
+                                             const float (&ow)[18], const float (&ot)[18]) {
+  const int sl = t / NP, i = t % NP;
+  const int f = st.face[sl];
+  const int e = st.cell[sl];
+  const int fl = st.flags[sl];
+  const bool is_owner = (fl & 1) == 0;
+  const bool bnd = (fl & 2) != 0;
+  const float side = (fl & 16) ? 1.f : -1.f;
+  const double* tnp = fc.tnormal + ((size_t)f * NP + i) * 3;
+  const float tn[3] = {float(tnp[0]), float(tnp[1]), float(tnp[2])};
+  const float4 ar = mf.arow[t];
+  const float a0 = ar.x, a1 = ar.y, a2 = ar.z;
+  const float mag = fmaxf(ar.w, 1e-30f);
+  float dir[3] = {a0 / mag * side, a1 / mag * side, a2 / mag * side};
+  const float sg = is_owner ? 1.f : -1.f;
+  const float t0 = sg * tn[0], t1 = sg * tn[1], t2 = sg * tn[2];
+  if (dir[0] * t0 + dir[1] * t1 + dir[2] * t2 < 0.5f) { dir[0] = t0; dir[1] = t1; dir[2] = t2; }
+  float Fc[5], Fp[3][5];
+  ausm_up<float>(ow, ot, dir, Fc);
+  euler_flux<float>(ow, Fp);
+  float* Jo = mb.Jm + (size_t)t * 10;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) Jo[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
+  if (visc) {
+    float qa[5], ga[13];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qa[v] = 0.5f * (ow[v] + ot[v]);
+#pragma unroll
+    for (int k = 0; k < 13; ++k) ga[k] = 0.5f * (ow[5 + k] + ot[5 + k]);
+    float Gc[3][5], Go[3][5];
+    viscous_flux<float>(qa, ga, ga + 9, mu, ga[12], Gc);
+    viscous_flux<float>(ow, ow + 5, ow + 14, mu, ow[17], Go);
+    float jv[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+      jv[v] = (a0 * Gc[0][v] + a1 * Gc[1][v] + a2 * Gc[2][v]) - (a0 * Go[0][v] + a1 * Go[1][v] + a2 * Go[2][v]);
+    if (bnd) {
+      // interior penalty (core/fr_operators/flux_kernels.py:140-200)
+      const float eta = float(C_IP) * (mu + ow[17]) / float(hcell[e]);
+      const float scale = eta * ar.w * side;
+#pragma unroll
+      for (int v = 1; v < 4; ++v) jv[v] += -scale * (ow[v] - ot[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Jo[5 + v] = jv[v];
+  }
+}
+
 template <int S, int NP>
 __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
-                                                 const double* __restrict__ hcell, float mu, int visc) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= st.n * NP) return;
+                                                 const double* __restrict__ hcell, float mu, int visc,
+                                                 const int32_t* __restrict__ rest, int n_rest) {
+  // slot points not taken by the paired kernel (boundary, interpolated or
+  // without a matched partner); all of them when rest is null
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (rest ? n_rest : st.n * NP)) return;
+  const int t = rest ? rest[idx] : idx;
   constexpr int NFP = 6 * NP;
   const int sl = t / NP, i = t % NP;
   const int f = st.face[sl];
@@ -516,7 +574,6 @@ __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, 
   const bool is_owner = (fl & 1) == 0;
   const bool bnd = (fl & 2) != 0;
   const int ax = (fl >> 2) & 3;
-  const float side = (fl & 16) ? 1.f : -1.f;
   const int FW = mb.FW;
   const int nf = visc ? 18 : 5;
   float ow[18], ot[18];
@@ -569,42 +626,42 @@ __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, 
       }
     }
   }
-  const float4 ar = mf.arow[t];
-  const float a0 = ar.x, a1 = ar.y, a2 = ar.z;
-  const float mag = fmaxf(ar.w, 1e-30f);
-  float dir[3] = {a0 / mag * side, a1 / mag * side, a2 / mag * side};
-  const float sg = is_owner ? 1.f : -1.f;
-  const float t0 = sg * tn[0], t1 = sg * tn[1], t2 = sg * tn[2];
-  if (dir[0] * t0 + dir[1] * t1 + dir[2] * t2 < 0.5f) { dir[0] = t0; dir[1] = t1; dir[2] = t2; }
-  float Fc[5], Fp[3][5];
-  ausm_up<float>(ow, ot, dir, Fc);
-  euler_flux<float>(ow, Fp);
-  float* Jo = mb.Jm + (size_t)t * 10;
+  mx_face_jump<NP>(fc, st, mf, mb, hcell, mu, visc, t, ow, ot);
+}
+
+// Matched interior face points in pairs: slot point t (owner side) and its
+// partner t2 (the neighbour side's slot point at the matched face point) read
+// the same two face-point rows, own and other swapped; one thread loads them
+// once and forms both jumps
+template <int S, int NP>
+__global__ void __launch_bounds__(256) k_mx_face_pair(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
+                                                      const double* __restrict__ hcell, float mu, int visc,
+                                                      const int2* __restrict__ pairs, int n_pairs) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_pairs) return;
+  constexpr int NFP = 6 * NP;
+  const int2 pr = pairs[idx];
+  const int t = pr.x, t2 = pr.y;
+  const int sl = t / NP, i = t % NP;
+  const int f = st.face[sl];
+  const int e = st.cell[sl];
+  const int fl = st.flags[sl];
+  const int ax = (fl >> 2) & 3;
+  const int FW = mb.FW;
+  const int nf = visc ? 18 : 5;
+  const int oc = fc.neighbor[f];
+  float ra[18], rb[18];
+  {
+    const float* xa = mb.XF + (size_t)e * FW * NFP + (ax * 2 + ((fl & 16) ? 1 : 0)) * NP + i;
+    const float* xb = mb.XF + (size_t)oc * FW * NFP + mf.ofp[t];
 #pragma unroll
-  for (int v = 0; v < 5; ++v) Jo[v] = Fc[v] * mag * side - (a0 * Fp[0][v] + a1 * Fp[1][v] + a2 * Fp[2][v]);
-  if (visc) {
-    float qa[5], ga[13];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) qa[v] = 0.5f * (ow[v] + ot[v]);
-#pragma unroll
-    for (int k = 0; k < 13; ++k) ga[k] = 0.5f * (ow[5 + k] + ot[5 + k]);
-    float Gc[3][5], Go[3][5];
-    viscous_flux<float>(qa, ga, ga + 9, mu, ga[12], Gc);
-    viscous_flux<float>(ow, ow + 5, ow + 14, mu, ow[17], Go);
-    float jv[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v)
-      jv[v] = (a0 * Gc[0][v] + a1 * Gc[1][v] + a2 * Gc[2][v]) - (a0 * Go[0][v] + a1 * Go[1][v] + a2 * Go[2][v]);
-    if (bnd) {
-      // interior penalty (core/fr_operators/flux_kernels.py:140-200)
-      const float eta = float(C_IP) * (mu + ow[17]) / float(hcell[e]);
-      const float scale = eta * ar.w * side;
-#pragma unroll
-      for (int v = 1; v < 4; ++v) jv[v] += -scale * (ow[v] - ot[v]);
+    for (int k = 0; k < 18; ++k) {
+      ra[k] = k < nf ? __ldg(xa + k * NFP) : 0.f;
+      rb[k] = k < nf ? __ldg(xb + k * NFP) : 0.f;
     }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) Jo[5 + v] = jv[v];
   }
+  mx_face_jump<NP>(fc, st, mf, mb, hcell, mu, visc, t, ra, rb);
+  mx_face_jump<NP>(fc, st, mf, mb, hcell, mu, visc, t2, rb, ra);
 }
 
 // ---------------------------------------------------------------------------
