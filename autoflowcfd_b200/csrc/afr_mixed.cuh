@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(256) k_mx_face(Faces fc, Bc bc, SlotTable st, 
 // the same two face-point rows, own and other swapped; one thread loads them
 // once and forms both jumps
 template <int S, int NP>
-__global__ void __launch_bounds__(256) k_mx_face_pair(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
+__global__ void __launch_bounds__(256, 3) k_mx_face_pair(Faces fc, Bc bc, SlotTable st, MxFace mf, MxBuf mb,
                                                       const double* __restrict__ hcell, float mu, int visc,
                                                       const int2* __restrict__ pairs, int n_pairs) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
