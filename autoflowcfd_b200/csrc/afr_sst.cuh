@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
 constexpr int SST_FACE_WARPS = 4;
 
 template <int S, int NP>
-__global__ void __launch_bounds__(32 * SST_FACE_WARPS) k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
+__global__ void __launch_bounds__(32 * SST_FACE_WARPS, 16) k_sst_face(Geom g, Ops ops, Faces fc, SstArgs a) {
   constexpr int W = SST_FACE_WARPS, RW = 17;  // RW: po (8), pn of the first (4) and second (4) source, pad
   constexpr int MT = (NP + 7) / 8;            // row tiles of the face points
   __shared__ double sR[W][NP * RW];
