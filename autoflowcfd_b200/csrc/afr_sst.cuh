@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128) k_sst_point(Geom g, Ops ops, SstArgs a, i
   __shared__ double f[CPB * S * 5];     // rho u, rho v, rho w, k, omega; then the pt outputs
   __shared__ double gc[CPB * S * 3 * 5];
   __shared__ double sInv[CPB * S * 9];  // inverse Jacobians; then the sp8 outputs (row stride 9)
-  __shared__ double sU[CPB * S * 8];    // state rows (stride nv <= 8)
+  __shared__ double sU[CPB * S * 7];    // state rows (stride nv = 7: SST handles carry n_vars 7)
   const int e0 = cell_base + blockIdx.x * CPB;
   const int nc = min(CPB, cell_end - e0);
   const int ct = cell_type(g, e0);
